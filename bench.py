@@ -1,0 +1,418 @@
+"""Benchmark: relative 5D capture-tube solve (ENO2 / Lax-Friedrichs / RK2).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (the 89M-cell table): RelativeGrid(65, 48, 21, 21, 8.0) — 65 x 65
+relative positions on [-8, 8] m, 48 headings, 21 x 21 speed levels —
+reversible_free_a3 physics (both accelerations 3 m/s^2), CFL 0.8, horizon
+3.0 s = 900 RK2 steps = 1800 stage launches.  Values and local arithmetic are
+float32 (the fast path).  One bench step = one full solve to the horizon:
+initialise the capture field, advance 900 steps.
+
+Metric: cell-backups/s = cells x stages / seconds (one cell-backup = one ENO/LF
+stage update of one cell).  `value` times device-resident solves with CUDA
+events on the solver's stream; `e2e` times the same solve through the public
+RelativeSolver API with host buffers: the initial field uploaded from pinned
+memory and the final field and arrival times read back every step.  The
+field (357.7 MB) is larger than the 126 MB L2, so no flush is needed between
+iterations.
+
+Multi-GPU (torchrun): every rank solves its own table (independent replicas,
+weak scaling, no data-path collective); `value` = all ranks' cell-backups over
+the slowest rank's device time.
+
+--impl reference runs the reference's own CPU implementation of the path
+(native_relative.cpp compiled from the reference sources into
+oracle/_ref/relative5d) on all host cores, on a bounded sample of the same
+workload (the same grid and physics, a few RK2 steps per bench step).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+from pathlib import Path
+import shutil
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO / "pursuit-evasion-core_b200"))
+sys.path.insert(0, str(REPO))
+
+GRID = dict(positions=65, headings=48, p_speeds=21, e_speeds=21, extent=8.0)
+HORIZON = 3.0
+METRIC = "cell-backups/s"
+REF_EXE = REPO / "oracle" / "_ref" / "relative5d"
+ORACLE_LIB = REPO / "oracle" / "_build" / "liboracle.so"
+
+
+def a3_config():
+    from pursuit_evasion_b200.reversible.model import ReversibleConfig, VehicleLimits
+
+    return ReversibleConfig(
+        name="reversible_free_a3",
+        pursuer=VehicleLimits(-1.0, 2.0, 3.0, 1.0),
+        evader=VehicleLimits(-0.5, 1.0, 3.0, 2.0),
+    )
+
+
+def workload_name():
+    g = GRID
+    return (f"relative5d_eno2_lf_rk2 RelativeGrid({g['positions']},{g['headings']},"
+            f"{g['p_speeds']},{g['e_speeds']},{g['extent']}) reversible_free_a3 "
+            f"horizon {HORIZON} s cfl 0.8")
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu_index = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        if shutil.which("nvidia-smi") is None:
+            return
+        fd, self.path = tempfile.mkstemp(prefix="pe_clocks_", suffix=".csv")
+        os.close(fd)
+        self.file = open(self.path, "w")
+        self.proc = subprocess.Popen(
+            ["nvidia-smi", "-i", str(self.gpu_index), f"--query-gpu={self.QUERY}",
+             "--format=csv,noheader,nounits", "-lms", "200"],
+            stdout=self.file, stderr=subprocess.DEVNULL)
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.file.close()
+        rows = []
+        for line in Path(self.path).read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) == 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        sm_max = max(float(r[2]) for r in rows if r[2].replace(".", "").isdigit())
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4)
+                          if r[5 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": sm_max, "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def measured_peaks():
+    path = REPO / "MEASURED_PEAKS.json"
+    if path.exists():
+        data = json.loads(path.read_text())
+        return float(data["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """dram bytes per stage launch from the committed ncu summary, if any."""
+    path = REPO / "profiles" / "relative5d_stage_traffic.json"
+    if path.exists():
+        return json.loads(path.read_text())
+    return None
+
+
+def reference_sample(cells_grid, steps, threads):
+    """Run the reference executable on the bench grid for `steps` RK2 steps;
+    returns (update_seconds, internal_steps)."""
+    from pursuit_evasion_b200.reversible.relative_solver import cfl_limit
+    from pursuit_evasion_b200.reversible.free_dp import RelativeGrid
+
+    config = a3_config()
+    grid = RelativeGrid(**GRID)
+    limit = cfl_limit(config, grid)
+    horizon = steps * limit
+    p, e = config.pursuer, config.evader
+    out = Path(tempfile.mkdtemp(prefix="pe_refbench_"))
+    options = {
+        "positions": grid.positions, "headings": grid.headings,
+        "p-speeds": grid.p_speeds, "e-speeds": grid.e_speeds,
+        "extent": grid.extent, "radius": config.capture_radius,
+        "p-min": p.speed_min, "p-max": p.speed_max, "e-min": e.speed_min,
+        "e-max": e.speed_max, "p-acceleration": p.acceleration,
+        "e-acceleration": e.acceleration, "p-curvature": p.max_curvature,
+        "e-curvature": e.max_curvature, "horizon": repr(horizon),
+        "output-dt": repr(horizon), "order": 2, "cfl": 0.8, "threads": threads,
+        "history": 0, "output": str(out),
+    }
+    cmd = [str(REF_EXE)] + [str(x) for k, v in options.items()
+                            for x in ("--" + k, v)]
+    try:
+        subprocess.run(cmd, check=True, capture_output=True)
+        timing = json.loads((out / "timing.json").read_text())
+    finally:
+        shutil.rmtree(out, ignore_errors=True)
+    return float(timing["update_seconds"]), int(timing["internal_steps"])
+
+
+def oracle_sample(steps, threads):
+    """The oracle port (oracle/relative5d.c) on the bench grid, `steps` RK2
+    steps; used only when the reference executable is not built."""
+    import ctypes
+    from tests import oracle_lib
+    from pursuit_evasion_b200.reversible.free_dp import RelativeGrid
+
+    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    o = oracle_lib.load()
+    grid = RelativeGrid(**GRID)
+    cfg = o.rel_cfg(a3_config(), grid)
+    n = grid.states
+    a = np.empty(n, np.float32)
+    b = np.empty(n, np.float32)
+    arr = np.empty(n, np.float32)
+    o.lib.po_rel_init(ctypes.addressof(cfg), a.ctypes.data, arr.ctypes.data)
+    dt = o.rel_cfl_limit(cfg)
+    t0 = time.perf_counter()
+    for k in range(steps):
+        o.rel_stage_f32(cfg, a, b, arr, dt, k * dt, 0)
+        o.rel_stage_f32(cfg, b, a, arr, dt, k * dt, 1)
+    return time.perf_counter() - t0, steps
+
+
+def cpu_baseline(steps=3):
+    threads = os.cpu_count() or 1
+    cells = int(np.prod([GRID["p_speeds"], GRID["e_speeds"], GRID["headings"],
+                         GRID["positions"], GRID["positions"]]))
+    if REF_EXE.exists():
+        seconds, taken = reference_sample(cells, steps, threads)
+        kind = "reference"
+        what = "native_relative.cpp built from the reference sources"
+    else:
+        seconds, taken = oracle_sample(steps, threads)
+        kind = "port"
+        what = "oracle/relative5d.c restatement"
+    value = cells * taken * 2 / seconds
+    return {
+        "value": value, "unit": METRIC, "cores": threads, "kind": kind,
+        "sample": (f"{what}: {taken} RK2 steps ({2 * taken} stages) of the "
+                   f"{cells}-cell bench grid, update loop only, "
+                   f"{seconds:.3f} s on {threads} threads"),
+    }
+
+
+# ---------------------------------------------------------------------------
+def run_reference_arm(args, world, rank):
+    if rank != 0:
+        return
+    steps_per_sample = 2
+    threads = os.cpu_count() or 1
+    cells = int(np.prod(list(GRID.values())[:4]) * GRID["positions"])
+    for _ in range(args.warmup):
+        if REF_EXE.exists():
+            reference_sample(cells, steps_per_sample, threads)
+        else:
+            oracle_sample(steps_per_sample, threads)
+    total_s = 0.0
+    total_steps = 0
+    for _ in range(args.steps):
+        if REF_EXE.exists():
+            s, n = reference_sample(cells, steps_per_sample, threads)
+        else:
+            s, n = oracle_sample(steps_per_sample, threads)
+        total_s += s
+        total_steps += n
+    value = cells * total_steps * 2 / total_s
+    kind = "reference" if REF_EXE.exists() else "port"
+    line = {
+        "impl": "reference",
+        "metric": METRIC, "value": value, "unit": METRIC,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * total_s / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 storage, f64 local", "data": "synthetic (deterministic grid)",
+        "config": {"workload": workload_name(), "cells": cells,
+                   "sample_rk2_steps_per_step": steps_per_sample,
+                   "parallelism": f"OpenMP {threads} threads"},
+        "cpu_baseline": {
+            "value": value, "unit": METRIC, "cores": threads, "kind": kind,
+            "sample": (f"{steps_per_sample} RK2 steps of the bench grid per "
+                       f"step, update loop only (reference timing.json)"),
+        },
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, world, rank, local):
+    import torch
+
+    from pursuit_evasion_b200 import _native
+    from pursuit_evasion_b200.reversible.free_dp import RelativeGrid
+    from pursuit_evasion_b200.reversible.relative_solver import RelativeSolver
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    config = a3_config()
+    grid = RelativeGrid(**GRID)
+    cells = grid.states
+    solver = RelativeSolver(config, grid, local_precision=args.precision,
+                            device=local)
+    stream = torch.cuda.current_stream()
+    solver.set_stream(stream.cuda_stream)
+    stages_per_solve = None
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+
+    def one_solve():
+        solver.initialize()
+        return solver.advance(HORIZON)
+
+    for _ in range(args.warmup):
+        steps = one_solve()
+    stages_per_solve = 2 * steps
+    solver.synchronize()
+
+    clocks = ClockSampler(local)
+    barrier()
+    clocks.start()
+    launches0 = _native.launch_count()
+    solver.profile(True)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for _ in range(args.steps):
+        one_solve()
+    end.record(stream)
+    barrier()
+    clock_info = clocks.stop()
+    launches = _native.launch_count() - launches0
+    elapsed_ms = start.elapsed_time(end)
+    stage_ms = [solver.kernel_time(0), solver.kernel_time(1)]
+    solver.profile(False)
+    solver.synchronize()
+
+    # e2e: public API with host buffers, pinned memory both ways.
+    host_init = torch.empty(cells, dtype=torch.float32, pin_memory=True)
+    host_field = torch.empty(cells, dtype=torch.float32, pin_memory=True)
+    host_arrival = torch.empty(cells, dtype=torch.float32, pin_memory=True)
+    solver.initialize()
+    solver.copy_field_to(host_init.data_ptr())  # the capture field as the input
+    init_np = host_init.numpy()
+    barrier()
+    e_start, e_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e_start.record(stream)
+    for _ in range(args.steps):
+        solver.initialize(init_np)
+        solver.advance(HORIZON)
+        solver.copy_field_to(host_field.data_ptr())
+        solver._lib.pe_relative_copy_arrival(solver._h, host_arrival.data_ptr())
+    e_end.record(stream)
+    barrier()
+    e2e_ms = e_start.elapsed_time(e_end)
+
+    # max over ranks
+    times = torch.tensor([elapsed_ms, e2e_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(times, op=torch.distributed.ReduceOp.MAX)
+    elapsed_ms, e2e_ms = times.tolist()
+    backups = cells * stages_per_solve * args.steps * world
+    value = backups / (elapsed_ms / 1e3)
+    e2e_value = backups / (e2e_ms / 1e3)
+
+    line = None
+    if rank == 0:
+        peak, peak_kind = measured_peaks()
+        (ms1, n1), (ms2, n2) = stage_ms
+        bytes1, bytes2 = 8 * cells, 12 * cells
+        achieved = (bytes1 * n1 + bytes2 * n2) / ((ms1 + ms2) / 1e3) / 1e9
+        traffic = profile_traffic()
+        roofline = {
+            "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",
+            "kernel": "rel5_stage_fast_kernel (stage 1 + stage 2)",
+            "algorithmic_bytes_per_launch": {"stage1": bytes1, "stage2": bytes2},
+            "avg_launch_ms": {"stage1": ms1 / max(n1, 1), "stage2": ms2 / max(n2, 1)},
+            "traffic": None if traffic is None else traffic.get("bytes_per_launch"),
+        }
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": elapsed_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if args.precision == "float32" else "f32 storage, f64 local",
+            "data": "synthetic (deterministic grid, no dataset)",
+            "config": {
+                "workload": workload_name(), "cells": cells,
+                "stages_per_step": stages_per_solve,
+                "precision": args.precision,
+                "l2": "inputs larger than L2 (357.7 MB field), no flush",
+                "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+            },
+            "roofline": roofline,
+            "e2e": {"value": e2e_value, "unit": METRIC,
+                    "h2d_bytes_per_step": 4 * cells,
+                    "d2h_bytes_per_step": 8 * cells,
+                    "ms_per_step": e2e_ms / args.steps},
+            "gpu_launches": int(launches),
+            "clocks": clock_info,
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline()
+        print(json.dumps(line), flush=True)
+    solver.close()
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    return line
+
+
+def main():
+    parser = argparse.ArgumentParser(description=__doc__)
+    parser.add_argument("--gpus", type=int, default=1)
+    parser.add_argument("--steps", type=int, default=5)
+    parser.add_argument("--warmup", type=int, default=3)
+    parser.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    parser.add_argument("--precision", choices=["float32", "float64"],
+                        default="float32")
+    parser.add_argument("--no-cpu-baseline", action="store_true")
+    args = parser.parse_args()
+    # At least three warm-up solves are always run.
+    args.warmup = max(args.warmup, 3)
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        run_reference_arm(args, world, rank)
+    else:
+        run_ours(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,137 @@
+/*
+ * pe_b200.h — C ABI of the B200 game-value solver (libpe_b200.so).
+ *
+ * Plain C types only.  Every function returns PE_OK (0) or a negative error
+ * code; pe_last_error() then holds a message for the calling thread.  A handle
+ * owns its device buffers and one CUDA stream; the caller owns host buffers.
+ * Use one handle per host thread.
+ *
+ * Reference interfaces these entry points replace (pursuit-evasion-core,
+ * paths under src/pursuit_evasion/):
+ *   - reversible/free_dp.py:259-261 runs the native executable
+ *     reversible/native_relative.cpp:236-271 (argv in, fields.f32 out);
+ *   - reversible/gpu_relative.py:170-179 and :322-342 launch the CuPy
+ *     RawKernels `initialize` and `advance` (gpu_relative.py:26-45).
+ * The relative-5D handle takes the reference executable's options
+ * (native_relative.cpp:19-26, :244-262) as pe_relative_params, and performs
+ * the executable's init (native_relative.cpp:91-100), its step loop
+ * (:173-190) and its two stages per RK2 step (:124-172) on the GPU.
+ */
+#ifndef PE_B200_H
+#define PE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PE_ABI_VERSION 1
+
+enum {
+  PE_OK = 0,
+  PE_EINVAL = -1,     /* invalid option or argument (reference: "Invalid solver options") */
+  PE_ENOMEM = -2,     /* device allocation failed */
+  PE_ENONFINITE = -3, /* an update produced a non-finite value
+                         (reference: native_relative.cpp:162-163) */
+  PE_ETIMEOUT = -4,   /* a bounded device wait gave up */
+  PE_ECUDA = -5,      /* any other CUDA runtime error */
+  PE_ESTATE = -6      /* call out of order (e.g. advance before init) */
+};
+
+enum { PE_LOCAL_F32 = 0, PE_LOCAL_F64 = 1 };
+enum { PE_SCHEME_ENO_LF = 0 };
+
+/* Options of the reference executable native_relative.cpp:19-26, plus the
+ * scheme, the local arithmetic precision and the CUDA device. */
+typedef struct pe_relative_params {
+  int32_t positions, headings, p_speeds, e_speeds; /* RelativeGrid */
+  double extent;                                   /* --extent */
+  double capture_radius;                           /* --radius */
+  double p_speed_min, p_speed_max, p_acceleration, p_curvature;
+  double e_speed_min, e_speed_max, e_acceleration, e_curvature;
+  double cfl;        /* --cfl, in (0, 1] */
+  int32_t order;     /* --order, 1 or 2 */
+  int32_t scheme;    /* PE_SCHEME_ENO_LF */
+  int32_t precision; /* PE_LOCAL_F64 reproduces the reference executable bit
+                        for bit; PE_LOCAL_F32 is the fast path */
+  int32_t device;    /* CUDA device ordinal */
+} pe_relative_params;
+
+typedef struct pe_relative pe_relative;
+
+/* Library ABI version (PE_ABI_VERSION). */
+int pe_version(void);
+
+/* Message of the last failed call on this thread ("" if none). */
+const char *pe_last_error(void);
+
+/* Number of kernels this library has launched in this process. */
+int64_t pe_launch_count(void);
+
+/* Number of cells and the CFL time-step limit of a relative grid, computed
+ * on the host exactly as native_relative.cpp:70-81 (no GPU needed). */
+int pe_relative_cells(const pe_relative_params *params, int64_t *cells);
+int pe_relative_cfl_limit(const pe_relative_params *params, double *dt_limit);
+
+/* Validate options (native_relative.cpp:263-268) and allocate the field,
+ * the stage buffer and the arrival array on params->device. */
+int pe_relative_create(const pe_relative_params *params, pe_relative **out);
+
+/* Run the handle's work on a caller-owned stream (cudaStream_t passed as
+ * void*; NULL restores the handle's own stream). */
+int pe_relative_set_stream(pe_relative *h, void *cuda_stream);
+
+/* Initialise at time start_time.  initial == NULL: the circular capture field
+ * float(hypot(x, y) - radius) of native_relative.cpp:91-100, computed in
+ * double on the host for one (y, x) plane and broadcast on the device.
+ * Otherwise a full host field of `cells` floats (a warm start or a
+ * continuation).  arrival == NULL: arrival = start_time where the field is
+ * <= 0, else NaN. */
+int pe_relative_init(pe_relative *h, const float *initial,
+                     const float *arrival, double start_time);
+
+/* Advance the handle's time to `goal` with internal steps of
+ * min(cfl_limit, goal - t) (native_relative.cpp:180-190).  Enqueues the
+ * work; steps_taken (may be NULL) receives the number of steps. */
+int pe_relative_advance(pe_relative *h, double goal, int64_t *steps_taken);
+
+/* One step of exactly dt (dt > 0). */
+int pe_relative_step(pe_relative *h, double dt);
+
+/* Current time and step count. */
+int pe_relative_time(const pe_relative *h, double *t, int64_t *steps);
+
+/* Wait for the handle's work; returns PE_ENONFINITE if any update since the
+ * last check produced a non-finite value. */
+int pe_relative_synchronize(pe_relative *h);
+
+/* Copy the current field / arrival times (cells floats each) to host memory
+ * (synchronous; the copies come from the handle's stream). */
+int pe_relative_copy_field(pe_relative *h, float *host_field);
+int pe_relative_copy_arrival(pe_relative *h, float *host_arrival);
+
+/* Device address of the current field (cells floats, storage order
+ * [vP, vE, psi, y, x]); valid until the next step or destroy. */
+int pe_relative_device_field(pe_relative *h, float **device_field);
+
+/* Sup-norm change max|V_new - V_old| of the most recent step, reduced in
+ * double, and the largest increase of any cell since init (the reference's
+ * maximum_increase diagnostic, native_relative.cpp:166, :233).  Synchronises. */
+int pe_relative_stats(pe_relative *h, double *residual, double *max_increase);
+
+/* Per-stage kernel timing with CUDA events on the handle's stream: enable,
+ * then read the summed device milliseconds and launch count of stage 1
+ * (stage=0) or stage 2 (stage=1) since enabling. */
+int pe_relative_profile(pe_relative *h, int enable);
+int pe_relative_kernel_time(pe_relative *h, int stage, double *total_ms,
+                            int64_t *launches);
+
+/* Release device memory and the handle. */
+int pe_relative_destroy(pe_relative *h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PE_B200_H */

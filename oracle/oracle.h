@@ -1,0 +1,56 @@
+/*
+ * CPU ORACLE — test infrastructure only (see relative5d.c).  These functions
+ * are the checker for the CUDA path: tests, the smoke check and the CPU
+ * baseline leg of bench.py call them; the product never does.
+ */
+#ifndef PE_ORACLE_H
+#define PE_ORACLE_H
+#include <stddef.h>
+#include <stdint.h>
+
+#define PO_ENOMEM (-2)
+#define PO_ENONFINITE (-3)
+#define PO_EINVAL (-1)
+
+/* Relative 5D game: storage [vP, vE, psi, y, x], x fastest. */
+typedef struct {
+  int nx, nh, nvp, nve, order;
+  double extent, radius, vp_lo, vp_hi, ve_lo, ve_hi, acc_p, acc_e, curv_p,
+      curv_e, cfl;
+} po_rel_cfg;
+
+size_t po_rel_cells(const po_rel_cfg *c);
+double po_rel_cfl_limit(const po_rel_cfg *c);
+void po_rel_init(const po_rel_cfg *c, float *field, float *arrival);
+void po_rel_init_f64(const po_rel_cfg *c, double *field);
+int po_rel_stage_f32(const po_rel_cfg *c, const float *src, float *dst,
+                     float *arrival, double dt, double t, int blend,
+                     double *max_increase);
+int po_rel_stage_f64(const po_rel_cfg *c, const double *src, double *dst,
+                     double dt, int blend);
+int po_rel_solve_f32(const po_rel_cfg *c, double horizon, double output_dt,
+                     float *frames, float *arrival, long *steps_out);
+int po_rel_solve_f64(const po_rel_cfg *c, double horizon, double output_dt,
+                     double *final, long *steps_out);
+
+/* Dense 8D game: storage [xP, yP, thP, vP, xE, yE, thE, vE], vE fastest. */
+typedef struct {
+  int n, nh, np, ne, order;
+  int linear_speed;  /* 1: inward one-sided slopes at the speed bounds */
+  int avoid_square;  /* 1: reference square-arena avoid floor; 0: none */
+  float extent, arena, radius, p_lo, p_hi, e_lo, e_hi, ap, ae, kp, ke;
+  double cfl;
+} po_w8_cfg;
+
+size_t po_w8_cells(const po_w8_cfg *c);
+double po_w8_dt_limit(const po_w8_cfg *c);
+void po_w8_init_square(const po_w8_cfg *c, float *a, float *arrival);
+double po_rect_separation(double px, double py, double pth, double ex,
+                          double ey, double eth, double p_len, double p_wid,
+                          double e_len, double e_wid);
+void po_w8_init_contact(const po_w8_cfg *c, double p_len, double p_wid,
+                        double e_len, double e_wid, float *a, float *arrival);
+int po_w8_stage(const po_w8_cfg *c, const float *src, float *dst,
+                const float *base, float *arrival, float dt, double tau);
+
+#endif

@@ -1,0 +1,460 @@
+// C-ABI of the relative 5D solver handle (declared in include/pe_b200.h).
+//
+// Host-side restatement of the reference executable's driver
+// (native_relative.cpp:68-90 set-up, :91-100 init, :173-190 step loop); the
+// per-cell work runs in relative5d_fast.cu / relative5d_exact.cu.
+#include <cmath>
+#include <cstring>
+#include <utility>
+#include <vector>
+
+#include "pe_internal.h"
+#include "relative5d.cuh"
+
+struct pe_relative {
+  pe_relative_params p{};
+  pe::Rel5Grid g{};
+  double limit = 0;
+  float *a = nullptr, *b = nullptr, *arrival = nullptr, *plane = nullptr;
+  double *sn = nullptr, *cs = nullptr;
+  float *snf = nullptr, *csf = nullptr;
+  pe::Rel5Stats *stats = nullptr;       // device
+  pe::Rel5Stats *host_stats = nullptr;  // pinned mirror
+  cudaStream_t own = nullptr, stream = nullptr;
+  double t = 0;
+  int64_t steps = 0;
+  bool initialized = false;
+  bool profiling = false;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending[2];
+  std::vector<cudaEvent_t> spare;
+  double prof_ms[2] = {0, 0};
+  int64_t prof_n[2] = {0, 0};
+};
+
+namespace {
+
+using pe::fail;
+
+bool finite_all(std::initializer_list<double> values) {
+  for (double v : values)
+    if (!std::isfinite(v)) return false;
+  return true;
+}
+
+int validate(const pe_relative_params *p) {
+  if (!p) return fail(PE_EINVAL, "params is NULL");
+  if (p->positions < 3 || p->headings < 4 || p->p_speeds < 3 ||
+      p->e_speeds < 3)
+    return fail(PE_EINVAL,
+                "Invalid solver options: grid needs positions>=3, headings>=4, "
+                "speeds>=3");
+  if (p->order != 1 && p->order != 2)
+    return fail(PE_EINVAL, "Invalid solver options: order must be 1 or 2");
+  if (p->scheme != PE_SCHEME_ENO_LF)
+    return fail(PE_EINVAL, "Invalid solver options: unknown scheme %d",
+                p->scheme);
+  if (p->precision != PE_LOCAL_F32 && p->precision != PE_LOCAL_F64)
+    return fail(PE_EINVAL, "Invalid solver options: unknown precision %d",
+                p->precision);
+  if (!finite_all({p->extent, p->capture_radius, p->p_speed_min,
+                   p->p_speed_max, p->p_acceleration, p->p_curvature,
+                   p->e_speed_min, p->e_speed_max, p->e_acceleration,
+                   p->e_curvature, p->cfl}))
+    return fail(PE_EINVAL, "Invalid solver options: non-finite value");
+  if (p->extent <= p->capture_radius || p->capture_radius <= 0 ||
+      p->cfl <= 0 || p->cfl > 1 || p->p_acceleration <= 0 ||
+      p->e_acceleration <= 0 || p->p_curvature <= 0 || p->e_curvature <= 0 ||
+      p->p_speed_min >= p->p_speed_max || p->e_speed_min >= p->e_speed_max)
+    return fail(PE_EINVAL, "Invalid solver options");
+  if ((int64_t)p->p_speeds * p->e_speeds > 65535 || p->headings > 65535 ||
+      (int64_t)p->positions * p->positions > (1 << 30))
+    return fail(PE_EINVAL, "Invalid solver options: grid too large");
+  return PE_OK;
+}
+
+pe::Rel5Grid make_grid(const pe_relative_params *p) {
+  pe::Rel5Grid g{};
+  const double pi = std::acos(-1.0);
+  g.nx = p->positions;
+  g.nh = p->headings;
+  g.nvp = p->p_speeds;
+  g.nve = p->e_speeds;
+  g.order = p->order;
+  g.sy = g.nx;
+  g.sp = (int64_t)g.nx * g.nx;
+  g.se = g.sp * g.nh;
+  g.sv = g.se * g.nve;
+  g.n = g.sv * g.nvp;
+  g.extent = p->extent;
+  g.dx = 2 * p->extent / (p->positions - 1);
+  g.dphi = 2 * pi / p->headings;
+  g.dvp = (p->p_speed_max - p->p_speed_min) / (p->p_speeds - 1);
+  g.dve = (p->e_speed_max - p->e_speed_min) / (p->e_speeds - 1);
+  g.vp_lo = p->p_speed_min;
+  g.ve_lo = p->e_speed_min;
+  g.acc_p = p->p_acceleration;
+  g.acc_e = p->e_acceleration;
+  g.curv_p = p->p_curvature;
+  g.curv_e = p->e_curvature;
+  return g;
+}
+
+double cfl_limit(const pe_relative_params *p, const pe::Rel5Grid &g) {
+  const double VP = std::max(std::abs(p->p_speed_min), std::abs(p->p_speed_max));
+  const double VE = std::max(std::abs(p->e_speed_min), std::abs(p->e_speed_max));
+  const double rate = (VP + VE + VP * p->p_curvature * p->extent) / g.dx +
+                      (VE + VP * p->p_curvature * p->extent) / g.dx +
+                      (VP * p->p_curvature + VE * p->e_curvature) / g.dphi +
+                      p->p_acceleration / g.dvp + p->e_acceleration / g.dve;
+  return p->cfl / rate;
+}
+
+void release(pe_relative *h) {
+  cudaFree(h->a);
+  cudaFree(h->b);
+  cudaFree(h->arrival);
+  cudaFree(h->plane);
+  cudaFree(h->sn);
+  cudaFree(h->cs);
+  cudaFree(h->snf);
+  cudaFree(h->csf);
+  cudaFree(h->stats);
+  if (h->host_stats) cudaFreeHost(h->host_stats);
+  for (auto &list : h->pending)
+    for (auto &e : list) {
+      cudaEventDestroy(e.first);
+      cudaEventDestroy(e.second);
+    }
+  for (auto e : h->spare) cudaEventDestroy(e);
+  if (h->own) cudaStreamDestroy(h->own);
+}
+
+cudaEvent_t take_event(pe_relative *h) {
+  if (!h->spare.empty()) {
+    cudaEvent_t e = h->spare.back();
+    h->spare.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+// Sum the elapsed time of recorded stage launches (waits for them).
+int drain_profile(pe_relative *h) {
+  for (int s = 0; s < 2; s++) {
+    for (auto &pr : h->pending[s]) {
+      PE_CUDA_TRY(cudaEventSynchronize(pr.second));
+      float ms = 0;
+      PE_CUDA_TRY(cudaEventElapsedTime(&ms, pr.first, pr.second));
+      h->prof_ms[s] += ms;
+      h->prof_n[s] += 1;
+      h->spare.push_back(pr.first);
+      h->spare.push_back(pr.second);
+    }
+    h->pending[s].clear();
+  }
+  return PE_OK;
+}
+
+int launch_stage(pe_relative *h, int stage, const float *src, float *dst,
+                 double dt, int blend) {
+  pe::Rel5Stage s{};
+  s.src = src;
+  s.dst = dst;
+  s.arrival = h->arrival;
+  s.sn = h->sn;
+  s.cs = h->cs;
+  s.snf = h->snf;
+  s.csf = h->csf;
+  s.dt = dt;
+  s.t = h->t;
+  s.stats = h->stats;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (h->profiling) {
+    e0 = take_event(h);
+    e1 = take_event(h);
+    PE_CUDA_TRY(cudaEventRecord(e0, h->stream));
+  }
+  const cudaError_t err = h->p.precision == PE_LOCAL_F64
+                              ? pe::rel5_stage_f64(h->g, s, blend, h->stream)
+                              : pe::rel5_stage_f32(h->g, s, blend, h->stream);
+  if (err != cudaSuccess) return pe::cuda_fail(err, "relative stage launch");
+  pe::count_launches(1);
+  if (h->profiling) {
+    PE_CUDA_TRY(cudaEventRecord(e1, h->stream));
+    h->pending[stage].push_back({e0, e1});
+    if (h->pending[stage].size() > 4096) return drain_profile(h);
+  }
+  return PE_OK;
+}
+
+int step_impl(pe_relative *h, double dt) {
+  PE_CUDA_TRY(cudaMemsetAsync(&h->stats->residual, 0, sizeof(unsigned long long),
+                              h->stream));
+  int rc;
+  if (h->g.order == 1) {
+    rc = launch_stage(h, 0, h->a, h->b, dt, 0);
+    if (rc) return rc;
+    std::swap(h->a, h->b);
+  } else {
+    rc = launch_stage(h, 0, h->a, h->b, dt, 0);
+    if (rc) return rc;
+    rc = launch_stage(h, 1, h->b, h->a, dt, 1);
+    if (rc) return rc;
+  }
+  h->t += dt;
+  h->steps += 1;
+  return PE_OK;
+}
+
+int read_stats(pe_relative *h) {
+  PE_CUDA_TRY(cudaMemcpyAsync(h->host_stats, h->stats, sizeof(pe::Rel5Stats),
+                              cudaMemcpyDeviceToHost, h->stream));
+  PE_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  if (h->host_stats->nonfinite)
+    return fail(PE_ENONFINITE, "Nonfinite field update");
+  return PE_OK;
+}
+
+int enter(pe_relative *h) {
+  if (!h) return fail(PE_EINVAL, "handle is NULL");
+  PE_CUDA_TRY(cudaSetDevice(h->p.device));
+  return PE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pe_relative_cells(const pe_relative_params *params, int64_t *cells) {
+  const int rc = validate(params);
+  if (rc) return rc;
+  if (!cells) return fail(PE_EINVAL, "cells is NULL");
+  *cells = make_grid(params).n;
+  return PE_OK;
+}
+
+int pe_relative_cfl_limit(const pe_relative_params *params, double *dt_limit) {
+  const int rc = validate(params);
+  if (rc) return rc;
+  if (!dt_limit) return fail(PE_EINVAL, "dt_limit is NULL");
+  *dt_limit = cfl_limit(params, make_grid(params));
+  return PE_OK;
+}
+
+int pe_relative_create(const pe_relative_params *params, pe_relative **out) {
+  if (!out) return fail(PE_EINVAL, "out is NULL");
+  *out = nullptr;
+  int rc = validate(params);
+  if (rc) return rc;
+  PE_CUDA_TRY(cudaSetDevice(params->device));
+  pe_relative *h = new pe_relative();
+  h->p = *params;
+  h->g = make_grid(params);
+  h->limit = cfl_limit(params, h->g);
+  const size_t bytes = sizeof(float) * (size_t)h->g.n;
+  const int nh = h->g.nh;
+  std::vector<double> sn(nh), cs(nh);
+  std::vector<float> snf(nh), csf(nh);
+  const double pi = std::acos(-1.0);
+  for (int k = 0; k < nh; k++) {
+    const double q = -pi + k * h->g.dphi;  // native_relative.cpp:84-89
+    sn[k] = std::sin(q);
+    cs[k] = std::cos(q);
+    snf[k] = (float)sn[k];
+    csf[k] = (float)cs[k];
+  }
+  cudaError_t err = cudaSuccess;
+  auto take = [&](cudaError_t e) {
+    if (err == cudaSuccess) err = e;
+  };
+  take(cudaStreamCreateWithFlags(&h->own, cudaStreamNonBlocking));
+  h->stream = h->own;
+  take(cudaMalloc(&h->a, bytes));
+  take(cudaMalloc(&h->b, bytes));
+  take(cudaMalloc(&h->arrival, bytes));
+  take(cudaMalloc(&h->plane, sizeof(float) * (size_t)h->g.sp));
+  take(cudaMalloc(&h->sn, sizeof(double) * nh));
+  take(cudaMalloc(&h->cs, sizeof(double) * nh));
+  take(cudaMalloc(&h->snf, sizeof(float) * nh));
+  take(cudaMalloc(&h->csf, sizeof(float) * nh));
+  take(cudaMalloc(&h->stats, sizeof(pe::Rel5Stats)));
+  take(cudaMallocHost(&h->host_stats, sizeof(pe::Rel5Stats)));
+  if (err == cudaSuccess) {
+    take(cudaMemcpy(h->sn, sn.data(), sizeof(double) * nh, cudaMemcpyHostToDevice));
+    take(cudaMemcpy(h->cs, cs.data(), sizeof(double) * nh, cudaMemcpyHostToDevice));
+    take(cudaMemcpy(h->snf, snf.data(), sizeof(float) * nh, cudaMemcpyHostToDevice));
+    take(cudaMemcpy(h->csf, csf.data(), sizeof(float) * nh, cudaMemcpyHostToDevice));
+    take(cudaMemset(h->stats, 0, sizeof(pe::Rel5Stats)));
+  }
+  if (err != cudaSuccess) {
+    rc = pe::cuda_fail(err, "pe_relative_create");
+    release(h);
+    delete h;
+    return rc;
+  }
+  *out = h;
+  return PE_OK;
+}
+
+int pe_relative_set_stream(pe_relative *h, void *cuda_stream) {
+  int rc = enter(h);
+  if (rc) return rc;
+  h->stream = cuda_stream ? (cudaStream_t)cuda_stream : h->own;
+  return PE_OK;
+}
+
+int pe_relative_init(pe_relative *h, const float *initial,
+                     const float *arrival, double start_time) {
+  int rc = enter(h);
+  if (rc) return rc;
+  if (!std::isfinite(start_time) || start_time < 0)
+    return fail(PE_EINVAL, "start_time must be finite and >= 0");
+  const size_t bytes = sizeof(float) * (size_t)h->g.n;
+  PE_CUDA_TRY(cudaMemsetAsync(h->stats, 0, sizeof(pe::Rel5Stats), h->stream));
+  if (!initial) {
+    // The circular capture field of native_relative.cpp:91-100, one (y, x)
+    // plane in double on the host, cast to float, broadcast on the device.
+    const int nx = h->g.nx;
+    std::vector<float> plane((size_t)nx * nx);
+    for (int iy = 0; iy < nx; iy++) {
+      const double y = -h->g.extent + iy * h->g.dx;
+      for (int ix = 0; ix < nx; ix++)
+        plane[(size_t)iy * nx + ix] = (float)(
+            std::hypot(-h->g.extent + ix * h->g.dx, y) - h->p.capture_radius);
+    }
+    PE_CUDA_TRY(cudaMemcpyAsync(h->plane, plane.data(),
+                                sizeof(float) * plane.size(),
+                                cudaMemcpyHostToDevice, h->stream));
+    PE_CUDA_TRY(pe::rel5_init(h->g, h->plane, h->a, h->arrival,
+                              (float)start_time, h->stream));
+    pe::count_launches(1);
+    PE_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  } else {
+    PE_CUDA_TRY(cudaMemcpyAsync(h->a, initial, bytes, cudaMemcpyHostToDevice,
+                                h->stream));
+    if (arrival) {
+      PE_CUDA_TRY(cudaMemcpyAsync(h->arrival, arrival, bytes,
+                                  cudaMemcpyHostToDevice, h->stream));
+    } else {
+      PE_CUDA_TRY(pe::rel5_init(h->g, nullptr, h->a, h->arrival,
+                                (float)start_time, h->stream));
+      pe::count_launches(1);
+    }
+    PE_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  }
+  h->t = start_time;
+  h->steps = 0;
+  h->initialized = true;
+  return PE_OK;
+}
+
+int pe_relative_advance(pe_relative *h, double goal, int64_t *steps_taken) {
+  int rc = enter(h);
+  if (rc) return rc;
+  if (!h->initialized) return fail(PE_ESTATE, "advance before init");
+  if (!std::isfinite(goal)) return fail(PE_EINVAL, "goal must be finite");
+  int64_t taken = 0;
+  while (h->t < goal - 1e-12) {
+    const double dt = std::min(h->limit, goal - h->t);
+    rc = step_impl(h, dt);
+    if (rc) return rc;
+    taken++;
+  }
+  if (steps_taken) *steps_taken = taken;
+  return PE_OK;
+}
+
+int pe_relative_step(pe_relative *h, double dt) {
+  int rc = enter(h);
+  if (rc) return rc;
+  if (!h->initialized) return fail(PE_ESTATE, "step before init");
+  if (!(dt > 0) || !std::isfinite(dt)) return fail(PE_EINVAL, "dt must be > 0");
+  return step_impl(h, dt);
+}
+
+int pe_relative_time(const pe_relative *h, double *t, int64_t *steps) {
+  if (!h) return fail(PE_EINVAL, "handle is NULL");
+  if (t) *t = h->t;
+  if (steps) *steps = h->steps;
+  return PE_OK;
+}
+
+int pe_relative_synchronize(pe_relative *h) {
+  int rc = enter(h);
+  if (rc) return rc;
+  return read_stats(h);
+}
+
+int pe_relative_copy_field(pe_relative *h, float *host_field) {
+  int rc = enter(h);
+  if (rc) return rc;
+  if (!host_field) return fail(PE_EINVAL, "host_field is NULL");
+  PE_CUDA_TRY(cudaMemcpyAsync(host_field, h->a, sizeof(float) * (size_t)h->g.n,
+                              cudaMemcpyDeviceToHost, h->stream));
+  return read_stats(h);
+}
+
+int pe_relative_copy_arrival(pe_relative *h, float *host_arrival) {
+  int rc = enter(h);
+  if (rc) return rc;
+  if (!host_arrival) return fail(PE_EINVAL, "host_arrival is NULL");
+  PE_CUDA_TRY(cudaMemcpyAsync(host_arrival, h->arrival,
+                              sizeof(float) * (size_t)h->g.n,
+                              cudaMemcpyDeviceToHost, h->stream));
+  return read_stats(h);
+}
+
+int pe_relative_device_field(pe_relative *h, float **device_field) {
+  if (!h || !device_field) return fail(PE_EINVAL, "NULL argument");
+  *device_field = h->a;
+  return PE_OK;
+}
+
+int pe_relative_stats(pe_relative *h, double *residual, double *max_increase) {
+  int rc = enter(h);
+  if (rc) return rc;
+  rc = read_stats(h);
+  if (rc) return rc;
+  double r, inc;
+  std::memcpy(&r, &h->host_stats->residual, sizeof r);
+  std::memcpy(&inc, &h->host_stats->increase, sizeof inc);
+  if (residual) *residual = r;
+  if (max_increase) *max_increase = inc;
+  return PE_OK;
+}
+
+int pe_relative_profile(pe_relative *h, int enable) {
+  int rc = enter(h);
+  if (rc) return rc;
+  rc = drain_profile(h);
+  if (rc) return rc;
+  h->profiling = enable != 0;
+  h->prof_ms[0] = h->prof_ms[1] = 0;
+  h->prof_n[0] = h->prof_n[1] = 0;
+  return PE_OK;
+}
+
+int pe_relative_kernel_time(pe_relative *h, int stage, double *total_ms,
+                            int64_t *launches) {
+  int rc = enter(h);
+  if (rc) return rc;
+  if (stage != 0 && stage != 1) return fail(PE_EINVAL, "stage must be 0 or 1");
+  rc = drain_profile(h);
+  if (rc) return rc;
+  if (total_ms) *total_ms = h->prof_ms[stage];
+  if (launches) *launches = h->prof_n[stage];
+  return PE_OK;
+}
+
+int pe_relative_destroy(pe_relative *h) {
+  if (!h) return PE_OK;
+  cudaSetDevice(h->p.device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  release(h);
+  delete h;
+  return PE_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,130 @@
+"""ctypes binding of libpe_b200.so (the C ABI declared in include/pe_b200.h).
+
+The library is the product path: importing this module fails loudly when the
+shared library is missing (build it with pursuit-evasion-core_b200/build.py);
+there is no CPU fallback.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+LIBRARY_PATH = Path(__file__).resolve().with_name("libpe_b200.so")
+
+PE_OK = 0
+PE_EINVAL = -1
+PE_ENOMEM = -2
+PE_ENONFINITE = -3
+PE_ETIMEOUT = -4
+PE_ECUDA = -5
+PE_ESTATE = -6
+
+PE_LOCAL_F32 = 0
+PE_LOCAL_F64 = 1
+PE_SCHEME_ENO_LF = 0
+
+
+class NativeError(RuntimeError):
+    """A libpe_b200 call failed; `code` is the negative PE_* code."""
+
+    def __init__(self, code, message):
+        super().__init__(f"{message} (code {code})")
+        self.code = code
+
+
+class NonFiniteError(NativeError, FloatingPointError):
+    pass
+
+
+class RelativeParams(ctypes.Structure):
+    _fields_ = [
+        ("positions", ctypes.c_int32),
+        ("headings", ctypes.c_int32),
+        ("p_speeds", ctypes.c_int32),
+        ("e_speeds", ctypes.c_int32),
+        ("extent", ctypes.c_double),
+        ("capture_radius", ctypes.c_double),
+        ("p_speed_min", ctypes.c_double),
+        ("p_speed_max", ctypes.c_double),
+        ("p_acceleration", ctypes.c_double),
+        ("p_curvature", ctypes.c_double),
+        ("e_speed_min", ctypes.c_double),
+        ("e_speed_max", ctypes.c_double),
+        ("e_acceleration", ctypes.c_double),
+        ("e_curvature", ctypes.c_double),
+        ("cfl", ctypes.c_double),
+        ("order", ctypes.c_int32),
+        ("scheme", ctypes.c_int32),
+        ("precision", ctypes.c_int32),
+        ("device", ctypes.c_int32),
+    ]
+
+
+_P = ctypes.c_void_p
+_I64P = ctypes.POINTER(ctypes.c_int64)
+_DP = ctypes.POINTER(ctypes.c_double)
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "pe_version": (ctypes.c_int, []),
+    "pe_last_error": (ctypes.c_char_p, []),
+    "pe_launch_count": (ctypes.c_int64, []),
+    "pe_relative_cells": (ctypes.c_int, [ctypes.POINTER(RelativeParams), _I64P]),
+    "pe_relative_cfl_limit": (ctypes.c_int, [ctypes.POINTER(RelativeParams), _DP]),
+    "pe_relative_create": (
+        ctypes.c_int,
+        [ctypes.POINTER(RelativeParams), ctypes.POINTER(ctypes.c_void_p)],
+    ),
+    "pe_relative_set_stream": (ctypes.c_int, [_P, _P]),
+    "pe_relative_init": (ctypes.c_int, [_P, _P, _P, ctypes.c_double]),
+    "pe_relative_advance": (ctypes.c_int, [_P, ctypes.c_double, _I64P]),
+    "pe_relative_step": (ctypes.c_int, [_P, ctypes.c_double]),
+    "pe_relative_time": (ctypes.c_int, [_P, _DP, _I64P]),
+    "pe_relative_synchronize": (ctypes.c_int, [_P]),
+    "pe_relative_copy_field": (ctypes.c_int, [_P, _P]),
+    "pe_relative_copy_arrival": (ctypes.c_int, [_P, _P]),
+    "pe_relative_device_field": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_void_p)]),
+    "pe_relative_stats": (ctypes.c_int, [_P, _DP, _DP]),
+    "pe_relative_profile": (ctypes.c_int, [_P, ctypes.c_int]),
+    "pe_relative_kernel_time": (ctypes.c_int, [_P, ctypes.c_int, _DP, _I64P]),
+    "pe_relative_destroy": (ctypes.c_int, [_P]),
+}
+
+_lib = None
+
+
+def library():
+    """Load libpe_b200.so once; raise if it is absent."""
+    global _lib
+    if _lib is None:
+        if not LIBRARY_PATH.exists():
+            raise ImportError(
+                f"{LIBRARY_PATH} is missing: build it with "
+                "pursuit-evasion-core_b200/build.py (no CPU fallback exists)"
+            )
+        lib = ctypes.CDLL(str(LIBRARY_PATH))
+        for name, (restype, argtypes) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = restype
+            fn.argtypes = argtypes
+        _lib = lib
+    return _lib
+
+
+def check(code):
+    """Raise the exception matching a PE_* return code."""
+    if code == PE_OK:
+        return
+    message = library().pe_last_error().decode(errors="replace")
+    if code == PE_EINVAL:
+        raise ValueError(message)
+    if code == PE_ENOMEM:
+        raise MemoryError(message)
+    if code == PE_ENONFINITE:
+        raise NonFiniteError(code, message)
+    raise NativeError(code, message)
+
+
+def launch_count():
+    return int(library().pe_launch_count())

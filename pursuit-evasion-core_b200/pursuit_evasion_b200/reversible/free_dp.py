@@ -1,0 +1,403 @@
+"""Drop-in `reversible.free_dp` for B200: the relative 5D capture-tube solve.
+
+Same Python API and the same completed-table directory as pursuit-evasion-core
+src/pursuit_evasion/reversible/free_dp.py:
+    solve(config, grid, output, *, horizon, output_dt, order, cfl, threads,
+          history, max_working_gb, disk_reserve_gb) -> meta dict
+writing meta.json (schema "reversible_relative5d_v1"), fields.f32
+([T, vP, vE, psi, y, x] float32, frame 0 = initial field), final.f32,
+arrival.f32, timing.json, progress.jsonl and solver.log, which the reference's
+RelativeTable (relative_table.py:11-61) reads.  The reference runs a g++/OpenMP
+executable per solve (free_dp.py:259-261); here the per-cell work runs in
+hand-written sm_100a kernels behind libpe_b200.so.
+
+Extra keywords (defaults keep the reference behaviour):
+    local_precision  "float64" (default) reproduces the reference executable
+                     bit for bit; "float32" is the fast path.
+    device           CUDA device ordinal.
+    tol              stop early once a step changes no cell by tol or more
+                     (sup-norm convergence); the last frame is the converged
+                     field and meta records `converged_time`.
+    warm_start       optional initial field (cells float32) replacing the
+                     circular capture field.
+    save_final       write final.f32 / arrival.f32 (default True).
+"""
+
+from __future__ import annotations
+
+from dataclasses import asdict, dataclass
+import hashlib
+import json
+import math
+import os
+from pathlib import Path
+import shutil
+import time
+
+import numpy as np
+
+from .model import config_dict
+from .relative_solver import RelativeSolver
+
+SCHEMA = "reversible_relative5d_v1"
+SOURCE_DIR = Path(__file__).resolve().parents[2] / "csrc"
+
+
+@dataclass(frozen=True)
+class RelativeGrid:
+    """Relative grid [vP, vE, psi, y, x]; same fields and checks as
+    free_dp.py:23-72 (positions >= 3, headings >= 4, speeds >= 3)."""
+
+    positions: int = 41
+    headings: int = 24
+    p_speeds: int = 7
+    e_speeds: int = 7
+    extent: float = 4.0
+
+    def __post_init__(self):
+        minimum = {"positions": 3, "headings": 4, "p_speeds": 3, "e_speeds": 3}
+        for name, low in minimum.items():
+            value = getattr(self, name)
+            if isinstance(value, bool) or int(value) != value or value < low:
+                raise ValueError(f"Invalid {name}: {value}")
+        if not np.isfinite(self.extent) or self.extent <= 0:
+            raise ValueError("extent must be finite and positive")
+
+    @property
+    def shape(self):
+        return (self.p_speeds, self.e_speeds, self.headings, self.positions,
+                self.positions)
+
+    @property
+    def states(self):
+        return math.prod(self.shape)
+
+    def axes(self, config):
+        p, e = config.pursuer, config.evader
+        return (
+            np.linspace(p.speed_min, p.speed_max, self.p_speeds),
+            np.linspace(e.speed_min, e.speed_max, self.e_speeds),
+            np.linspace(-np.pi, np.pi, self.headings, endpoint=False),
+            np.linspace(-self.extent, self.extent, self.positions),
+            np.linspace(-self.extent, self.extent, self.positions),
+        )
+
+    def to_dict(self):
+        return asdict(self)
+
+
+def output_times(horizon, output_dt):
+    """Frame times min(k * output_dt, horizon), k = 0..ceil(h/dt - 1e-10)."""
+    count = math.ceil(horizon / output_dt - 1e-10)
+    return np.minimum(np.arange(count + 1) * output_dt, horizon)
+
+
+def physics_signature(config):
+    """Table-compatibility signature (same keys as free_dp.py:80-96)."""
+    signature = {"capture_radius": float(config.capture_radius)}
+    for role in ("pursuer", "evader"):
+        limits = getattr(config, role)
+        signature[role] = {
+            k: float(getattr(limits, k))
+            for k in ("speed_min", "speed_max", "acceleration", "max_curvature")
+        }
+    if config.capture_rule != "center_distance":
+        signature["capture_rule"] = config.capture_rule
+    return signature
+
+
+def _validate(config, grid, horizon, output_dt, order, cfl, threads):
+    """Option checks of free_dp.py:99-128 (ValueError on any failure)."""
+    numbers = [horizon, output_dt, cfl, config.capture_radius, grid.extent]
+    for limits in (config.pursuer, config.evader):
+        numbers += [limits.speed_min, limits.speed_max, limits.acceleration,
+                    limits.max_curvature]
+        if (limits.speed_min >= limits.speed_max or limits.acceleration <= 0
+                or limits.max_curvature <= 0):
+            raise ValueError("Invalid vehicle limits")
+    if (not np.isfinite(numbers).all() or horizon <= 0 or output_dt <= 0
+            or not 0 < cfl <= 1):
+        raise ValueError("Invalid numeric solve options")
+    if (not 0 < config.capture_radius < grid.extent or order not in (1, 2)
+            or threads < 1):
+        raise ValueError("Invalid radius, order or thread count")
+
+
+def _source_digest():
+    digest = hashlib.sha256()
+    for path in sorted(SOURCE_DIR.glob("relative5d*")) + sorted(
+            SOURCE_DIR.glob("capi_relative.cu")):
+        digest.update(path.read_bytes())
+    return digest.hexdigest()
+
+
+def solve(
+    config,
+    grid,
+    output,
+    *,
+    horizon=2.0,
+    output_dt=0.1,
+    order=2,
+    cfl=0.8,
+    threads=4,
+    history=True,
+    max_working_gb=8.0,
+    disk_reserve_gb=10.0,
+    local_precision="float64",
+    device=0,
+    tol=None,
+    warm_start=None,
+    save_final=True,
+):
+    """Compute a new relative table directory on the GPU.
+
+    Refuses an existing non-empty output (FileExistsError), a working set
+    above max_working_gb (MemoryError, before anything is created) and too
+    little disk (OSError), like free_dp.py:145-176.  `threads` is accepted
+    for signature compatibility and recorded; the GPU does not use it.
+    """
+    solve_started = time.perf_counter()
+    if config.capture_rule != "center_distance":
+        raise ValueError("This legacy free-space solver uses circular capture")
+    _validate(config, grid, horizon, output_dt, order, cfl, threads)
+    if (not np.isfinite([max_working_gb, disk_reserve_gb]).all()
+            or max_working_gb <= 0 or disk_reserve_gb < 0):
+        raise ValueError("Invalid memory/disk guards")
+    if tol is not None and not (np.isfinite(tol) and tol > 0):
+        raise ValueError("tol must be a positive finite number")
+    if local_precision not in ("float32", "float64"):
+        raise ValueError("local_precision must be float32 or float64")
+    output = Path(output).resolve()
+    if output.exists() and any(output.iterdir()):
+        raise FileExistsError(f"Preserve existing output: {output}")
+    times = output_times(horizon, output_dt)
+    N = grid.states
+    working = N * 12
+    storage = N * 4 * ((2 if save_final else 0) + (len(times) if history else 0))
+    if working > max_working_gb * 1e9:
+        raise MemoryError(
+            f"Core arrays need {working / 1e9:.3f} GB, above guard {max_working_gb}"
+        )
+    output.parent.mkdir(parents=True, exist_ok=True)
+    free = shutil.disk_usage(output.parent).free
+    if storage + disk_reserve_gb * 1e9 > free:
+        raise OSError(
+            f"Output needs {storage / 1e9:.3f} GB while retaining "
+            f"{disk_reserve_gb} GB disk reserve"
+        )
+    initial = None
+    if warm_start is not None:
+        initial = np.ascontiguousarray(warm_start, dtype=np.float32).reshape(-1)
+        if initial.size != N or not np.isfinite(initial).all():
+            raise ValueError("warm_start must be a finite field of grid.states cells")
+
+    alloc_started = time.perf_counter()
+    solver = RelativeSolver(config, grid, order=order, cfl=cfl,
+                            local_precision=local_precision, device=device)
+    output.mkdir(exist_ok=True)
+    meta = {"schema": SCHEMA, "status": "running"}
+    try:
+        solver.initialize(initial)
+        allocation_seconds = time.perf_counter() - alloc_started
+        meta.update({
+            "schema": SCHEMA,
+            "backend": "b200_cuda",
+            "local_precision": local_precision,
+            "config": config_dict(config),
+            "physics": physics_signature(config),
+            "grid": grid.to_dict(),
+            "shape": list(grid.shape),
+            "state_order": ["x", "y", "psi", "vP", "vE"],
+            "axis_order": ["vP", "vE", "psi", "y", "x"],
+            "axes": [a.tolist() for a in grid.axes(config)],
+            "horizon": horizon,
+            "output_dt": output_dt,
+            "times": times.tolist(),
+            "order": order,
+            "cfl": cfl,
+            "threads": threads,
+            "history_saved": bool(history),
+            "dtype": "float32",
+            "target": "physical_capture_only",
+            "avoid": None,
+            "tube_projection": "min over every internal update",
+            "position_boundary":
+                "one-sided linear extrapolation; outside queries unresolved",
+            "speed_boundary":
+                "acceleration restricted to inward or zero at speed limits",
+            "heading_boundary": "periodic",
+            "source_sha256": _source_digest(),
+            "source_file": None,
+            "compile_seconds": 0.0,
+            "warm_start": warm_start is not None,
+            "tol": tol,
+            "cfl_dt_limit": solver.cfl_dt_limit,
+            "predicted_working_bytes": working,
+            "predicted_output_bytes": storage,
+            "device": int(device),
+            "status": "running",
+        })
+        (output / "meta.json").write_text(json.dumps(meta, indent=2) + "\n")
+        meta.update(_run(solver, output, times, history=history, tol=tol,
+                         save_final=save_final))
+        meta["allocation_seconds"] = allocation_seconds
+        meta["status"] = "complete"
+        if meta["frames"] != len(meta["times"]):
+            meta["status"] = "failed"
+            meta["failure"] = "Output time count mismatch"
+    except Exception as exc:
+        meta.update(status="failed", failure=str(exc))
+        (output / "meta.json").write_text(json.dumps(meta, indent=2) + "\n")
+        raise RuntimeError(f"Relative solve failed: {exc}") from exc
+    finally:
+        solver.close()
+    meta["total_wall_seconds"] = time.perf_counter() - solve_started
+    (output / "meta.json").write_text(json.dumps(meta, indent=2) + "\n")
+    if meta["status"] != "complete":
+        raise RuntimeError(f"Relative solve failed: {output / 'solver.log'}")
+    return meta
+
+
+def _run(solver, output, times, *, history, tol, save_final):
+    """Frame loop: advance to each output time, save the frame, log progress."""
+    N = solver.cells
+    host = np.empty(N, np.float32)
+    write_seconds = update_seconds = transfer_seconds = 0.0
+    frames = 1
+    converged_time = None
+    kept_times = [float(times[0])]
+    history_file = (output / "fields.f32").open("wb") if history else None
+    log = (output / "solver.log").open("w")
+    progress = (output / "progress.jsonl").open("w")
+    started = time.perf_counter()
+    try:
+        if history_file:
+            t0 = time.perf_counter()
+            solver.field(host)
+            transfer_seconds += time.perf_counter() - t0
+            t0 = time.perf_counter()
+            host.tofile(history_file)
+            write_seconds += time.perf_counter() - t0
+        for index, goal in enumerate(times[1:], start=1):
+            t0 = time.perf_counter()
+            if tol is None:
+                solver.advance(goal)
+                solver.synchronize()
+            else:
+                converged_time = _advance_until(solver, goal, tol)
+            update_seconds += time.perf_counter() - t0
+            frames += 1
+            kept_times.append(float(solver.time if converged_time else goal))
+            if history_file:
+                t0 = time.perf_counter()
+                solver.field(host)
+                transfer_seconds += time.perf_counter() - t0
+                t0 = time.perf_counter()
+                host.tofile(history_file)
+                write_seconds += time.perf_counter() - t0
+            if index % 5 == 0 or index == len(times) - 1 or converged_time:
+                resolved = int(np.isfinite(solver.arrival()).sum())
+                row = dict(time=kept_times[-1], steps=solver.steps,
+                           resolved=resolved,
+                           elapsed_seconds=time.perf_counter() - started)
+                progress.write(json.dumps(row) + "\n")
+                progress.flush()
+                log.write(f"budget={row['time']} steps={row['steps']} "
+                          f"resolved={resolved} elapsed={row['elapsed_seconds']}\n")
+                log.flush()
+            if converged_time is not None:
+                break
+    finally:
+        if history_file:
+            history_file.close()
+        log.close()
+        progress.close()
+    final_write = 0.0
+    if save_final:
+        t0 = time.perf_counter()
+        solver.field(host).tofile(output / "final.f32")
+        solver.arrival(host).tofile(output / "arrival.f32")
+        final_write = time.perf_counter() - t0
+    residual, increase = solver.stats()
+    timing = {
+        "states": N,
+        "working_array_bytes": 12 * N,
+        "cfl_dt_limit": solver.cfl_dt_limit,
+        "internal_steps": solver.steps,
+        "frames": frames,
+        "update_seconds": update_seconds,
+        "device_to_host_seconds": transfer_seconds,
+        "history_write_seconds": write_seconds,
+        "final_write_seconds": final_write,
+        "elapsed_seconds": time.perf_counter() - started,
+        "maximum_increase": increase,
+        "last_step_residual": residual,
+        "cell_backups_per_second":
+            N * solver.steps * (2 if _order(solver) == 2 else 1)
+            / max(update_seconds, 1e-12),
+    }
+    (output / "timing.json").write_text(json.dumps(timing) + "\n")
+    result = dict(timing)
+    result["times"] = kept_times
+    if converged_time is not None:
+        result["converged_time"] = converged_time
+    return result
+
+
+def _order(solver):
+    return solver._params.order
+
+
+def _advance_until(solver, goal, tol):
+    """Step toward `goal`; return the time at which a step's sup-norm change
+    fell below tol, or None if it did not before `goal`."""
+    limit = solver.cfl_dt_limit
+    while solver.time < goal - 1e-12:
+        solver.step(min(limit, goal - solver.time))
+        residual, _ = solver.stats()
+        if residual < tol:
+            return solver.time
+    return None
+
+
+def main():
+    import argparse
+    from .model import ReversibleConfig
+
+    parser = argparse.ArgumentParser(description=__doc__)
+    parser.add_argument("output")
+    parser.add_argument("--config")
+    parser.add_argument("--positions", type=int, default=41)
+    parser.add_argument("--headings", type=int, default=24)
+    parser.add_argument("--p-speeds", type=int, default=7)
+    parser.add_argument("--e-speeds", type=int, default=7)
+    parser.add_argument("--extent", type=float, default=4)
+    parser.add_argument("--horizon", type=float, default=2)
+    parser.add_argument("--output-dt", type=float, default=0.1)
+    parser.add_argument("--threads", type=int, default=4)
+    parser.add_argument("--order", type=int, choices=[1, 2], default=2)
+    parser.add_argument("--no-history", action="store_true")
+    parser.add_argument("--max-working-gb", type=float, default=8)
+    parser.add_argument("--local-precision", choices=["float32", "float64"],
+                        default="float64")
+    parser.add_argument("--tol", type=float)
+    args = parser.parse_args()
+    config = (
+        ReversibleConfig.from_dict(json.loads(Path(args.config).read_text()))
+        if args.config else ReversibleConfig()
+    )
+    grid = RelativeGrid(args.positions, args.headings, args.p_speeds,
+                        args.e_speeds, args.extent)
+    result = solve(config, grid, args.output, horizon=args.horizon,
+                   output_dt=args.output_dt, threads=args.threads,
+                   order=args.order, history=not args.no_history,
+                   max_working_gb=args.max_working_gb,
+                   local_precision=args.local_precision, tol=args.tol)
+    print(json.dumps({k: result[k] for k in
+                      ("status", "states", "update_seconds",
+                       "cell_backups_per_second")}, indent=2))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,193 @@
+"""ctypes access to the CPU oracle (oracle/_build/liboracle.so) and to the
+reference executables built from the reference sources (oracle/_ref/).
+
+Test infrastructure only: the checker the CUDA path is compared against.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import json
+from pathlib import Path
+import subprocess
+import tempfile
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parents[1]
+ORACLE_DIR = REPO / "oracle"
+ORACLE_LIB = ORACLE_DIR / "_build" / "liboracle.so"
+REF_RELATIVE = ORACLE_DIR / "_ref" / "relative5d"
+REF_WORLD = ORACLE_DIR / "_ref" / "reversible_world8d"
+
+
+class RelCfg(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int) for n in ("nx", "nh", "nvp", "nve", "order")] + [
+        (n, ctypes.c_double)
+        for n in ("extent", "radius", "vp_lo", "vp_hi", "ve_lo", "ve_hi",
+                  "acc_p", "acc_e", "curv_p", "curv_e", "cfl")
+    ]
+
+
+class W8Cfg(ctypes.Structure):
+    _fields_ = [
+        (n, ctypes.c_int)
+        for n in ("n", "nh", "np", "ne", "order", "linear_speed", "avoid_square")
+    ] + [
+        (n, ctypes.c_float)
+        for n in ("extent", "arena", "radius", "p_lo", "p_hi", "e_lo", "e_hi",
+                  "ap", "ae", "kp", "ke")
+    ] + [("cfl", ctypes.c_double)]
+
+
+_P = ctypes.c_void_p
+
+
+def _build():
+    subprocess.run(["make", "-s", "-C", str(ORACLE_DIR)], check=True)
+
+
+class Oracle:
+    def __init__(self, lib):
+        self.lib = lib
+        sig = {
+            "po_rel_cells": (ctypes.c_size_t, [_P]),
+            "po_rel_cfl_limit": (ctypes.c_double, [_P]),
+            "po_rel_init": (None, [_P, _P, _P]),
+            "po_rel_init_f64": (None, [_P, _P]),
+            "po_rel_stage_f32": (ctypes.c_int, [_P, _P, _P, _P, ctypes.c_double,
+                                                ctypes.c_double, ctypes.c_int, _P]),
+            "po_rel_stage_f64": (ctypes.c_int, [_P, _P, _P, ctypes.c_double,
+                                                ctypes.c_int]),
+            "po_rel_solve_f32": (ctypes.c_int, [_P, ctypes.c_double,
+                                                ctypes.c_double, _P, _P, _P]),
+            "po_rel_solve_f64": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_double,
+                                                _P, _P]),
+            "po_w8_cells": (ctypes.c_size_t, [_P]),
+            "po_w8_dt_limit": (ctypes.c_double, [_P]),
+            "po_w8_init_square": (None, [_P, _P, _P]),
+            "po_rect_separation": (ctypes.c_double, [ctypes.c_double] * 10),
+            "po_w8_init_contact": (None, [_P] + [ctypes.c_double] * 4 + [_P, _P]),
+            "po_w8_stage": (ctypes.c_int, [_P, _P, _P, _P, _P, ctypes.c_float,
+                                           ctypes.c_double]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+
+    # -- relative 5D ---------------------------------------------------------
+    @staticmethod
+    def rel_cfg(config, grid, order=2, cfl=0.8):
+        p, e = config.pursuer, config.evader
+        return RelCfg(grid.positions, grid.headings, grid.p_speeds,
+                      grid.e_speeds, order, grid.extent, config.capture_radius,
+                      p.speed_min, p.speed_max, e.speed_min, e.speed_max,
+                      p.acceleration, e.acceleration, p.max_curvature,
+                      e.max_curvature, cfl)
+
+    def rel_cfl_limit(self, cfg):
+        return self.lib.po_rel_cfl_limit(ctypes.addressof(cfg))
+
+    def rel_solve_f32(self, cfg, horizon, output_dt):
+        """Frames [T, N] and arrival of the reference executable's solve."""
+        n = self.lib.po_rel_cells(ctypes.addressof(cfg))
+        count = int(np.ceil(horizon / output_dt - 1e-10)) + 1
+        frames = np.zeros((count, n), np.float32)
+        arrival = np.zeros(n, np.float32)
+        steps = ctypes.c_long()
+        rc = self.lib.po_rel_solve_f32(ctypes.addressof(cfg), horizon, output_dt,
+                                       frames.ctypes.data, arrival.ctypes.data,
+                                       ctypes.addressof(steps))
+        assert rc == 0, rc
+        return frames, arrival, steps.value
+
+    def rel_solve_f64(self, cfg, horizon, output_dt):
+        """Final field of the same step sequence with double storage."""
+        n = self.lib.po_rel_cells(ctypes.addressof(cfg))
+        final = np.zeros(n, np.float64)
+        steps = ctypes.c_long()
+        rc = self.lib.po_rel_solve_f64(ctypes.addressof(cfg), horizon, output_dt,
+                                       final.ctypes.data, ctypes.addressof(steps))
+        assert rc == 0, rc
+        return final, steps.value
+
+    def rel_stage_f32(self, cfg, src, dst, arrival, dt, t, blend):
+        inc = ctypes.c_double()
+        rc = self.lib.po_rel_stage_f32(ctypes.addressof(cfg), src.ctypes.data,
+                                       dst.ctypes.data,
+                                       None if arrival is None else arrival.ctypes.data,
+                                       dt, t, blend, ctypes.addressof(inc))
+        return rc, inc.value
+
+    # -- dense 8D ------------------------------------------------------------
+    def w8_cells(self, cfg):
+        return self.lib.po_w8_cells(ctypes.addressof(cfg))
+
+    def w8_dt_limit(self, cfg):
+        return self.lib.po_w8_dt_limit(ctypes.addressof(cfg))
+
+    def w8_init_square(self, cfg):
+        n = self.w8_cells(cfg)
+        a = np.zeros(n, np.float32)
+        arr = np.zeros(n, np.float32)
+        self.lib.po_w8_init_square(ctypes.addressof(cfg), a.ctypes.data,
+                                   arr.ctypes.data)
+        return a, arr
+
+    def w8_init_contact(self, cfg, p_body, e_body):
+        n = self.w8_cells(cfg)
+        a = np.zeros(n, np.float32)
+        arr = np.zeros(n, np.float32)
+        self.lib.po_w8_init_contact(ctypes.addressof(cfg), p_body[0], p_body[1],
+                                    e_body[0], e_body[1], a.ctypes.data,
+                                    arr.ctypes.data)
+        return a, arr
+
+    def w8_stage(self, cfg, src, dst, base, arrival, dt, tau):
+        return self.lib.po_w8_stage(ctypes.addressof(cfg), src.ctypes.data,
+                                    dst.ctypes.data,
+                                    None if base is None else base.ctypes.data,
+                                    None if arrival is None else arrival.ctypes.data,
+                                    dt, tau)
+
+    def rect_separation(self, p, e, p_body, e_body):
+        return self.lib.po_rect_separation(p[0], p[1], p[2], e[0], e[1], e[2],
+                                           p_body[0], p_body[1], e_body[0],
+                                           e_body[1])
+
+
+_oracle = None
+
+
+def load():
+    global _oracle
+    if _oracle is None:
+        if not ORACLE_LIB.exists():
+            _build()
+        _oracle = Oracle(ctypes.CDLL(str(ORACLE_LIB)))
+    return _oracle
+
+
+def run_reference_relative(config, grid, *, horizon, output_dt, order=2,
+                           cfl=0.8, threads=4, history=True):
+    """Run the reference executable (built from native_relative.cpp) with the
+    argv free_dp.solve would pass (free_dp.py:198-224); returns its output
+    folder.  Requires oracle/_ref/relative5d."""
+    p, e = config.pursuer, config.evader
+    folder = Path(tempfile.mkdtemp(prefix="pe_ref_"))
+    options = {
+        "positions": grid.positions, "headings": grid.headings,
+        "p-speeds": grid.p_speeds, "e-speeds": grid.e_speeds,
+        "extent": grid.extent, "radius": config.capture_radius,
+        "p-min": p.speed_min, "p-max": p.speed_max,
+        "e-min": e.speed_min, "e-max": e.speed_max,
+        "p-acceleration": p.acceleration, "e-acceleration": e.acceleration,
+        "p-curvature": p.max_curvature, "e-curvature": e.max_curvature,
+        "horizon": horizon, "output-dt": output_dt, "order": order, "cfl": cfl,
+        "threads": threads, "history": int(history), "output": str(folder),
+    }
+    cmd = [str(REF_RELATIVE)] + [str(x) for k, v in options.items()
+                                 for x in ("--" + k, v)]
+    subprocess.run(cmd, check=True, capture_output=True)
+    return folder, json.loads((folder / "timing.json").read_text())
