@@ -5,7 +5,8 @@
 Workload (the 89M-cell table): RelativeGrid(65, 48, 21, 21, 8.0) — 65 x 65
 relative positions on [-8, 8] m, 48 headings, 21 x 21 speed levels —
 reversible_free_a3 physics (both accelerations 3 m/s^2), CFL 0.8, horizon
-3.0 s = 900 RK2 steps = 1800 stage launches.  Values and local arithmetic are
+3.0 s in 0.1-s frames = 900 RK2 steps = 1800 stage launches (the step
+sequence of the reference driver, native_relative.cpp:173-190).  Values and local arithmetic are
 float32 (the fast path).  One bench step = one full solve to the horizon:
 initialise the capture field, advance 900 steps.
 
@@ -47,6 +48,7 @@ sys.path.insert(0, str(REPO))
 
 GRID = dict(positions=65, headings=48, p_speeds=21, e_speeds=21, extent=8.0)
 HORIZON = 3.0
+OUTPUT_DT = 0.1  # frame boundaries split the steps as in the reference driver
 METRIC = "cell-backups/s"
 REF_EXE = REPO / "oracle" / "_ref" / "relative5d"
 ORACLE_LIB = REPO / "oracle" / "_build" / "liboracle.so"
@@ -293,9 +295,19 @@ def run_ours(args, world, rank, local):
         if world > 1:
             torch.distributed.barrier()
 
+    from pursuit_evasion_b200.reversible.free_dp import output_times
+
+    frame_times = output_times(HORIZON, OUTPUT_DT)[1:]
+
+    def advance_all():
+        taken = 0
+        for goal in frame_times:
+            taken += solver.advance(goal)
+        return taken
+
     def one_solve():
         solver.initialize()
-        return solver.advance(HORIZON)
+        return advance_all()
 
     for _ in range(args.warmup):
         steps = one_solve()
@@ -332,7 +344,7 @@ def run_ours(args, world, rank, local):
     e_start.record(stream)
     for _ in range(args.steps):
         solver.initialize(init_np)
-        solver.advance(HORIZON)
+        advance_all()
         solver.copy_field_to(host_field.data_ptr())
         solver._lib.pe_relative_copy_arrival(solver._h, host_arrival.data_ptr())
     e_end.record(stream)

@@ -112,9 +112,11 @@ int pe_relative_synchronize(pe_relative *h);
 int pe_relative_copy_field(pe_relative *h, float *host_field);
 int pe_relative_copy_arrival(pe_relative *h, float *host_arrival);
 
-/* Device address of the current field (cells floats, storage order
- * [vP, vE, psi, y, x]); valid until the next step or destroy. */
+/* Device address of the current field: storage order [vP, vE, psi, y, x]
+ * with every x row padded to pe_relative_row_pitch() floats (pad = 0);
+ * valid until the next step or destroy. */
 int pe_relative_device_field(pe_relative *h, float **device_field);
+int pe_relative_row_pitch(const pe_relative *h, int32_t *floats);
 
 /* Sup-norm change max|V_new - V_old| of the most recent step, reduced in
  * double, and the largest increase of any cell since init (the reference's

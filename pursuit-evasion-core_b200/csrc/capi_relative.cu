@@ -14,6 +14,7 @@
 struct pe_relative {
   pe_relative_params p{};
   pe::Rel5Grid g{};
+  pe::Rel5Tile tile{};
   double limit = 0;
   float *a = nullptr, *b = nullptr, *arrival = nullptr, *plane = nullptr;
   double *sn = nullptr, *cs = nullptr;
@@ -80,11 +81,13 @@ pe::Rel5Grid make_grid(const pe_relative_params *p) {
   g.nvp = p->p_speeds;
   g.nve = p->e_speeds;
   g.order = p->order;
-  g.sy = g.nx;
-  g.sp = (int64_t)g.nx * g.nx;
+  g.xp = (g.nx + 3) / 4 * 4;  // rows padded to 16 bytes
+  g.sy = g.xp;
+  g.sp = (int64_t)g.nx * g.xp;
   g.se = g.sp * g.nh;
   g.sv = g.se * g.nve;
-  g.n = g.sv * g.nvp;
+  g.n_padded = g.sv * g.nvp;
+  g.n = (int64_t)g.nx * g.nx * g.nh * g.nve * g.nvp;
   g.extent = p->extent;
   g.dx = 2 * p->extent / (p->positions - 1);
   g.dphi = 2 * pi / p->headings;
@@ -176,9 +179,10 @@ int launch_stage(pe_relative *h, int stage, const float *src, float *dst,
     e1 = take_event(h);
     PE_CUDA_TRY(cudaEventRecord(e0, h->stream));
   }
-  const cudaError_t err = h->p.precision == PE_LOCAL_F64
-                              ? pe::rel5_stage_f64(h->g, s, blend, h->stream)
-                              : pe::rel5_stage_f32(h->g, s, blend, h->stream);
+  const cudaError_t err =
+      h->p.precision == PE_LOCAL_F64
+          ? pe::rel5_stage_f64(h->g, s, blend, h->stream)
+          : pe::rel5_stage_f32(h->g, h->tile, s, blend, h->stream);
   if (err != cudaSuccess) return pe::cuda_fail(err, "relative stage launch");
   pe::count_launches(1);
   if (h->profiling) {
@@ -212,6 +216,8 @@ int read_stats(pe_relative *h) {
   PE_CUDA_TRY(cudaMemcpyAsync(h->host_stats, h->stats, sizeof(pe::Rel5Stats),
                               cudaMemcpyDeviceToHost, h->stream));
   PE_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  if (h->host_stats->timeout)
+    return fail(PE_ETIMEOUT, "a bounded device wait gave up");
   if (h->host_stats->nonfinite)
     return fail(PE_ENONFINITE, "Nonfinite field update");
   return PE_OK;
@@ -253,7 +259,8 @@ int pe_relative_create(const pe_relative_params *params, pe_relative **out) {
   h->p = *params;
   h->g = make_grid(params);
   h->limit = cfl_limit(params, h->g);
-  const size_t bytes = sizeof(float) * (size_t)h->g.n;
+  h->tile = pe::rel5_default_tile(h->g);
+  const size_t bytes = sizeof(float) * (size_t)h->g.n_padded;
   const int nh = h->g.nh;
   std::vector<double> sn(nh), cs(nh);
   std::vector<float> snf(nh), csf(nh);
@@ -311,7 +318,7 @@ int pe_relative_init(pe_relative *h, const float *initial,
   if (rc) return rc;
   if (!std::isfinite(start_time) || start_time < 0)
     return fail(PE_EINVAL, "start_time must be finite and >= 0");
-  const size_t bytes = sizeof(float) * (size_t)h->g.n;
+  const size_t bytes = sizeof(float) * (size_t)h->g.n;  // dense host field
   PE_CUDA_TRY(cudaMemsetAsync(h->stats, 0, sizeof(pe::Rel5Stats), h->stream));
   if (!initial) {
     // The circular capture field of native_relative.cpp:91-100, one (y, x)
@@ -332,11 +339,18 @@ int pe_relative_init(pe_relative *h, const float *initial,
     pe::count_launches(1);
     PE_CUDA_TRY(cudaStreamSynchronize(h->stream));
   } else {
-    PE_CUDA_TRY(cudaMemcpyAsync(h->a, initial, bytes, cudaMemcpyHostToDevice,
+    // Dense host field -> stage buffer -> padded field.
+    PE_CUDA_TRY(cudaMemcpyAsync(h->b, initial, bytes, cudaMemcpyHostToDevice,
                                 h->stream));
+    PE_CUDA_TRY(pe::rel5_unpack(h->g, h->b, h->a, h->stream));
+    pe::count_launches(1);
     if (arrival) {
-      PE_CUDA_TRY(cudaMemcpyAsync(h->arrival, arrival, bytes,
-                                  cudaMemcpyHostToDevice, h->stream));
+      PE_CUDA_TRY(pe::rel5_init(h->g, nullptr, h->a, h->arrival,
+                                (float)start_time, h->stream));
+      PE_CUDA_TRY(cudaMemcpyAsync(h->b, arrival, bytes, cudaMemcpyHostToDevice,
+                                  h->stream));
+      PE_CUDA_TRY(pe::rel5_unpack(h->g, h->b, h->arrival, h->stream));
+      pe::count_launches(2);
     } else {
       PE_CUDA_TRY(pe::rel5_init(h->g, nullptr, h->a, h->arrival,
                                 (float)start_time, h->stream));
@@ -391,7 +405,11 @@ int pe_relative_copy_field(pe_relative *h, float *host_field) {
   int rc = enter(h);
   if (rc) return rc;
   if (!host_field) return fail(PE_EINVAL, "host_field is NULL");
-  PE_CUDA_TRY(cudaMemcpyAsync(host_field, h->a, sizeof(float) * (size_t)h->g.n,
+  // Padded field -> dense stage buffer -> host (the stage buffer is free
+  // between steps).
+  PE_CUDA_TRY(pe::rel5_pack(h->g, h->a, h->b, h->stream));
+  pe::count_launches(1);
+  PE_CUDA_TRY(cudaMemcpyAsync(host_field, h->b, sizeof(float) * (size_t)h->g.n,
                               cudaMemcpyDeviceToHost, h->stream));
   return read_stats(h);
 }
@@ -400,8 +418,9 @@ int pe_relative_copy_arrival(pe_relative *h, float *host_arrival) {
   int rc = enter(h);
   if (rc) return rc;
   if (!host_arrival) return fail(PE_EINVAL, "host_arrival is NULL");
-  PE_CUDA_TRY(cudaMemcpyAsync(host_arrival, h->arrival,
-                              sizeof(float) * (size_t)h->g.n,
+  PE_CUDA_TRY(pe::rel5_pack(h->g, h->arrival, h->b, h->stream));
+  pe::count_launches(1);
+  PE_CUDA_TRY(cudaMemcpyAsync(host_arrival, h->b, sizeof(float) * (size_t)h->g.n,
                               cudaMemcpyDeviceToHost, h->stream));
   return read_stats(h);
 }
@@ -409,6 +428,12 @@ int pe_relative_copy_arrival(pe_relative *h, float *host_arrival) {
 int pe_relative_device_field(pe_relative *h, float **device_field) {
   if (!h || !device_field) return fail(PE_EINVAL, "NULL argument");
   *device_field = h->a;
+  return PE_OK;
+}
+
+int pe_relative_row_pitch(const pe_relative *h, int32_t *floats) {
+  if (!h || !floats) return fail(PE_EINVAL, "NULL argument");
+  *floats = h->g.xp;
   return PE_OK;
 }
 

@@ -1,8 +1,13 @@
 // Relative 5D ENO/Lax-Friedrichs capture-tube kernels: shared declarations.
 //
-// Storage order [vP, vE, psi, y, x], x fastest (the reference's fields.f32
-// frame layout, free_dp.py:45-54).  One launch = one stage of the RK1/RK2
-// update of native_relative.cpp:124-172 over every cell.
+// Device layout: the reference's storage order [vP, vE, psi, y, x]
+// (free_dp.py:45-54) with every x row padded to `xp` floats (a multiple of 4)
+// so that rows, planes and 4-cell chunks are 16-byte aligned for bulk async
+// copies and vector loads.  Pad lanes hold 0.  Host copies convert between
+// this pitched layout and the dense table layout.
+//
+// One stage launch = one stage of the RK1/RK2 update of
+// native_relative.cpp:124-172 over every cell.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -12,8 +17,10 @@ namespace pe {
 
 struct Rel5Grid {
   int nx, nh, nvp, nve, order;
-  int64_t n;               // cells
-  int64_t sy, sp, se, sv;  // strides of y, psi, vE, vP (x stride is 1)
+  int xp;                  // padded row length (floats), multiple of 4
+  int64_t n;               // cells (dense)
+  int64_t n_padded;        // floats of one padded field
+  int64_t sy, sp, se, sv;  // padded strides of y, psi, vE, vP (x stride 1)
   double extent, dx, dphi, dvp, dve;
   double vp_lo, ve_lo, acc_p, acc_e, curv_p, curv_e;
 };
@@ -23,34 +30,54 @@ struct Rel5Stats {
   unsigned long long residual;  // bits of a non-negative double
   unsigned long long increase;  // bits of a non-negative double
   unsigned int nonfinite;       // set when an update is not finite
-  unsigned int pad;
+  unsigned int timeout;         // set when a bounded device wait gave up
 };
 
 struct Rel5Stage {
   const float *src;  // stage input
   float *dst;        // stage output (stage 2: also holds the step's old V)
-  float *arrival;    // first-crossing time, NaN until the cell enters
+  float *arrival;    // first-crossing time, NaN until the cell enters (padded)
   const double *sn, *cs;   // sin/cos of the heading axis, double
   const float *snf, *csf;  // the same, rounded to float
   double dt, t;            // step size and the step's start time
   Rel5Stats *stats;
 };
 
+// Tiling of the fast stage kernel: a CTA owns `rows` y-rows of one (vP, vE)
+// plane stack and sweeps `psi_chunk` consecutive headings.
+struct Rel5Tile {
+  int rows;       // y rows per CTA
+  int psi_chunk;  // headings per CTA
+};
+
+// Shared memory the fast kernel needs for a tile.
+size_t rel5_fast_smem_bytes(const Rel5Grid &g, const Rel5Tile &t);
+
+// Default tile for a grid (rows chosen so rows * xp/4 threads ~ 256).
+Rel5Tile rel5_default_tile(const Rel5Grid &g);
+
 // Fast path: float32 local arithmetic.  blend = 0 for stage 1 (or the only
 // stage of RK1), 1 for the RK2 averaging stage.
-cudaError_t rel5_stage_f32(const Rel5Grid &g, const Rel5Stage &s, int blend,
-                           cudaStream_t stream);
+cudaError_t rel5_stage_f32(const Rel5Grid &g, const Rel5Tile &t,
+                           const Rel5Stage &s, int blend, cudaStream_t stream);
 
 // Exact path: double local arithmetic in the reference's operation order,
 // built without contraction so it reproduces native_relative.cpp bit for bit.
 cudaError_t rel5_stage_f64(const Rel5Grid &g, const Rel5Stage &s, int blend,
                            cudaStream_t stream);
 
-// Broadcast a (y, x) plane of initial values over every (vP, vE, psi) and set
-// arrival = start_time where the value is <= 0, NaN elsewhere.  With
-// plane == nullptr the field is taken as already filled and only arrival is
-// set.
+// Broadcast a (y, x) plane of initial values (dense, nx*nx) over every
+// (vP, vE, psi), zero the row padding, and set arrival = start_time where the
+// value is <= 0, NaN elsewhere.  With plane == nullptr the field is taken as
+// already filled and only arrival (and the padding) is set.
 cudaError_t rel5_init(const Rel5Grid &g, const float *plane, float *field,
                       float *arrival, float start_time, cudaStream_t stream);
+
+// Convert one field between the padded device layout and the dense table
+// layout (device to device).
+cudaError_t rel5_pack(const Rel5Grid &g, const float *padded, float *dense,
+                      cudaStream_t stream);
+cudaError_t rel5_unpack(const Rel5Grid &g, const float *dense, float *padded,
+                        cudaStream_t stream);
 
 }  // namespace pe

@@ -85,6 +85,7 @@ SIGNATURES = {
     "pe_relative_copy_field": (ctypes.c_int, [_P, _P]),
     "pe_relative_copy_arrival": (ctypes.c_int, [_P, _P]),
     "pe_relative_device_field": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_void_p)]),
+    "pe_relative_row_pitch": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int32)]),
     "pe_relative_stats": (ctypes.c_int, [_P, _DP, _DP]),
     "pe_relative_profile": (ctypes.c_int, [_P, ctypes.c_int]),
     "pe_relative_kernel_time": (ctypes.c_int, [_P, ctypes.c_int, _DP, _I64P]),
