@@ -118,6 +118,20 @@ int pe_relative_copy_arrival(pe_relative *h, float *host_arrival);
 int pe_relative_device_field(pe_relative *h, float **device_field);
 int pe_relative_row_pitch(const pe_relative *h, int32_t *floats);
 
+/* Tile shape of the float32 stage kernel: a CTA owns `rows` y rows of one
+ * (vP, vE) pair and sweeps `psi_chunk` headings.  (0, 0) restores the
+ * default; shapes that exceed the kernel's thread or shared-memory limits
+ * are rejected with PE_EINVAL.  Results do not depend on the tile. */
+int pe_relative_set_tile(pe_relative *h, int32_t rows, int32_t psi_chunk);
+int pe_relative_get_tile(const pe_relative *h, int32_t *rows,
+                         int32_t *psi_chunk);
+
+/* Launch shape of the float32 stage kernel for the handle's tile: threads
+ * per CTA, dynamic shared memory per CTA, and CTAs resident per SM at the
+ * most recent launch (0 before the first). */
+int pe_relative_kernel_info(const pe_relative *h, int32_t *threads,
+                            int32_t *smem_bytes, int32_t *resident_ctas);
+
 /* Sup-norm change max|V_new - V_old| of the most recent step, reduced in
  * double, and the largest increase of any cell since init (the reference's
  * maximum_increase diagnostic, native_relative.cpp:166, :233).  Synchronises. */
@@ -132,6 +146,59 @@ int pe_relative_kernel_time(pe_relative *h, int stage, double *total_ms,
 
 /* Release device memory and the handle. */
 int pe_relative_destroy(pe_relative *h);
+
+/* ------------------------------------------------------------------------
+ * Dense 8D game [xP, yP, thP, vP, xE, yE, thE, vE] (vE fastest).
+ *
+ * Replaces the reference executable native_world.cpp (argv options
+ * :76-110, surfaces :155-176, stage :261-314, frame loop :315-336) run by
+ * reversible/world_dp.py:361-372, and the CuPy kernels `init`/`advance` of
+ * reversible/gpu_map_game.py:43-75 (without obstacle clearance grids).
+ * Arithmetic is float32 in the reference's order and reproduces the
+ * executable bit for bit.
+ * ------------------------------------------------------------------------ */
+typedef struct pe_world_params {
+  int32_t positions, headings, p_speeds, e_speeds; /* WorldGrid */
+  double extent;         /* --extent */
+  double arena;          /* --arena (square half width; avoid_mode 1) */
+  double capture_radius; /* --radius (square surfaces init) */
+  double p_speed_min, p_speed_max, p_acceleration, p_curvature;
+  double e_speed_min, e_speed_max, e_acceleration, e_curvature;
+  double cfl;                    /* --cfl */
+  int32_t order;                 /* --order, 1 or 2 */
+  int32_t linear_speed_boundary; /* --linear-speed-boundary */
+  int32_t avoid_mode;            /* 0: none; 1: max(|xP|,|yP|) - arena + 1e-6 */
+  int32_t device;
+} pe_world_params;
+
+typedef struct pe_world pe_world;
+
+int pe_world_cells(const pe_world_params *params, int64_t *cells);
+/* dt bound of native_world.cpp:133-135. */
+int pe_world_dt_limit(const pe_world_params *params, double *dt);
+int pe_world_create(const pe_world_params *params, pe_world **out);
+/* Capture field: oriented-rectangle contact value (separating axes, double,
+ * local_game/geometry.py:15-36) of the two footprints at every grid pose;
+ * arrival 0 where <= 0. */
+int pe_world_init_contact(pe_world *h, double p_length, double p_width,
+                          double e_length, double e_width);
+/* The reference's square-arena surfaces (native_world.cpp:155-176). */
+int pe_world_init_square(pe_world *h);
+/* A host field (continuation, native_world.cpp:177-191). */
+int pe_world_init_field(pe_world *h, const float *field, const float *arrival,
+                        double start_time);
+int pe_world_advance(pe_world *h, double goal, int64_t *steps_taken);
+int pe_world_step(pe_world *h, double dt);
+int pe_world_time(const pe_world *h, double *t, int64_t *steps);
+int pe_world_synchronize(pe_world *h);
+int pe_world_copy_field(pe_world *h, float *host_field);
+int pe_world_copy_arrival(pe_world *h, float *host_arrival);
+/* max |V_new - V_old| of the most recent step. */
+int pe_world_residual(pe_world *h, double *residual);
+int pe_world_set_stream(pe_world *h, void *cuda_stream);
+int pe_world_profile(pe_world *h, int enable);
+int pe_world_kernel_time(pe_world *h, double *total_ms, int64_t *launches);
+int pe_world_destroy(pe_world *h);
 
 #ifdef __cplusplus
 }

@@ -53,4 +53,22 @@ void po_w8_init_contact(const po_w8_cfg *c, double p_len, double p_wid,
 int po_w8_stage(const po_w8_cfg *c, const float *src, float *dst,
                 const float *base, float *arrival, float dt, double tau);
 
+/* Relative 5D semi-Lagrangian backup (FP64). */
+#define PO_SL_TUBE 0
+#define PO_SL_MINTIME 1
+typedef struct {
+  int nx, nh, nvp, nve, mode;
+  double extent, radius, vp_lo, vp_hi, ve_lo, ve_hi, acc_p, acc_e, curv_p,
+      curv_e, dt;
+} po_sl_cfg;
+
+void po_sl_integrated_speed(double v, double a, double dt, double vmin,
+                            double vmax, double *v_out, double *dist);
+void po_sl_successor(const po_sl_cfg *c, double x, double y, double psi,
+                     double vp, double ve, int up, int ue, double out[5]);
+double po_sl_interpolate(const po_sl_cfg *c, const double *V, const double s[5]);
+int po_sl_backup(const po_sl_cfg *c, const double *V, double *out,
+                 uint8_t *policy_p, uint8_t *policy_e);
+void po_sl_init(const po_sl_cfg *c, double *V);
+
 #endif

@@ -437,6 +437,36 @@ int pe_relative_row_pitch(const pe_relative *h, int32_t *floats) {
   return PE_OK;
 }
 
+int pe_relative_set_tile(pe_relative *h, int32_t rows, int32_t psi_chunk) {
+  int rc = enter(h);
+  if (rc) return rc;
+  pe::Rel5Tile t{rows, psi_chunk};
+  if (rows == 0 && psi_chunk == 0) t = pe::rel5_default_tile(h->g);
+  if (!pe::rel5_tile_valid(h->g, t))
+    return fail(PE_EINVAL, "tile rows=%d psi_chunk=%d does not fit this grid",
+                rows, psi_chunk);
+  h->tile = t;
+  return PE_OK;
+}
+
+int pe_relative_get_tile(const pe_relative *h, int32_t *rows,
+                         int32_t *psi_chunk) {
+  if (!h) return fail(PE_EINVAL, "handle is NULL");
+  if (rows) *rows = h->tile.rows;
+  if (psi_chunk) *psi_chunk = h->tile.psi_chunk;
+  return PE_OK;
+}
+
+int pe_relative_kernel_info(const pe_relative *h, int32_t *threads,
+                            int32_t *smem_bytes, int32_t *resident_ctas) {
+  if (!h) return fail(PE_EINVAL, "handle is NULL");
+  const int consumer_warps = (h->tile.rows * (h->g.xp / 4) + 31) / 32;
+  if (threads) *threads = 32 * (consumer_warps + 1);
+  if (smem_bytes) *smem_bytes = (int32_t)pe::rel5_fast_smem_bytes(h->g, h->tile);
+  if (resident_ctas) *resident_ctas = pe::rel5_last_resident_ctas();
+  return PE_OK;
+}
+
 int pe_relative_stats(pe_relative *h, double *residual, double *max_increase) {
   int rc = enter(h);
   if (rc) return rc;

@@ -56,6 +56,12 @@ size_t rel5_fast_smem_bytes(const Rel5Grid &g, const Rel5Tile &t);
 // Default tile for a grid (rows chosen so rows * xp/4 threads ~ 256).
 Rel5Tile rel5_default_tile(const Rel5Grid &g);
 
+// Resident CTAs per SM of the most recent fast-stage launch.
+int rel5_last_resident_ctas();
+
+// Whether a tile fits the kernel's limits (threads, shared memory).
+bool rel5_tile_valid(const Rel5Grid &g, const Rel5Tile &t);
+
 // Fast path: float32 local arithmetic.  blend = 0 for stage 1 (or the only
 // stage of RK1), 1 for the RK2 averaging stage.
 cudaError_t rel5_stage_f32(const Rel5Grid &g, const Rel5Tile &t,

@@ -1,19 +1,19 @@
 // Relative 5D ENO/LF stage, fast variant: float32 storage and float32 local
 // arithmetic, one launch per RK stage (native_relative.cpp:124-172).
 //
-// Work decomposition.  A CTA owns `rows` consecutive y rows of one (vP, vE)
-// pair and sweeps `psi_chunk` consecutive headings.  A thread owns one
-// 16-byte chunk of 4 consecutive x cells in one row.  For each heading step
-// the CTA needs, in shared memory:
-//   * its own (vP, vE) plane at headings psi-2 .. psi+2, rows y0-2 .. y0+R+1
-//     (the heading window and the y halo), kept in a ring of 6 slots;
+// Work decomposition.  A work item is `rows` consecutive y rows of one
+// (vP, vE) pair over `psi_chunk` consecutive headings; a persistent CTA walks
+// a strided list of items.  A thread owns one 16-byte chunk of 4 consecutive
+// x cells in one row.  For each heading step the CTA needs, in shared memory:
+//   * its own (vP, vE) plane, rows y0-2 .. y0+R+1 (the y halo), in a ring of
+//     6 slots: the current heading for the y and x neighbours and the heading
+//     two ahead to refill each thread's 5-heading register window;
 //   * the 8 neighbour planes (vE+-1, vE+-2, vP+-1, vP+-2) at the current
 //     heading, rows y0 .. y0+R-1, in a ring of 2 slots.
 // All of it arrives by bulk asynchronous copies (the TMA engine,
-// cp.async.bulk) that complete on mbarriers; thread 0 issues the copies two
-// heading steps ahead, so the 4-cell chunks are computed from shared memory
-// while the next planes stream in.  Every wait is bounded: a wait that gives
-// up sets the handle's timeout flag instead of hanging.
+// cp.async.bulk) issued by a producer warp that runs ahead across items, and
+// completes on mbarriers.  Every wait is bounded: a wait that gives up sets
+// the handle's timeout flag instead of hanging.
 //
 // Arithmetic.  The 4 cells of a chunk are processed as two float2 pairs with
 // sm_100 packed FP32 instructions (__ffma2_rn / __fadd2_rn / __fmul2_rn).
@@ -24,6 +24,7 @@
 // agree with the double-local reference to float rounding except where an
 // ENO selection is tied to rounding; relative5d_exact.cu is the bit-exact
 // path.
+#include <algorithm>
 #include <cstdio>
 
 #include "relative5d.cuh"
@@ -35,6 +36,7 @@ constexpr int OWN_SLOTS = 6;
 constexpr int NB_SLOTS = 2;
 constexpr int NEIGHBOURS = 8;  // vE-2, vE-1, vE+1, vE+2, vP-2, vP-1, vP+1, vP+2
 constexpr int MAX_THREADS = 512;
+constexpr int TARGET_THREADS = 256;  // launch bound: two CTAs of 256 per SM
 constexpr unsigned WAIT_LIMIT = 1u << 22;
 
 // ---------------------------------------------------------------- PTX helpers
@@ -151,7 +153,7 @@ __device__ __forceinline__ void slope_pair_any(float2 m2, float2 m1, float2 v,
 
 // ENO slopes along x for the 4 cells x0..x0+3 from the window x0-2..x0+5,
 // sharing edge differences and ENO selections between neighbouring cells.
-template <int ORDER>
+template <int ORDER, bool EDGE>
 __device__ __forceinline__ void slopes_x(const float w[8], int x0, int nx,
                                          float lo[4], float hi[4]) {
   float e[7];
@@ -172,9 +174,9 @@ __device__ __forceinline__ void slopes_x(const float w[8], int x0, int nx,
     for (int k = 2; k < 7; k++) m[k] = eno_pick(d2[k - 1], d2[k]);
     // Next to an end the missing outer second difference is replaced by the
     // centred one (native_relative.cpp:58-63).
-    if (x0 == 0) m[3] = d2[3];
-    const int k_end = nx - x0;  // window node of x = nx-2
-    if (k_end >= 2 && k_end <= 5) {
+    if (EDGE) {
+      if (x0 == 0) m[3] = d2[3];
+      const int k_end = nx - x0;  // window node of x = nx-2
 #pragma unroll
       for (int k = 2; k <= 5; k++)
         if (k == k_end) m[k + 1] = d2[k];
@@ -186,9 +188,9 @@ __device__ __forceinline__ void slopes_x(const float w[8], int x0, int nx,
     }
   }
   // One-sided first differences at the two end nodes.
-  if (x0 == 0) lo[0] = hi[0] = e[2];
-  const int i_end = nx - 1 - x0;
-  if (i_end >= 0 && i_end < 4) {
+  if (EDGE) {
+    if (x0 == 0) lo[0] = hi[0] = e[2];
+    const int i_end = nx - 1 - x0;
 #pragma unroll
     for (int i = 0; i < 4; i++)
       if (i == i_end) lo[i] = hi[i] = e[i + 1];
@@ -198,336 +200,470 @@ __device__ __forceinline__ void slopes_x(const float w[8], int x0, int nx,
 struct FastArgs {
   Rel5Grid g;
   Rel5Stage s;
-  int rows, psi_chunk, slabs, chunks, xc;
+  int rows, psi_chunk, slabs, chunks, xc, consumer_warps, items;
   float ihx, ihp, ihv, ihe;
   float dt;
 };
 
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile(
+      "{\n .reg .b64 state;\n"
+      " mbarrier.arrive.shared::cta.b64 state, [%0];\n}" ::"r"(smem_u32(bar))
+      : "memory");
+}
+
+// Shared memory layout of one CTA.
+struct SmemLayout {
+  int own_floats, nb_floats;
+  int own_off, nb_off;                 // floats
+  int bar_off, red_off, trig_off;      // bytes
+  int bytes;
+};
+
+__host__ __device__ inline SmemLayout smem_layout(int rows, int xp, int headings) {
+  SmemLayout L;
+  L.own_floats = (rows + 4) * xp;
+  L.nb_floats = rows * xp;
+  L.own_off = 0;
+  L.nb_off = OWN_SLOTS * L.own_floats;
+  L.bar_off = 4 * (L.nb_off + NB_SLOTS * NEIGHBOURS * L.nb_floats);
+  L.red_off = L.bar_off + 8 * 2 * (OWN_SLOTS + NB_SLOTS);
+  L.trig_off = L.red_off + 4 * (MAX_THREADS / 32);
+  L.bytes = L.trig_off + 4 * 2 * headings;
+  return L;
+}
+
+// One work item: `rows` y rows (from y0) of one (vP, vE) pair over `steps`
+// headings from p0.  Items are numbered heading chunk first, so that the
+// CTAs resident at any moment share the planes of a few headings in L2.
+struct Item {
+  int iv, ie, y0, r_eff, p0, steps;
+};
+
+__device__ __forceinline__ Item decode_item(const FastArgs &a, int idx) {
+  Item it;
+  const int slab = idx % a.slabs;
+  idx /= a.slabs;
+  it.ie = idx % a.g.nve;
+  idx /= a.g.nve;
+  it.iv = idx % a.g.nvp;
+  const int chunk = idx / a.g.nvp;
+  it.y0 = slab * a.rows;
+  it.r_eff = min(a.rows, a.g.nx - it.y0);
+  it.p0 = chunk * a.psi_chunk;
+  it.steps = min(a.psi_chunk, a.g.nh - it.p0);
+  return it;
+}
+
+// Persistent, warp-specialised stage kernel.  Each CTA walks the items
+// blockIdx.x, blockIdx.x + gridDim.x, ...  Warps 0..consumer_warps-1 compute
+// 4-cell chunks; the last warp is the producer: its lane 0 issues every bulk
+// copy in the order the consumers need them, across item boundaries, waiting
+// on a ring slot's "empty" barrier (one arrival per consumer warp) before
+// refilling it.  Consumers wait on the slots' "full" barriers.  Own planes of
+// an item are numbered d = -2 .. steps+1; plane d is read at step d-2 (the
+// heading window refill) and at step d (centre, y and x neighbours).
 template <int ORDER, int BLEND>
-__global__ void __launch_bounds__(MAX_THREADS)
-    rel5_stage_tma_kernel(const FastArgs a) {
+__global__ void __launch_bounds__(TARGET_THREADS, 2)
+    rel5_stage_kernel(const FastArgs a) {
   extern __shared__ __align__(128) float smem[];
   const Rel5Grid &g = a.g;
   const int R = a.rows, XP = g.xp;
-  const int own_floats = (R + 4) * XP;
-  const int nb_floats = R * XP;
-  float *own = smem;                                      // [6][R+4][XP]
-  float *nbr = own + OWN_SLOTS * own_floats;              // [2][8][R][XP]
-  uint64_t *bars = reinterpret_cast<uint64_t *>(nbr + NB_SLOTS * NEIGHBOURS * nb_floats);
-  uint64_t *own_bar = bars, *nb_bar = bars + OWN_SLOTS;
-  float *red = reinterpret_cast<float *>(bars + OWN_SLOTS + NB_SLOTS);
+  const SmemLayout L = smem_layout(R, XP, g.nh);
+  float *own = smem + L.own_off;  // [6][R+4][XP]
+  float *nbr = smem + L.nb_off;   // [2][8][R][XP]
+  char *raw = reinterpret_cast<char *>(smem);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(raw + L.bar_off);
+  uint64_t *own_full = bars, *own_empty = bars + OWN_SLOTS;
+  uint64_t *nb_full = bars + 2 * OWN_SLOTS, *nb_empty = nb_full + NB_SLOTS;
+  float *red = reinterpret_cast<float *>(raw + L.red_off);
+  float *trig = reinterpret_cast<float *>(raw + L.trig_off);  // [nh][cos, sin]
 
-  // Block -> (slab, vE, vP, heading chunk); the heading chunk is outermost so
-  // that resident CTAs share the planes of a few headings in L2.
-  int b = blockIdx.x;
-  const int slab = b % a.slabs;
-  b /= a.slabs;
-  const int ie = b % g.nve;
-  b /= g.nve;
-  const int iv = b % g.nvp;
-  const int chunk = b / g.nvp;
-  const int y0 = slab * R;
-  const int r_eff = min(R, g.nx - y0);
-  const int p0 = chunk * a.psi_chunk;
-  const int steps = min(a.psi_chunk, g.nh - p0);
   const int64_t PP = (int64_t)g.nx * XP;  // plane pitch
-
-  const int tid = threadIdx.x;
-  const int r = tid / a.xc, c = tid % a.xc;
-  const bool active = r < r_eff;
-  const int x0 = 4 * c;
-
-  // Neighbour planes that exist (uniform per CTA).
-  const int nb_e[NEIGHBOURS] = {ie - 2, ie - 1, ie + 1, ie + 2, ie, ie, ie, ie};
-  const int nb_v[NEIGHBOURS] = {iv, iv, iv, iv, iv - 2, iv - 1, iv + 1, iv + 2};
-
-  // Copies are issued by thread 0 only.
-  const int row_lo = max(0, y0 - 2), row_hi = min(g.nx, y0 + r_eff + 2);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const bool producer = warp == a.consumer_warps;
+  unsigned int *timeout = &a.s.stats->timeout;
   auto plane_index = [&](int v_idx, int e_idx, int psi) -> int64_t {
     return ((int64_t)v_idx * g.nve + e_idx) * g.nh + psi;
   };
-  auto issue_own = [&](int d) {  // own plane at relative heading d
-    const int slot = (d + 2) % OWN_SLOTS;
-    const int psi = ((p0 + d) % g.nh + g.nh) % g.nh;
-    const float *src = a.s.src + plane_index(iv, ie, psi) * PP + (int64_t)row_lo * XP;
-    float *dst = own + slot * own_floats + (row_lo - (y0 - 2)) * XP;
-    const uint32_t bytes = (uint32_t)((row_hi - row_lo) * XP * 4);
-    mbar_expect_tx(&own_bar[slot], bytes);
-    bulk_load(dst, src, bytes, &own_bar[slot]);
-  };
-  auto issue_nb = [&](int k) {  // neighbour planes for step k
-    const int slot = k % NB_SLOTS;
-    const int psi = p0 + k;
-    uint32_t total = 0;
-    const uint32_t bytes = (uint32_t)(r_eff * XP * 4);
-#pragma unroll
-    for (int q = 0; q < NEIGHBOURS; q++)
-      if (nb_e[q] >= 0 && nb_e[q] < g.nve && nb_v[q] >= 0 && nb_v[q] < g.nvp)
-        total += bytes;
-    mbar_expect_tx(&nb_bar[slot], total);
-#pragma unroll
-    for (int q = 0; q < NEIGHBOURS; q++)
-      if (nb_e[q] >= 0 && nb_e[q] < g.nve && nb_v[q] >= 0 && nb_v[q] < g.nvp)
-        bulk_load(nbr + (slot * NEIGHBOURS + q) * nb_floats,
-                  a.s.src + plane_index(nb_v[q], nb_e[q], psi) * PP + (int64_t)y0 * XP,
-                  bytes, &nb_bar[slot]);
-  };
 
   if (tid == 0) {
-    for (int i = 0; i < OWN_SLOTS + NB_SLOTS; i++) mbar_init(&bars[i], 1);
+    for (int i = 0; i < OWN_SLOTS; i++) {
+      mbar_init(&own_full[i], 1);
+      mbar_init(&own_empty[i], a.consumer_warps);
+    }
+    for (int i = 0; i < NB_SLOTS; i++) {
+      mbar_init(&nb_full[i], 1);
+      mbar_init(&nb_empty[i], a.consumer_warps);
+    }
     fence_barrier_init();
   }
-  // Rows of the y halo outside the grid are never copied: zero them once.
-  for (int slot = 0; slot < OWN_SLOTS; slot++)
-    for (int i = tid; i < (R + 4) * XP; i += blockDim.x) {
-      const int row = y0 - 2 + i / XP;
-      if (row < 0 || row >= g.nx) own[slot * own_floats + i] = 0.f;
-    }
-  __syncthreads();
-  int last_own = -3, last_nb = -1;  // latest issued (thread 0)
-  if (tid == 0) {
-    for (int d = -2; d <= 3 && d <= steps + 1; d++) {
-      issue_own(d);
-      last_own = d;
-    }
-    for (int k = 0; k < NB_SLOTS && k < steps; k++) {
-      issue_nb(k);
-      last_nb = k;
-    }
+  for (int k = tid; k < g.nh; k += blockDim.x) {
+    trig[2 * k] = __ldg(a.s.csf + k);
+    trig[2 * k + 1] = __ldg(a.s.snf + k);
   }
-
-  // Per-thread constants.
-  const float ext = (float)g.extent, dxf = (float)g.dx;
-  const float vp = (float)(g.vp_lo + iv * g.dvp);
-  const float ve = (float)(g.ve_lo + ie * g.dve);
-  const float wp = fabsf(vp) * (float)g.curv_p;
-  const float we = fabsf(ve) * (float)g.curv_e;
-  const float ap = (float)g.acc_p, ae = (float)g.acc_e;
-  const float plo = iv == 0 ? 0.f : -ap, phi = iv == g.nvp - 1 ? 0.f : ap;
-  const float elo = ie == 0 ? 0.f : -ae, ehi = ie == g.nve - 1 ? 0.f : ae;
-  const bool p_inner = iv > 0 && iv < g.nvp - 1;
-  const bool e_inner = ie > 0 && ie < g.nve - 1;
-  const int iy = y0 + r;
-  const float y = fmaf((float)iy, dxf, -ext);
-  float xs[4];
-#pragma unroll
-  for (int i = 0; i < 4; i++) xs[i] = fmaf((float)(x0 + i), dxf, -ext);
-  const float2 negx_a = make_float2(-xs[0], -xs[1]), negx_b = make_float2(-xs[2], -xs[3]);
-  const float2 absx_a = make_float2(fabsf(xs[0]), fabsf(xs[1]));
-  const float2 absx_b = make_float2(fabsf(xs[2]), fabsf(xs[3]));
-  const float hx = 0.5f * a.ihx, hp = 0.5f * a.ihp, hv = 0.5f * a.ihv, he = 0.5f * a.ihe;
-  const float dt = a.dt;
-  const int ctr = (r + 2) * XP + x0;  // this chunk in an own slot
+  __syncthreads();
 
   float residual = 0.f;
-  float2 finite_acc = f2(0.f);
+  bool bad = false;
   bool alive = true;
-  unsigned int *timeout = &a.s.stats->timeout;
 
-  for (int k = 0; k < steps; k++) {
-    // Wait for own planes up to k+2 and the neighbour planes of step k.
-    if (alive) {
-      for (int d = (k == 0 ? -2 : k + 2); d <= k + 2 && d <= steps + 1; d++)
-        alive &= wait_phase(&own_bar[(d + 2) % OWN_SLOTS], ((d + 2) / OWN_SLOTS) & 1, timeout);
-      if (alive) alive &= wait_phase(&nb_bar[k % NB_SLOTS], (k / NB_SLOTS) & 1, timeout);
-    }
-    const int ip = p0 + k;
-    if (active && alive) {
-      const float *o0 = own + ((k + 2) % OWN_SLOTS) * own_floats;  // heading k
-      const float *om1 = own + ((k + 1) % OWN_SLOTS) * own_floats;
-      const float *om2 = own + ((k) % OWN_SLOTS) * own_floats;
-      const float *op1 = own + ((k + 3) % OWN_SLOTS) * own_floats;
-      const float *op2 = own + ((k + 4) % OWN_SLOTS) * own_floats;
-      const float *nb = nbr + (k % NB_SLOTS) * NEIGHBOURS * nb_floats + r * XP + x0;
-
-      const float4 C = *reinterpret_cast<const float4 *>(o0 + ctr);
-      const float2 v_a = lo2(C), v_b = hi2(C);
-
-      // x: window x0-2 .. x0+5
-      const float2 xl = *reinterpret_cast<const float2 *>(o0 + ctr - 2);
-      const float2 xr = *reinterpret_cast<const float2 *>(o0 + ctr + 4);
-      const float w[8] = {xl.x, xl.y, C.x, C.y, C.z, C.w, xr.x, xr.y};
-      float xlo[4], xhi[4];
-      slopes_x<ORDER>(w, x0, g.nx, xlo, xhi);
-      const float2 lx_a = make_float2(xlo[0], xlo[1]), lx_b = make_float2(xlo[2], xlo[3]);
-      const float2 hx_a = make_float2(xhi[0], xhi[1]), hx_b = make_float2(xhi[2], xhi[3]);
-
-      // y: rows iy-2 .. iy+2 of heading k
-      float2 ly_a, ly_b, hy_a, hy_b;
-      {
-        const float4 m2 = *reinterpret_cast<const float4 *>(o0 + ctr - 2 * XP);
-        const float4 m1 = *reinterpret_cast<const float4 *>(o0 + ctr - XP);
-        const float4 p1 = *reinterpret_cast<const float4 *>(o0 + ctr + XP);
-        const float4 p2 = *reinterpret_cast<const float4 *>(o0 + ctr + 2 * XP);
-        slope_pair_any<ORDER>(lo2(m2), lo2(m1), v_a, lo2(p1), lo2(p2), iy, g.nx, ly_a, hy_a);
-        slope_pair_any<ORDER>(hi2(m2), hi2(m1), v_b, hi2(p1), hi2(p2), iy, g.nx, ly_b, hy_b);
-      }
-      // psi: periodic, the ring holds headings k-2 .. k+2
-      float2 lp_a, lp_b, hp_a, hp_b;
-      {
-        const float4 m2 = *reinterpret_cast<const float4 *>(om2 + ctr);
-        const float4 m1 = *reinterpret_cast<const float4 *>(om1 + ctr);
-        const float4 p1 = *reinterpret_cast<const float4 *>(op1 + ctr);
-        const float4 p2 = *reinterpret_cast<const float4 *>(op2 + ctr);
-        slope_pair<ORDER, false>(lo2(m2), lo2(m1), v_a, lo2(p1), lo2(p2), 2, 5, lp_a, hp_a);
-        slope_pair<ORDER, false>(hi2(m2), hi2(m1), v_b, hi2(p1), hi2(p2), 2, 5, lp_b, hp_b);
-      }
-      // vE and vP: neighbour slots
-      float2 le_a, le_b, he_a, he_b, lv_a, lv_b, hv_a, hv_b;
-      {
-        const float4 m2 = *reinterpret_cast<const float4 *>(nb + 0 * nb_floats);
-        const float4 m1 = *reinterpret_cast<const float4 *>(nb + 1 * nb_floats);
-        const float4 p1 = *reinterpret_cast<const float4 *>(nb + 2 * nb_floats);
-        const float4 p2 = *reinterpret_cast<const float4 *>(nb + 3 * nb_floats);
-        slope_pair_any<ORDER>(lo2(m2), lo2(m1), v_a, lo2(p1), lo2(p2), ie, g.nve, le_a, he_a);
-        slope_pair_any<ORDER>(hi2(m2), hi2(m1), v_b, hi2(p1), hi2(p2), ie, g.nve, le_b, he_b);
-      }
-      {
-        const float4 m2 = *reinterpret_cast<const float4 *>(nb + 4 * nb_floats);
-        const float4 m1 = *reinterpret_cast<const float4 *>(nb + 5 * nb_floats);
-        const float4 p1 = *reinterpret_cast<const float4 *>(nb + 6 * nb_floats);
-        const float4 p2 = *reinterpret_cast<const float4 *>(nb + 7 * nb_floats);
-        slope_pair_any<ORDER>(lo2(m2), lo2(m1), v_a, lo2(p1), lo2(p2), iv, g.nvp, lv_a, hv_a);
-        slope_pair_any<ORDER>(hi2(m2), hi2(m1), v_b, hi2(p1), hi2(p2), iv, g.nvp, lv_b, hv_b);
-      }
-
-      // Hamiltonian + dissipation (native_relative.cpp:144-157).
-      const float bx = fmaf(ve, __ldg(a.s.csf + ip), -vp);
-      const float by = ve * __ldg(a.s.snf + ip);
-      const float2 bx2 = f2(bx), by2 = f2(by);
-      const float ax_coef = fmaf(wp, fabsf(y), fabsf(bx)) * a.ihx;  // alpha_x / h
-      const float ap_coef = (wp + we) * a.ihp, av_coef = ap * a.ihv, ae_coef = ae * a.ihe;
-      const float2 absby = f2(fabsf(by));
-      const float4 prev4 =
-          BLEND ? *reinterpret_cast<const float4 *>(
-                      a.s.dst + plane_index(iv, ie, ip) * PP + (int64_t)iy * XP + x0)
-                : C;
-
-      float2 out[2];
-#pragma unroll
-      for (int h = 0; h < 2; h++) {
-        const float2 lx = h ? lx_b : lx_a, hxv = h ? hx_b : hx_a;
-        const float2 ly = h ? ly_b : ly_a, hy = h ? hy_b : hy_a;
-        const float2 lp = h ? lp_b : lp_a, hpv = h ? hp_b : hp_a;
-        const float2 lv = h ? lv_b : lv_a, hvv = h ? hv_b : hv_a;
-        const float2 le = h ? le_b : le_a, hev = h ? he_b : he_a;
-        const float2 v = h ? v_b : v_a;
-        const float2 negx = h ? negx_b : negx_a, absx = h ? absx_b : absx_a;
-        // centred gradients g = (lo + hi) / (2h); jumps hi - lo (unscaled)
-        const float2 gx = __fmul2_rn(__fadd2_rn(lx, hxv), f2(hx));
-        const float2 gy = __fmul2_rn(__fadd2_rn(ly, hy), f2(hx));
-        const float2 gpn = __fmul2_rn(__fadd2_rn(lp, hpv), f2(-hp));  // -gp
-        const float2 gv = __fmul2_rn(__fadd2_rn(lv, hvv), f2(hv));
-        const float2 ge = __fmul2_rn(__fadd2_rn(le, hev), f2(he));
-        float2 H = __ffma2_rn(by2, gy, __fmul2_rn(bx2, gx));
-        float2 t = __ffma2_rn(f2(y), gx, gpn);  // y*gx - gp
-        t = __ffma2_rn(negx, gy, t);             // - x*gy
-        float hs[2] = {H.x, H.y};
-        const float ts[2] = {t.x, t.y}, gps[2] = {gpn.x, gpn.y};
-        const float gvs[2] = {gv.x, gv.y}, ges[2] = {ge.x, ge.y};
-#pragma unroll
-        for (int l = 0; l < 2; l++) {
-          hs[l] = fmaf(-wp, fabsf(ts[l]), hs[l]);
-          hs[l] = fmaf(we, fabsf(gps[l]), hs[l]);
-          hs[l] += p_inner ? -ap * fabsf(gvs[l]) : fminf(plo * gvs[l], phi * gvs[l]);
-          hs[l] += e_inner ? ae * fabsf(ges[l]) : fmaxf(elo * ges[l], ehi * ges[l]);
-        }
-        H = make_float2(hs[0], hs[1]);
-        // dissipation: sum alpha_k/h_k * (hi - lo)_k
-        const float2 ay = __fmul2_rn(__ffma2_rn(f2(wp), absx, absby), f2(a.ihx));
-        float2 diss = __fmul2_rn(f2(ax_coef), sub2(hxv, lx));
-        diss = __ffma2_rn(ay, sub2(hy, ly), diss);
-        diss = __ffma2_rn(f2(ap_coef), sub2(hpv, lp), diss);
-        diss = __ffma2_rn(f2(av_coef), sub2(hvv, lv), diss);
-        diss = __ffma2_rn(f2(ae_coef), sub2(hev, le), diss);
-        H = __ffma2_rn(f2(0.5f), diss, H);
-        float2 value = __ffma2_rn(f2(dt), make_float2(fminf(H.x, 0.f), fminf(H.y, 0.f)), v);
-        const float2 prev = BLEND ? (h ? hi2(prev4) : lo2(prev4)) : v;
-        if (BLEND) value = __fmul2_rn(f2(0.5f), __fadd2_rn(prev, value));
-        if (x0 + 2 * h + 1 >= g.nx) {  // row padding stays 0
-          if (x0 + 2 * h >= g.nx) value.x = 0.f;
-          value.y = 0.f;
-        }
-        finite_acc = __ffma2_rn(value, f2(0.f), finite_acc);
-        out[h] = value;
-        if (BLEND || ORDER == 1) {
-          const float2 change = sub2(value, prev);
-          residual = fmaxf(residual, fmaxf(fabsf(change.x), fabsf(change.y)));
-          const float pv[2] = {prev.x, prev.y}, nv[2] = {value.x, value.y};
-#pragma unroll
-          for (int l = 0; l < 2; l++) {
-            const int ix = x0 + 2 * h + l;
-            if (pv[l] > 0.f && nv[l] <= 0.f && ix < g.nx) {
-              float *slot = a.s.arrival + plane_index(iv, ie, ip) * PP +
-                            (int64_t)iy * XP + ix;
-              if (isnan(*slot))
-                *slot = (float)(a.s.t + a.s.dt * (double)pv[l] /
-                                            ((double)pv[l] - (double)nv[l]));
-            }
+  if (producer) {
+    if (lane == 0) {
+      unsigned og = 0, ng = 0;  // own planes / neighbour sets issued so far
+      for (int idx = blockIdx.x; idx < a.items && alive; idx += gridDim.x) {
+        const Item it = decode_item(a, idx);
+        const int row_lo = max(0, it.y0 - 2), row_hi = min(g.nx, it.y0 + it.r_eff + 2);
+        const uint32_t own_bytes = (uint32_t)((row_hi - row_lo) * XP * 4);
+        const float *own_src = a.s.src + (int64_t)row_lo * XP;
+        const int own_dst = (row_lo - (it.y0 - 2)) * XP;
+        const uint32_t nb_bytes = (uint32_t)(it.r_eff * XP * 4);
+        int nb_e[NEIGHBOURS], nb_v[NEIGHBOURS], nb_count = 0;
+        {
+          const int de[NEIGHBOURS] = {-2, -1, 1, 2, 0, 0, 0, 0};
+          const int dv[NEIGHBOURS] = {0, 0, 0, 0, -2, -1, 1, 2};
+          for (int q = 0; q < NEIGHBOURS; q++) {
+            nb_e[q] = it.ie + de[q];
+            nb_v[q] = it.iv + dv[q];
+            const bool ok = nb_e[q] >= 0 && nb_e[q] < g.nve && nb_v[q] >= 0 && nb_v[q] < g.nvp;
+            if (!ok) nb_e[q] = -1;
+            nb_count += ok;
           }
         }
+        auto issue_own = [&](int d) {
+          const int slot = (int)(og % OWN_SLOTS);
+          const unsigned use = og / OWN_SLOTS;
+          if (use > 0) alive &= wait_phase(&own_empty[slot], (uint32_t)((use - 1) & 1), timeout);
+          if (!alive) return;
+          fence_async_shared();
+          const int psi = ((it.p0 + d) % g.nh + g.nh) % g.nh;
+          mbar_expect_tx(&own_full[slot], own_bytes);
+          bulk_load(own + slot * L.own_floats + own_dst,
+                    own_src + plane_index(it.iv, it.ie, psi) * PP, own_bytes,
+                    &own_full[slot]);
+          og++;
+        };
+        auto issue_nb = [&](int k) {
+          const int slot = (int)(ng % NB_SLOTS);
+          const unsigned use = ng / NB_SLOTS;
+          if (use > 0) alive &= wait_phase(&nb_empty[slot], (uint32_t)((use - 1) & 1), timeout);
+          if (!alive) return;
+          fence_async_shared();
+          mbar_expect_tx(&nb_full[slot], nb_bytes * nb_count);
+          for (int q = 0; q < NEIGHBOURS; q++)
+            if (nb_e[q] >= 0)
+              bulk_load(nbr + (slot * NEIGHBOURS + q) * L.nb_floats,
+                        a.s.src + plane_index(nb_v[q], nb_e[q], it.p0 + k) * PP +
+                            (int64_t)it.y0 * XP,
+                        nb_bytes, &nb_full[slot]);
+          ng++;
+        };
+        for (int d = -2; d <= 1 && alive; d++) issue_own(d);
+        for (int k = 0; k < it.steps && alive; k++) {
+          issue_own(k + 2);
+          if (alive) issue_nb(k);
+        }
       }
-      const float4 result = make_float4(out[0].x, out[0].y, out[1].x, out[1].y);
-      *reinterpret_cast<float4 *>(a.s.dst + plane_index(iv, ie, ip) * PP +
-                                  (int64_t)iy * XP + x0) = result;
+      // Every issued copy is consumed by the consumer warps, which wait for
+      // it; after a timeout wait (bounded) for the last one before exiting.
+      if (!alive && og > 0)
+        wait_phase(&own_full[(og - 1) % OWN_SLOTS], (uint32_t)(((og - 1) / OWN_SLOTS) & 1),
+                   timeout);
     }
-    __syncthreads();
-    // Refill: the slot of heading k-2 and the neighbour slot of step k are
-    // free now.
-    if (tid == 0 && alive) {
-      fence_async_shared();
-      if (k + 4 <= steps + 1) {
-        issue_own(k + 4);
-        last_own = k + 4;
+  } else {
+    const int r = tid / a.xc, c = tid % a.xc;
+    const int x0 = 4 * c;
+    const float ext = (float)g.extent, dxf = (float)g.dx;
+    const float ap = (float)g.acc_p, ae = (float)g.acc_e;
+    float xs[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) xs[i] = fmaf((float)(x0 + i), dxf, -ext);
+    const float2 negx_a = make_float2(-xs[0], -xs[1]), negx_b = make_float2(-xs[2], -xs[3]);
+    const float2 absx_a = make_float2(fabsf(xs[0]), fabsf(xs[1]));
+    const float2 absx_b = make_float2(fabsf(xs[2]), fabsf(xs[3]));
+    const float hx = 0.5f * a.ihx, hp = 0.5f * a.ihp, hv = 0.5f * a.ihv, he = 0.5f * a.ihe;
+    const float dt = a.dt;
+    const int ctr = (r + 2) * XP + x0;  // this chunk in an own slot
+    const int nbo = r * XP + x0;        // this chunk in a neighbour slot
+    const bool x_edge = x0 == 0 || x0 + 5 >= g.nx;  // chunk touches an x end
+    const bool tail = x0 + 4 > g.nx;                // chunk holds row padding
+    float2 finite_acc = f2(0.f);
+    unsigned og = 0, ng = 0;
+
+    for (int idx = blockIdx.x; idx < a.items; idx += gridDim.x) {
+      const Item it = decode_item(a, idx);
+      const bool active = r < it.r_eff;
+      const int iy = it.y0 + r;
+      const bool y_edge = iy < 2 || iy + 2 >= g.nx;
+      const float vp = (float)(g.vp_lo + it.iv * g.dvp);
+      const float ve = (float)(g.ve_lo + it.ie * g.dve);
+      const float wp = fabsf(vp) * (float)g.curv_p;
+      const float we = fabsf(ve) * (float)g.curv_e;
+      const float plo = it.iv == 0 ? 0.f : -ap, phi = it.iv == g.nvp - 1 ? 0.f : ap;
+      const float elo = it.ie == 0 ? 0.f : -ae, ehi = it.ie == g.nve - 1 ? 0.f : ae;
+      const bool p_inner = it.iv > 0 && it.iv < g.nvp - 1;
+      const bool e_inner = it.ie > 0 && it.ie < g.nve - 1;
+      const bool v_slope_inner = it.iv >= 2 && it.iv + 2 < g.nvp;
+      const bool e_slope_inner = it.ie >= 2 && it.ie + 2 < g.nve;
+      const float y = fmaf((float)iy, dxf, -ext);
+      const float ap_coef = (wp + we) * a.ihp, av_coef = ap * a.ihv, ae_coef = ae * a.ihe;
+      const float2 ay_a = __fmul2_rn(__fmul2_rn(f2(wp), absx_a), f2(a.ihx));
+      const float2 ay_b = __fmul2_rn(__fmul2_rn(f2(wp), absx_b), f2(a.ihx));
+      const float wy = wp * fabsf(y) * a.ihx;
+      const int64_t out0 =
+          plane_index(it.iv, it.ie, it.p0) * PP + (int64_t)iy * XP + x0;
+      float *gdst = a.s.dst + out0;
+      float *garr = a.s.arrival + out0;
+      const unsigned base = og;  // global index of own plane d = -2
+
+      // Heading window: this chunk at headings k-2 .. k+2.
+      float4 win[5];
+#pragma unroll
+      for (int d = 0; d < 5; d++) {
+        const unsigned q = base + d;
+        const int slot = (int)(q % OWN_SLOTS);
+        if (alive) alive &= wait_phase(&own_full[slot], (uint32_t)((q / OWN_SLOTS) & 1), timeout);
+        win[d] = *reinterpret_cast<const float4 *>(own + slot * L.own_floats + ctr);
       }
-      if (k + 2 < steps) {
-        issue_nb(k + 2);
-        last_nb = k + 2;
+
+      for (int k = 0; k < it.steps; k++) {
+        if (k > 0) {
+          const unsigned q = base + k + 4;  // plane k+2
+          const int slot = (int)(q % OWN_SLOTS);
+          if (alive) alive &= wait_phase(&own_full[slot], (uint32_t)((q / OWN_SLOTS) & 1), timeout);
+#pragma unroll
+          for (int d = 0; d < 4; d++) win[d] = win[d + 1];
+          win[4] = *reinterpret_cast<const float4 *>(own + slot * L.own_floats + ctr);
+        }
+        const int ns = (int)(ng % NB_SLOTS);
+        if (alive) alive &= wait_phase(&nb_full[ns], (uint32_t)((ng / NB_SLOTS) & 1), timeout);
+        const int cslot = (int)((base + k + 2) % OWN_SLOTS);  // plane k
+
+        if (active && alive) {
+          const float *o0 = own + cslot * L.own_floats + ctr;
+          const float *nb = nbr + ns * NEIGHBOURS * L.nb_floats + nbo;
+          const float4 C = win[2];
+          const float2 v_a = lo2(C), v_b = hi2(C);
+
+          // x: window x0-2 .. x0+5
+          const float2 xl = *reinterpret_cast<const float2 *>(o0 - 2);
+          const float2 xr = *reinterpret_cast<const float2 *>(o0 + 4);
+          const float w[8] = {xl.x, xl.y, C.x, C.y, C.z, C.w, xr.x, xr.y};
+          float xlo[4], xhi[4];
+          if (x_edge)
+            slopes_x<ORDER, true>(w, x0, g.nx, xlo, xhi);
+          else
+            slopes_x<ORDER, false>(w, x0, g.nx, xlo, xhi);
+          const float2 lx_a = make_float2(xlo[0], xlo[1]), lx_b = make_float2(xlo[2], xlo[3]);
+          const float2 hx_a = make_float2(xhi[0], xhi[1]), hx_b = make_float2(xhi[2], xhi[3]);
+
+          // y: rows iy-2 .. iy+2 of heading k
+          float2 ly_a, ly_b, hy_a, hy_b;
+          {
+            const float4 m2 = *reinterpret_cast<const float4 *>(o0 - 2 * XP);
+            const float4 m1 = *reinterpret_cast<const float4 *>(o0 - XP);
+            const float4 p1 = *reinterpret_cast<const float4 *>(o0 + XP);
+            const float4 p2 = *reinterpret_cast<const float4 *>(o0 + 2 * XP);
+            if (y_edge) {
+              slope_pair<ORDER, true>(lo2(m2), lo2(m1), v_a, lo2(p1), lo2(p2), iy, g.nx, ly_a, hy_a);
+              slope_pair<ORDER, true>(hi2(m2), hi2(m1), v_b, hi2(p1), hi2(p2), iy, g.nx, ly_b, hy_b);
+            } else {
+              slope_pair<ORDER, false>(lo2(m2), lo2(m1), v_a, lo2(p1), lo2(p2), iy, g.nx, ly_a, hy_a);
+              slope_pair<ORDER, false>(hi2(m2), hi2(m1), v_b, hi2(p1), hi2(p2), iy, g.nx, ly_b, hy_b);
+            }
+          }
+          // psi: periodic, from the register window
+          float2 lp_a, lp_b, hp_a, hp_b;
+          slope_pair<ORDER, false>(lo2(win[0]), lo2(win[1]), v_a, lo2(win[3]), lo2(win[4]), 2, 5, lp_a, hp_a);
+          slope_pair<ORDER, false>(hi2(win[0]), hi2(win[1]), v_b, hi2(win[3]), hi2(win[4]), 2, 5, lp_b, hp_b);
+          // vE and vP: neighbour slots
+          float2 le_a, le_b, he_a, he_b, lv_a, lv_b, hv_a, hv_b;
+          {
+            const float4 m2 = *reinterpret_cast<const float4 *>(nb + 0 * L.nb_floats);
+            const float4 m1 = *reinterpret_cast<const float4 *>(nb + 1 * L.nb_floats);
+            const float4 p1 = *reinterpret_cast<const float4 *>(nb + 2 * L.nb_floats);
+            const float4 p2 = *reinterpret_cast<const float4 *>(nb + 3 * L.nb_floats);
+            if (e_slope_inner) {
+              slope_pair<ORDER, false>(lo2(m2), lo2(m1), v_a, lo2(p1), lo2(p2), it.ie, g.nve, le_a, he_a);
+              slope_pair<ORDER, false>(hi2(m2), hi2(m1), v_b, hi2(p1), hi2(p2), it.ie, g.nve, le_b, he_b);
+            } else {
+              slope_pair<ORDER, true>(lo2(m2), lo2(m1), v_a, lo2(p1), lo2(p2), it.ie, g.nve, le_a, he_a);
+              slope_pair<ORDER, true>(hi2(m2), hi2(m1), v_b, hi2(p1), hi2(p2), it.ie, g.nve, le_b, he_b);
+            }
+          }
+          {
+            const float4 m2 = *reinterpret_cast<const float4 *>(nb + 4 * L.nb_floats);
+            const float4 m1 = *reinterpret_cast<const float4 *>(nb + 5 * L.nb_floats);
+            const float4 p1 = *reinterpret_cast<const float4 *>(nb + 6 * L.nb_floats);
+            const float4 p2 = *reinterpret_cast<const float4 *>(nb + 7 * L.nb_floats);
+            if (v_slope_inner) {
+              slope_pair<ORDER, false>(lo2(m2), lo2(m1), v_a, lo2(p1), lo2(p2), it.iv, g.nvp, lv_a, hv_a);
+              slope_pair<ORDER, false>(hi2(m2), hi2(m1), v_b, hi2(p1), hi2(p2), it.iv, g.nvp, lv_b, hv_b);
+            } else {
+              slope_pair<ORDER, true>(lo2(m2), lo2(m1), v_a, lo2(p1), lo2(p2), it.iv, g.nvp, lv_a, hv_a);
+              slope_pair<ORDER, true>(hi2(m2), hi2(m1), v_b, hi2(p1), hi2(p2), it.iv, g.nvp, lv_b, hv_b);
+            }
+          }
+
+          // Hamiltonian + dissipation (native_relative.cpp:144-157).
+          const int ip = it.p0 + k;
+          const float bx = fmaf(ve, trig[2 * ip], -vp);
+          const float by = ve * trig[2 * ip + 1];
+          const float2 bx2 = f2(bx), by2 = f2(by);
+          const float ax_coef = fmaf(fabsf(bx), a.ihx, wy);  // alpha_x / h
+          const float aby = fabsf(by) * a.ihx;
+          const float4 prev4 = BLEND ? *reinterpret_cast<const float4 *>(gdst) : C;
+
+          float2 out[2];
+#pragma unroll
+          for (int h = 0; h < 2; h++) {
+            const float2 lx = h ? lx_b : lx_a, hxv = h ? hx_b : hx_a;
+            const float2 ly = h ? ly_b : ly_a, hy = h ? hy_b : hy_a;
+            const float2 lp = h ? lp_b : lp_a, hpv = h ? hp_b : hp_a;
+            const float2 lv = h ? lv_b : lv_a, hvv = h ? hv_b : hv_a;
+            const float2 le = h ? le_b : le_a, hev = h ? he_b : he_a;
+            const float2 v = h ? v_b : v_a;
+            const float2 negx = h ? negx_b : negx_a;
+            const float2 ay = __fadd2_rn(h ? ay_b : ay_a, f2(aby));
+            // centred gradients g = (lo + hi) / (2h); jumps hi - lo (unscaled)
+            const float2 gx = __fmul2_rn(__fadd2_rn(lx, hxv), f2(hx));
+            const float2 gy = __fmul2_rn(__fadd2_rn(ly, hy), f2(hx));
+            const float2 gpn = __fmul2_rn(__fadd2_rn(lp, hpv), f2(-hp));  // -gp
+            const float2 gv = __fmul2_rn(__fadd2_rn(lv, hvv), f2(hv));
+            const float2 ge = __fmul2_rn(__fadd2_rn(le, hev), f2(he));
+            float2 H = __ffma2_rn(by2, gy, __fmul2_rn(bx2, gx));
+            float2 t = __ffma2_rn(f2(y), gx, gpn);  // y*gx - gp
+            t = __ffma2_rn(negx, gy, t);             // - x*gy
+            float hs[2] = {H.x, H.y};
+            const float ts[2] = {t.x, t.y}, gps[2] = {gpn.x, gpn.y};
+            const float gvs[2] = {gv.x, gv.y}, ges[2] = {ge.x, ge.y};
+#pragma unroll
+            for (int l = 0; l < 2; l++) {
+              hs[l] = fmaf(-wp, fabsf(ts[l]), hs[l]);
+              hs[l] = fmaf(we, fabsf(gps[l]), hs[l]);
+            }
+            if (p_inner) {
+#pragma unroll
+              for (int l = 0; l < 2; l++) hs[l] = fmaf(-ap, fabsf(gvs[l]), hs[l]);
+            } else {
+#pragma unroll
+              for (int l = 0; l < 2; l++) hs[l] += fminf(plo * gvs[l], phi * gvs[l]);
+            }
+            if (e_inner) {
+#pragma unroll
+              for (int l = 0; l < 2; l++) hs[l] = fmaf(ae, fabsf(ges[l]), hs[l]);
+            } else {
+#pragma unroll
+              for (int l = 0; l < 2; l++) hs[l] += fmaxf(elo * ges[l], ehi * ges[l]);
+            }
+            H = make_float2(hs[0], hs[1]);
+            // dissipation: sum alpha_k/h_k * (hi - lo)_k
+            float2 diss = __fmul2_rn(f2(ax_coef), sub2(hxv, lx));
+            diss = __ffma2_rn(ay, sub2(hy, ly), diss);
+            diss = __ffma2_rn(f2(ap_coef), sub2(hpv, lp), diss);
+            diss = __ffma2_rn(f2(av_coef), sub2(hvv, lv), diss);
+            diss = __ffma2_rn(f2(ae_coef), sub2(hev, le), diss);
+            H = __ffma2_rn(f2(0.5f), diss, H);
+            float2 value =
+                __ffma2_rn(f2(dt), make_float2(fminf(H.x, 0.f), fminf(H.y, 0.f)), v);
+            const float2 prev = BLEND ? (h ? hi2(prev4) : lo2(prev4)) : v;
+            if (BLEND) value = __fmul2_rn(f2(0.5f), __fadd2_rn(prev, value));
+            if (tail && x0 + 2 * h + 1 >= g.nx) {  // row padding stays 0
+              if (x0 + 2 * h >= g.nx) value.x = 0.f;
+              value.y = 0.f;
+            }
+            finite_acc = __ffma2_rn(value, f2(0.f), finite_acc);
+            out[h] = value;
+            if (BLEND || ORDER == 1) {
+              const float2 change = sub2(value, prev);
+              residual = fmaxf(residual, fmaxf(fabsf(change.x), fabsf(change.y)));
+              // First crossing of zero (native_relative.cpp:167-168).  The
+              // update never increases a cell, so a crossing has
+              // prev * value <= 0 with prev > 0.
+              const float2 sgn = __fmul2_rn(prev, value);
+              if (sgn.x <= 0.f || sgn.y <= 0.f) {
+                const float pv[2] = {prev.x, prev.y}, nv[2] = {value.x, value.y};
+#pragma unroll
+                for (int l = 0; l < 2; l++) {
+                  float *slot = garr + 2 * h + l;
+                  if (pv[l] > 0.f && nv[l] <= 0.f && x0 + 2 * h + l < g.nx && isnan(*slot))
+                    *slot = (float)(a.s.t + a.s.dt * (double)pv[l] /
+                                                ((double)pv[l] - (double)nv[l]));
+                }
+              }
+            }
+          }
+          *reinterpret_cast<float4 *>(gdst) =
+              make_float4(out[0].x, out[0].y, out[1].x, out[1].y);
+        }
+        // Release plane k (and the window-only planes at the item's ends) and
+        // this step's neighbour set.
+        __syncwarp();
+        if (lane == 0) {
+          if (k == 0) {
+            mbar_arrive(&own_empty[(int)(base % OWN_SLOTS)]);
+            mbar_arrive(&own_empty[(int)((base + 1) % OWN_SLOTS)]);
+          }
+          mbar_arrive(&own_empty[cslot]);
+          if (k == it.steps - 1) {
+            mbar_arrive(&own_empty[(int)((base + it.steps + 2) % OWN_SLOTS)]);
+            mbar_arrive(&own_empty[(int)((base + it.steps + 3) % OWN_SLOTS)]);
+          }
+          mbar_arrive(&nb_empty[ns]);
+        }
+        ng++;
+        gdst += PP;
+        garr += PP;
       }
+      og = base + it.steps + 4;
     }
+    bad = !(isfinite(finite_acc.x) && isfinite(finite_acc.y));
   }
 
   // Block reductions: non-finite flag and the largest change.
-  const bool bad = active && !(isfinite(finite_acc.x) && isfinite(finite_acc.y));
   if (__syncthreads_or(bad) && tid == 0) atomicOr(&a.s.stats->nonfinite, 1u);
   if (BLEND || ORDER == 1) {
     for (int off = 16; off > 0; off >>= 1)
       residual = fmaxf(residual, __shfl_xor_sync(0xffffffffu, residual, off));
-    if ((tid & 31) == 0) red[tid >> 5] = residual;
+    if (lane == 0) red[warp] = residual;
     __syncthreads();
     if (tid == 0) {
       float m = 0.f;
-      for (int w = 0; w < (int)((blockDim.x + 31) >> 5); w++) m = fmaxf(m, red[w]);
+      for (int w = 0; w < (int)(blockDim.x >> 5); w++) m = fmaxf(m, red[w]);
       if (m > 0.f)
         atomicMax(&a.s.stats->residual,
                   (unsigned long long)__double_as_longlong((double)m));
     }
   }
-  if (__syncthreads_or(!alive) && tid == 0) {
-    // A wait gave up: wait (bounded) for the last phase issued on every
-    // barrier, so no copy is still writing this CTA's shared memory when it
-    // exits.  Phases complete in order.
-    for (int d = last_own; d >= last_own - OWN_SLOTS + 1 && d >= -2; d--)
-      for (unsigned i = 0; i < WAIT_LIMIT; i++)
-        if (mbar_try_wait(&own_bar[(d + 2) % OWN_SLOTS], ((d + 2) / OWN_SLOTS) & 1)) break;
-    for (int k = last_nb; k >= last_nb - NB_SLOTS + 1 && k >= 0; k--)
-      for (unsigned i = 0; i < WAIT_LIMIT; i++)
-        if (mbar_try_wait(&nb_bar[k % NB_SLOTS], (k / NB_SLOTS) & 1)) break;
-  }
 }
 
+int g_last_resident = 0;
+
 template <int ORDER, int BLEND>
-cudaError_t launch(const FastArgs &args, size_t smem, int threads, int blocks,
+cudaError_t launch(const FastArgs &args, size_t smem, int threads,
                    cudaStream_t stream) {
-  static bool configured = false;
-  if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(rel5_stage_tma_kernel<ORDER, BLEND>,
+  // Resident CTAs per SM for this (shared memory, block size); recomputed
+  // when either changes.
+  static int configured_smem = 0, configured_threads = 0;
+  static int resident = 0;
+  if (configured_smem != (int)smem || configured_threads != threads || resident == 0) {
+    cudaError_t e = cudaFuncSetAttribute(rel5_stage_kernel<ORDER, BLEND>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         227 * 1024);
+                                         (int)smem);
     if (e != cudaSuccess) return e;
-    configured = true;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &resident, rel5_stage_kernel<ORDER, BLEND>, threads, smem);
+    if (e != cudaSuccess) return e;
+    if (resident < 1) return cudaErrorInvalidConfiguration;
+    configured_smem = (int)smem;
+    configured_threads = threads;
   }
-  rel5_stage_tma_kernel<ORDER, BLEND><<<blocks, threads, smem, stream>>>(args);
+  int device = 0, sms = 0;
+  cudaGetDevice(&device);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  const int blocks = std::min(args.items, sms * resident);
+  g_last_resident = resident;
+  rel5_stage_kernel<ORDER, BLEND><<<blocks, threads, smem, stream>>>(args);
   return cudaGetLastError();
 }
 
@@ -589,18 +725,18 @@ cudaError_t rel5_unpack(const Rel5Grid &g, const float *dense, float *padded,
   return cudaGetLastError();
 }
 
+int rel5_last_resident_ctas() { return g_last_resident; }
+
 size_t rel5_fast_smem_bytes(const Rel5Grid &g, const Rel5Tile &t) {
-  const size_t own = (size_t)OWN_SLOTS * (t.rows + 4) * g.xp;
-  const size_t nb = (size_t)NB_SLOTS * NEIGHBOURS * t.rows * g.xp;
-  return 4 * (own + nb) + 8 * (OWN_SLOTS + NB_SLOTS) + 4 * (MAX_THREADS / 32);
+  return (size_t)smem_layout(t.rows, g.xp, g.nh).bytes;
 }
 
 Rel5Tile rel5_default_tile(const Rel5Grid &g) {
   const int xc = g.xp / 4;
-  Rel5Tile t{1, 12};
-  // rows: at most 256 threads, fewest idle rows, then most rows.
+  Rel5Tile t{1, 8};
+  // rows: at most 7 consumer warps, fewest idle rows, then most rows.
   int best_waste = 1 << 30;
-  for (int rows = 1; rows * xc <= 256 && rows <= g.nx; rows++) {
+  for (int rows = 1; rows * xc <= TARGET_THREADS - 32 && rows <= g.nx; rows++) {
     const int slabs = (g.nx + rows - 1) / rows;
     const int waste = slabs * rows - g.nx;
     if (waste < best_waste || (waste == best_waste && rows > t.rows)) {
@@ -608,33 +744,42 @@ Rel5Tile rel5_default_tile(const Rel5Grid &g) {
       t.rows = rows;
     }
   }
-  t.psi_chunk = g.nh < 12 ? g.nh : 12;
+  // Heading chunks of 24 measured fastest on the 65x48x21x21 grid (B200).
+  t.psi_chunk = g.nh < 24 ? g.nh : 24;
   return t;
+}
+
+bool rel5_tile_valid(const Rel5Grid &g, const Rel5Tile &t) {
+  if (t.rows < 1 || t.rows > g.nx || t.psi_chunk < 1 || t.psi_chunk > g.nh)
+    return false;
+  const int consumer_warps = (t.rows * (g.xp / 4) + 31) / 32;
+  if (32 * (consumer_warps + 1) > TARGET_THREADS) return false;
+  return rel5_fast_smem_bytes(g, t) <= 227 * 1024;
 }
 
 cudaError_t rel5_stage_f32(const Rel5Grid &g, const Rel5Tile &t,
                            const Rel5Stage &s, int blend, cudaStream_t stream) {
+  if (!rel5_tile_valid(g, t)) return cudaErrorInvalidConfiguration;
   FastArgs args;
   args.g = g;
   args.s = s;
   args.rows = t.rows;
   args.psi_chunk = t.psi_chunk;
   args.xc = g.xp / 4;
+  args.consumer_warps = (t.rows * args.xc + 31) / 32;
   args.slabs = (g.nx + t.rows - 1) / t.rows;
   args.chunks = (g.nh + t.psi_chunk - 1) / t.psi_chunk;
+  args.items = args.slabs * g.nve * g.nvp * args.chunks;
   args.ihx = (float)(1.0 / g.dx);
   args.ihp = (float)(1.0 / g.dphi);
   args.ihv = (float)(1.0 / g.dvp);
   args.ihe = (float)(1.0 / g.dve);
   args.dt = (float)s.dt;
-  const int threads = ((t.rows * args.xc + 31) / 32) * 32;
-  if (threads > MAX_THREADS) return cudaErrorInvalidConfiguration;
+  const int threads = 32 * (args.consumer_warps + 1);
   const size_t smem = rel5_fast_smem_bytes(g, t);
-  if (smem > 227 * 1024) return cudaErrorInvalidConfiguration;
-  const int blocks = args.slabs * g.nve * g.nvp * args.chunks;
-  if (g.order == 1) return launch<1, 0>(args, smem, threads, blocks, stream);
-  if (blend) return launch<2, 1>(args, smem, threads, blocks, stream);
-  return launch<2, 0>(args, smem, threads, blocks, stream);
+  if (g.order == 1) return launch<1, 0>(args, smem, threads, stream);
+  if (blend) return launch<2, 1>(args, smem, threads, stream);
+  return launch<2, 0>(args, smem, threads, stream);
 }
 
 cudaError_t rel5_init(const Rel5Grid &g, const float *plane, float *field,

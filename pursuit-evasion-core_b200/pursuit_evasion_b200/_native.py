@@ -61,6 +61,31 @@ class RelativeParams(ctypes.Structure):
     ]
 
 
+class WorldParams(ctypes.Structure):
+    _fields_ = [
+        ("positions", ctypes.c_int32),
+        ("headings", ctypes.c_int32),
+        ("p_speeds", ctypes.c_int32),
+        ("e_speeds", ctypes.c_int32),
+        ("extent", ctypes.c_double),
+        ("arena", ctypes.c_double),
+        ("capture_radius", ctypes.c_double),
+        ("p_speed_min", ctypes.c_double),
+        ("p_speed_max", ctypes.c_double),
+        ("p_acceleration", ctypes.c_double),
+        ("p_curvature", ctypes.c_double),
+        ("e_speed_min", ctypes.c_double),
+        ("e_speed_max", ctypes.c_double),
+        ("e_acceleration", ctypes.c_double),
+        ("e_curvature", ctypes.c_double),
+        ("cfl", ctypes.c_double),
+        ("order", ctypes.c_int32),
+        ("linear_speed_boundary", ctypes.c_int32),
+        ("avoid_mode", ctypes.c_int32),
+        ("device", ctypes.c_int32),
+    ]
+
+
 _P = ctypes.c_void_p
 _I64P = ctypes.POINTER(ctypes.c_int64)
 _DP = ctypes.POINTER(ctypes.c_double)
@@ -86,10 +111,32 @@ SIGNATURES = {
     "pe_relative_copy_arrival": (ctypes.c_int, [_P, _P]),
     "pe_relative_device_field": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_void_p)]),
     "pe_relative_row_pitch": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int32)]),
+    "pe_relative_set_tile": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32]),
+    "pe_relative_get_tile": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int32),
+                                            ctypes.POINTER(ctypes.c_int32)]),
+    "pe_relative_kernel_info": (ctypes.c_int, [_P] + [ctypes.POINTER(ctypes.c_int32)] * 3),
     "pe_relative_stats": (ctypes.c_int, [_P, _DP, _DP]),
     "pe_relative_profile": (ctypes.c_int, [_P, ctypes.c_int]),
     "pe_relative_kernel_time": (ctypes.c_int, [_P, ctypes.c_int, _DP, _I64P]),
     "pe_relative_destroy": (ctypes.c_int, [_P]),
+    "pe_world_cells": (ctypes.c_int, [ctypes.POINTER(WorldParams), _I64P]),
+    "pe_world_dt_limit": (ctypes.c_int, [ctypes.POINTER(WorldParams), _DP]),
+    "pe_world_create": (ctypes.c_int, [ctypes.POINTER(WorldParams),
+                                       ctypes.POINTER(ctypes.c_void_p)]),
+    "pe_world_init_contact": (ctypes.c_int, [_P] + [ctypes.c_double] * 4),
+    "pe_world_init_square": (ctypes.c_int, [_P]),
+    "pe_world_init_field": (ctypes.c_int, [_P, _P, _P, ctypes.c_double]),
+    "pe_world_advance": (ctypes.c_int, [_P, ctypes.c_double, _I64P]),
+    "pe_world_step": (ctypes.c_int, [_P, ctypes.c_double]),
+    "pe_world_time": (ctypes.c_int, [_P, _DP, _I64P]),
+    "pe_world_synchronize": (ctypes.c_int, [_P]),
+    "pe_world_copy_field": (ctypes.c_int, [_P, _P]),
+    "pe_world_copy_arrival": (ctypes.c_int, [_P, _P]),
+    "pe_world_residual": (ctypes.c_int, [_P, _DP]),
+    "pe_world_set_stream": (ctypes.c_int, [_P, _P]),
+    "pe_world_profile": (ctypes.c_int, [_P, ctypes.c_int]),
+    "pe_world_kernel_time": (ctypes.c_int, [_P, _DP, _I64P]),
+    "pe_world_destroy": (ctypes.c_int, [_P]),
 }
 
 _lib = None

@@ -162,6 +162,24 @@ class RelativeSolver:
         _native.check(self._lib.pe_relative_device_field(self._h, ctypes.byref(ptr)))
         return ptr.value
 
+    @property
+    def tile(self):
+        """(rows, psi_chunk) of the float32 stage kernel."""
+        rows, chunk = ctypes.c_int32(), ctypes.c_int32()
+        _native.check(self._lib.pe_relative_get_tile(self._h, ctypes.byref(rows),
+                                                     ctypes.byref(chunk)))
+        return rows.value, chunk.value
+
+    def set_tile(self, rows, psi_chunk):
+        _native.check(self._lib.pe_relative_set_tile(self._h, int(rows),
+                                                     int(psi_chunk)))
+
+    def kernel_info(self):
+        """(threads per CTA, shared bytes per CTA, resident CTAs per SM)."""
+        vals = [ctypes.c_int32() for _ in range(3)]
+        _native.check(self._lib.pe_relative_kernel_info(self._h, *map(ctypes.byref, vals)))
+        return tuple(v.value for v in vals)
+
     def stats(self):
         """(residual of the last step, maximum increase since init)."""
         r = ctypes.c_double()

@@ -40,6 +40,16 @@ class W8Cfg(ctypes.Structure):
     ] + [("cfl", ctypes.c_double)]
 
 
+class SLCfg(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int) for n in ("nx", "nh", "nvp", "nve", "mode")] + [
+        (n, ctypes.c_double)
+        for n in ("extent", "radius", "vp_lo", "vp_hi", "ve_lo", "ve_hi",
+                  "acc_p", "acc_e", "curv_p", "curv_e", "dt")
+    ]
+
+
+SL_TUBE, SL_MINTIME = 0, 1
+
 _P = ctypes.c_void_p
 
 
@@ -70,6 +80,12 @@ class Oracle:
             "po_w8_init_contact": (None, [_P] + [ctypes.c_double] * 4 + [_P, _P]),
             "po_w8_stage": (ctypes.c_int, [_P, _P, _P, _P, _P, ctypes.c_float,
                                            ctypes.c_double]),
+            "po_sl_integrated_speed": (None, [ctypes.c_double] * 5 + [_P, _P]),
+            "po_sl_successor": (None, [_P] + [ctypes.c_double] * 5
+                                + [ctypes.c_int, ctypes.c_int, _P]),
+            "po_sl_interpolate": (ctypes.c_double, [_P, _P, _P]),
+            "po_sl_backup": (ctypes.c_int, [_P, _P, _P, _P, _P]),
+            "po_sl_init": (None, [_P, _P]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(lib, name)
@@ -150,6 +166,43 @@ class Oracle:
                                     None if base is None else base.ctypes.data,
                                     None if arrival is None else arrival.ctypes.data,
                                     dt, tau)
+
+    # -- semi-Lagrangian 5D -----------------------------------------------
+    @staticmethod
+    def sl_cfg(config, grid, dt, mode=SL_TUBE):
+        p, e = config.pursuer, config.evader
+        return SLCfg(grid.positions, grid.headings, grid.p_speeds, grid.e_speeds,
+                     mode, grid.extent, config.capture_radius, p.speed_min,
+                     p.speed_max, e.speed_min, e.speed_max, p.acceleration,
+                     e.acceleration, p.max_curvature, e.max_curvature, dt)
+
+    def sl_successor(self, cfg, state, up, ue):
+        out = np.zeros(5)
+        self.lib.po_sl_successor(ctypes.addressof(cfg), *map(float, state), up, ue,
+                                 out.ctypes.data)
+        return out
+
+    def sl_interpolate(self, cfg, V, state):
+        s = np.ascontiguousarray(state, dtype=np.float64)
+        return self.lib.po_sl_interpolate(ctypes.addressof(cfg), V.ctypes.data,
+                                          s.ctypes.data)
+
+    def sl_init(self, cfg, n):
+        V = np.zeros(n)
+        self.lib.po_sl_init(ctypes.addressof(cfg), V.ctypes.data)
+        return V
+
+    def sl_backup(self, cfg, V, with_policy=False):
+        V = np.ascontiguousarray(V, dtype=np.float64)
+        out = np.zeros_like(V)
+        pp = np.zeros(V.size, np.uint8) if with_policy else None
+        pe = np.zeros(V.size, np.uint8) if with_policy else None
+        rc = self.lib.po_sl_backup(ctypes.addressof(cfg), V.ctypes.data,
+                                   out.ctypes.data,
+                                   None if pp is None else pp.ctypes.data,
+                                   None if pe is None else pe.ctypes.data)
+        assert rc == 0, rc
+        return (out, pp, pe) if with_policy else out
 
     def rect_separation(self, p, e, p_body, e_body):
         return self.lib.po_rect_separation(p[0], p[1], p[2], e[0], e[1], e[2],

@@ -1,0 +1,181 @@
+"""Dense 8D ENO/LF step on the GPU against the reference executable's golden
+vectors, the reference executable itself, and the oracle; full-size
+properties on the 58M-cell contact grid (11^4 positions, 9^2 headings,
+7^2 speeds)."""
+
+import json
+import shutil
+import subprocess
+import tempfile
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from pursuit_evasion_b200 import _native
+from pursuit_evasion_b200.reversible.world_dp import WorldGrid, WorldSolver, solve
+from pursuit_evasion_b200.reversible.model import ReversibleConfig, VehicleLimits
+from tests import oracle_lib
+from tests.helpers import A3, DEFAULT, bits, config_from_physics, world_goldens
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = world_goldens()
+FOOTPRINT = (0.5, 0.3)  # length, width of both cars in the contact game
+
+
+def run_gpu(config, grid, times, *, order, linear, init, avoid=True):
+    with WorldSolver(config, grid, order=order,
+                     speed_boundary="linear" if linear else "legacy_signed",
+                     avoid=avoid) as s:
+        if init == "square":
+            s.init_square()
+        elif init == "contact":
+            s.init_contact(FOOTPRINT, FOOTPRINT)
+        else:
+            s.init_field(init)
+        frames = [s.field().copy()]
+        for goal in times[1:]:
+            s.advance(goal)
+            frames.append(s.field().copy())
+        return np.array(frames), s.arrival().copy(), s.steps
+
+
+@pytest.mark.parametrize("name", sorted(GOLDEN))
+def test_world_step_reproduces_reference_golden_bitwise(name):
+    z = GOLDEN[name]
+    n, nh, np_, ne = map(int, z["grid"])
+    config = config_from_physics(z["physics"])
+    grid = WorldGrid(n, nh, np_, ne, float(z["extent"]))
+    horizon, odt = float(z["horizon"]), float(z["output_dt"])
+    times = np.unique(np.minimum(np.arange(int(np.ceil(horizon / odt)) + 1) * odt,
+                                 horizon))
+    frames, arrival, steps = run_gpu(config, grid, times, order=int(z["order"]),
+                                     linear=int(z["linear"]), init="square")
+    assert steps == int(z["internal_steps"])
+    np.testing.assert_array_equal(bits(frames[-1]), bits(z["final"]))
+    np.testing.assert_array_equal(bits(arrival), bits(z["arrival"]))
+
+
+def oracle_world(oracle, config, grid, times, order, linear, avoid, initial):
+    p, e = config.pursuer, config.evader
+    cfg = oracle_lib.W8Cfg(grid.positions, grid.headings, grid.p_speeds,
+                           grid.e_speeds, order, linear, int(avoid), grid.extent,
+                           config.arena_half_width, config.capture_radius,
+                           p.speed_min, p.speed_max, e.speed_min, e.speed_max,
+                           p.acceleration, e.acceleration, p.max_curvature,
+                           e.max_curvature, 0.8)
+    if initial == "contact":
+        a, arrival = oracle.w8_init_contact(cfg, FOOTPRINT, FOOTPRINT)
+    else:
+        a, arrival = oracle.w8_init_square(cfg)
+    first = a.copy()
+    b = np.zeros_like(a)
+    maxdt, tau, steps = oracle.w8_dt_limit(cfg), 0.0, 0
+    for goal in times[1:]:
+        while tau < goal - 1e-10:
+            dt = min(maxdt, goal - tau)
+            if order == 1:
+                oracle.w8_stage(cfg, a, b, None, arrival, dt, tau)
+                a, b = b, a
+            else:
+                oracle.w8_stage(cfg, a, b, None, arrival, dt, tau)
+                oracle.w8_stage(cfg, b, a, a, arrival, dt, tau)
+            tau += dt
+            steps += 1
+    return first, a, arrival, steps
+
+
+@pytest.mark.parametrize("order", [1, 2])
+def test_contact_game_matches_oracle_bitwise(oracle, order):
+    grid = WorldGrid(7, 6, 4, 3, 3.0)
+    times = np.array([0.0, 0.05, 0.1])
+    first, final, arrival, steps = oracle_world(oracle, A3, grid, times, order, 1,
+                                                False, "contact")
+    frames, garrival, gsteps = run_gpu(A3, grid, times, order=order, linear=1,
+                                       init="contact", avoid=False)
+    assert gsteps == steps
+    np.testing.assert_array_equal(bits(frames[0]), bits(first))
+    np.testing.assert_array_equal(bits(frames[-1]), bits(final))
+    np.testing.assert_array_equal(bits(garrival), bits(arrival))
+    assert np.all(frames[-1] <= frames[0])  # tube minimum
+
+
+@pytest.mark.skipif(not oracle_lib.REF_WORLD.exists(),
+                    reason="reference executable not built (make -C oracle ref)")
+def test_contact_field_continuation_matches_reference_executable(oracle):
+    """The reference executable continued from our contact field
+    (--initial-field, native_world.cpp:177-191) equals the GPU step."""
+    config = DEFAULT
+    grid = WorldGrid(5, 4, 3, 3, 3.5)
+    with WorldSolver(config, grid) as s:
+        s.init_contact(FOOTPRINT, FOOTPRINT)
+        initial = s.field().copy()
+        s.advance(0.02)
+        ours = s.field().copy()
+        steps = s.steps
+    out = Path(tempfile.mkdtemp(prefix="pe_w8ref_"))
+    try:
+        initial.tofile(out / "initial.f32")
+        p, e = config.pursuer, config.evader
+        options = {"positions": 5, "headings": 4, "p-speeds": 3, "e-speeds": 3,
+                   "extent": 3.5, "arena": config.arena_half_width,
+                   "radius": config.capture_radius, "p-min": p.speed_min,
+                   "p-max": p.speed_max, "e-min": e.speed_min, "e-max": e.speed_max,
+                   "p-accel": p.acceleration, "e-accel": e.acceleration,
+                   "p-curvature": p.max_curvature, "e-curvature": e.max_curvature,
+                   "horizon": 0.02, "output-dt": 0.02, "order": 2, "cfl": 0.8,
+                   "threads": 2, "history": 0, "linear-speed-boundary": 1,
+                   "initial-field": str(out / "initial.f32"), "output": str(out / "run")}
+        cmd = [str(oracle_lib.REF_WORLD)] + [str(x) for k, v in options.items()
+                                             for x in ("--" + k, v)]
+        subprocess.run(cmd, check=True, capture_output=True)
+        theirs = np.fromfile(out / "run" / "final.f32", np.float32).reshape(grid.shape)
+        timing = json.loads((out / "run" / "native_timing.json").read_text())
+    finally:
+        shutil.rmtree(out)
+    assert steps == timing["internal_steps"]
+    np.testing.assert_array_equal(bits(ours), bits(theirs))
+
+
+def test_world_solve_writes_table(tmp_path):
+    grid = WorldGrid(5, 4, 3, 3, 3.5)
+    meta = solve(DEFAULT, grid, tmp_path / "w", horizon=0.04, output_dt=0.02,
+                 history=True)
+    assert meta["status"] == "complete"
+    fields = np.fromfile(tmp_path / "w" / "fields.f32", np.float32)
+    assert fields.size == 3 * grid.states
+    with pytest.raises(FileExistsError):
+        solve(DEFAULT, grid, tmp_path / "w", horizon=0.04)
+
+
+def test_contact_game_full_size_properties(oracle):
+    """11^4 x 9^2 x 7^2 = 58,110,129 cells, a3 limits, 0.5 x 0.3 m bodies.
+    Contact init equals the oracle's rectangle separation at sampled poses;
+    a few RK2 steps keep the field finite and never raise it."""
+    grid = WorldGrid(11, 9, 7, 7, 3.0)
+    assert grid.states == 58_110_129
+    launches = _native.launch_count()
+    with WorldSolver(A3, grid, avoid=False) as s:
+        s.init_contact(FOOTPRINT, FOOTPRINT)
+        v0 = s.field().copy()
+        for _ in range(3):
+            s.step(s.dt_limit)
+        v = s.field()
+        residual = s.residual()
+    assert _native.launch_count() - launches >= 7
+    dxd = 2 * np.float64(np.float32(grid.extent)) / (grid.positions - 1)
+    pos = lambda i: -np.float64(np.float32(grid.extent)) + i * dxd
+    ang = lambda i: -np.pi + i * 2 * np.pi / grid.headings
+    rng = np.random.default_rng(4)
+    for _ in range(200):
+        q = [int(rng.integers(0, m)) for m in grid.shape]
+        pose_p = (pos(q[0]), pos(q[1]), ang(q[2]))
+        pose_e = (pos(q[4]), pos(q[5]), ang(q[6]))
+        expect = np.float32(oracle.rect_separation(pose_p, pose_e, FOOTPRINT, FOOTPRINT))
+        assert v0[tuple(q)] == expect
+    assert np.isfinite(v).all()
+    assert np.all(v <= v0)
+    assert residual > 0
+    # exact contact: bodies overlapping at the same pose are captured
+    assert v0[5, 5, 0, 0, 5, 5, 0, 0] < 0
