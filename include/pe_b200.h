@@ -200,6 +200,57 @@ int pe_world_profile(pe_world *h, int enable);
 int pe_world_kernel_time(pe_world *h, double *total_ms, int64_t *launches);
 int pe_world_destroy(pe_world *h);
 
+/* ------------------------------------------------------------------------
+ * Relative 5D semi-Lagrangian min-max backup.
+ *
+ * No reference counterpart computes this 5D backup; it composes the
+ * reference's held-command successor (reversible/model.py:86-183), action
+ * catalogue (reversible/controllers.py:19-27), min-P/max-E order with the
+ * tube minimum (local_game/grid_game.py:218-230, the CUDA kernels
+ * `interpolate_p`/`reduce_e` it replaces in spirit) and 5D multilinear
+ * stencil (reversible/relative_table.py:76-102).
+ * ------------------------------------------------------------------------ */
+enum { PE_SL_TUBE = 0, PE_SL_MINTIME = 1 };
+
+typedef struct pe_semilag_params {
+  int32_t positions, headings, p_speeds, e_speeds; /* RelativeGrid */
+  double extent, capture_radius;
+  double p_speed_min, p_speed_max, p_acceleration, p_curvature;
+  double e_speed_min, e_speed_max, e_acceleration, e_curvature;
+  double dt;     /* held-command step; 0 selects the interpolation CFL step
+                    (no coordinate moves more than one grid spacing) */
+  int32_t mode;  /* PE_SL_TUBE: V' = min(V, min_u max_w V(s'));
+                    PE_SL_MINTIME: u' = 0 in the capture disk, else
+                    (1 - e^-dt) + e^-dt * min_u max_w u(s'), u = 1 - e^-T */
+  int32_t device;
+} pe_semilag_params;
+
+typedef struct pe_semilag pe_semilag;
+
+int pe_semilag_dt(const pe_semilag_params *params, double *dt);
+int pe_semilag_create(const pe_semilag_params *params, pe_semilag **out);
+/* initial == NULL: TUBE hypot(x,y) - r; MINTIME 0 in the capture disk, 1
+ * elsewhere.  Otherwise a dense host field (a warm start). */
+int pe_semilag_init(pe_semilag *h, const float *initial);
+/* One backup sweep; with_policy != 0 also records the optimal pursuer and
+ * evader action indices (catalogue order 3*i_a + i_k) of every cell. */
+int pe_semilag_backup(pe_semilag *h, int with_policy);
+/* Value iteration: up to max_iterations backups, checking the sup-norm
+ * change every check_every sweeps; stops once it is below tol (tol = 0: run
+ * all sweeps). */
+int pe_semilag_iterate(pe_semilag *h, int64_t max_iterations, double tol,
+                       int32_t check_every, int64_t *iterations,
+                       double *residual, int32_t *converged);
+int pe_semilag_residual(pe_semilag *h, double *residual);
+int pe_semilag_copy_value(pe_semilag *h, float *host_value);
+int pe_semilag_copy_policy(pe_semilag *h, uint8_t *host_p, uint8_t *host_e);
+int pe_semilag_device_value(pe_semilag *h, float **device_value);
+int pe_semilag_iterations(const pe_semilag *h, int64_t *iterations);
+int pe_semilag_set_stream(pe_semilag *h, void *cuda_stream);
+int pe_semilag_profile(pe_semilag *h, int enable);
+int pe_semilag_kernel_time(pe_semilag *h, double *total_ms, int64_t *launches);
+int pe_semilag_destroy(pe_semilag *h);
+
 #ifdef __cplusplus
 }
 #endif

@@ -69,6 +69,9 @@ void po_sl_successor(const po_sl_cfg *c, double x, double y, double psi,
 double po_sl_interpolate(const po_sl_cfg *c, const double *V, const double s[5]);
 int po_sl_backup(const po_sl_cfg *c, const double *V, double *out,
                  uint8_t *policy_p, uint8_t *policy_e);
+void po_sl_backup_cells(const po_sl_cfg *c, const double *V, size_t count,
+                        const int64_t *cells, double *out, uint8_t *policy_p,
+                        uint8_t *policy_e);
 void po_sl_init(const po_sl_cfg *c, double *V);
 
 #endif

@@ -155,73 +155,89 @@ double po_sl_interpolate(const po_sl_cfg *c, const double *V, const double s[5])
  * indices 3*ia+ik: (0,0) (-a,0) (a,0) (0,-k) (0,k) (-a,-k) (-a,k) (a,-k) (a,k). */
 static const int E_ORDER[9] = {4, 1, 7, 3, 5, 0, 2, 6, 8};
 
+/* Backup of one cell (flat index j): new value and the chosen actions. */
+static double backup_cell(const po_sl_cfg *c, const sl_geom *g, const double *V,
+                          size_t j, int *pick_p, int *pick_e) {
+  const double pi = acos(-1.0);
+  const double beta = exp(-c->dt);
+  const int ix = (int)(j % c->nx);
+  const size_t row = j / c->nx;
+  const int iy = (int)(row % c->nx);
+  const int ip = (int)((row / c->nx) % c->nh);
+  const int ie = (int)((row / ((size_t)c->nx * c->nh)) % c->nve);
+  const int iv = (int)(row / ((size_t)c->nx * c->nh * c->nve));
+  const double x = -c->extent + ix * g->dx, y = -c->extent + iy * g->dx;
+  const double psi = -pi + ip * g->dphi;
+  const double vp = c->vp_lo + iv * g->dvp, ve = c->ve_lo + ie * g->dve;
+  double worst[9];
+  int worst_e[9];
+  for (int up = 0; up < 9; up++) {
+    double w_best = -INFINITY, vals[9];
+    int w_idx = E_ORDER[0];
+    for (int ue = 0; ue < 9; ue++) {
+      double s[5];
+      po_sl_successor(c, x, y, psi, vp, ve, up, ue, s);
+      double v = po_sl_interpolate(c, V, s);
+      if (c->mode == PO_SL_MINTIME) v = v < 0 ? 0 : (v > 1 ? 1 : v);
+      vals[ue] = v;
+      if (v > w_best) w_best = v;
+    }
+    for (int r = 0; r < 9; r++)
+      if (vals[E_ORDER[r]] >= w_best - 1e-7) {
+        w_idx = E_ORDER[r];
+        break;
+      }
+    worst[up] = w_best;
+    worst_e[up] = w_idx;
+  }
+  double best = INFINITY;
+  for (int up = 0; up < 9; up++)
+    if (worst[up] < best) best = worst[up];
+  /* pursuer tie rule: smallest (|k|, |a|, index) among near-minima */
+  int pick = -1, pick_key = 1 << 30;
+  for (int up = 0; up < 9; up++) {
+    if (worst[up] > best + 1e-7) continue;
+    const int ka = abs(up % 3 - 1), aa = abs(up / 3 - 1);
+    const int key = (ka * 2 + aa) * 16 + up;
+    if (key < pick_key) {
+      pick_key = key;
+      pick = up;
+    }
+  }
+  if (pick_p) *pick_p = pick;
+  if (pick_e) *pick_e = worst_e[pick];
+  if (c->mode == PO_SL_TUBE) return best < V[j] ? best : V[j];
+  const double d = hypot(x, y) - c->radius;
+  return d <= 0 ? 0.0 : (1 - beta) + beta * best;
+}
+
 int po_sl_backup(const po_sl_cfg *c, const double *V, double *out,
                  uint8_t *policy_p, uint8_t *policy_e) {
   const sl_geom g = geom(c);
-  const double pi = acos(-1.0);
-  const double beta = exp(-c->dt);
   int bad = 0;
-#pragma omp parallel for schedule(dynamic, 64) reduction(| : bad)
-  for (size_t row = 0; row < g.n / c->nx; row++) {
-    const int iy = (int)(row % c->nx);
-    const int ip = (int)((row / c->nx) % c->nh);
-    const int ie = (int)((row / ((size_t)c->nx * c->nh)) % c->nve);
-    const int iv = (int)(row / ((size_t)c->nx * c->nh * c->nve));
-    const double y = -c->extent + iy * g.dx, psi = -pi + ip * g.dphi;
-    const double vp = c->vp_lo + iv * g.dvp, ve = c->ve_lo + ie * g.dve;
-    for (int ix = 0; ix < c->nx; ix++) {
-      const size_t j = row * c->nx + ix;
-      const double x = -c->extent + ix * g.dx;
-      double worst[9];
-      int worst_e[9];
-      for (int up = 0; up < 9; up++) {
-        double w_best = -INFINITY;
-        int w_idx = E_ORDER[0];
-        double vals[9];
-        for (int ue = 0; ue < 9; ue++) {
-          double s[5];
-          po_sl_successor(c, x, y, psi, vp, ve, up, ue, s);
-          double v = po_sl_interpolate(c, V, s);
-          if (c->mode == PO_SL_MINTIME) v = v < 0 ? 0 : (v > 1 ? 1 : v);
-          vals[ue] = v;
-          if (v > w_best) w_best = v;
-        }
-        for (int r = 0; r < 9; r++)
-          if (vals[E_ORDER[r]] >= w_best - 1e-7) {
-            w_idx = E_ORDER[r];
-            break;
-          }
-        worst[up] = w_best;
-        worst_e[up] = w_idx;
-      }
-      double best = INFINITY;
-      for (int up = 0; up < 9; up++)
-        if (worst[up] < best) best = worst[up];
-      /* pursuer tie rule: smallest (|k|, |a|, index) among near-minima */
-      int pick = -1, pick_key = 1 << 30;
-      for (int up = 0; up < 9; up++) {
-        if (worst[up] > best + 1e-7) continue;
-        const int ka = abs(up % 3 - 1), aa = abs(up / 3 - 1);
-        const int key = (ka * 2 + aa) * 16 + up;
-        if (key < pick_key) {
-          pick_key = key;
-          pick = up;
-        }
-      }
-      double value;
-      if (c->mode == PO_SL_TUBE) {
-        value = best < V[j] ? best : V[j];
-      } else {
-        const double d = hypot(x, y) - c->radius;
-        value = d <= 0 ? 0.0 : (1 - beta) + beta * best;
-      }
-      if (!isfinite(value)) bad = 1;
-      out[j] = value;
-      if (policy_p) policy_p[j] = (uint8_t)pick;
-      if (policy_e) policy_e[j] = (uint8_t)worst_e[pick];
-    }
+#pragma omp parallel for schedule(dynamic, 256) reduction(| : bad)
+  for (size_t j = 0; j < g.n; j++) {
+    int pp, pe;
+    const double value = backup_cell(c, &g, V, j, &pp, &pe);
+    if (!isfinite(value)) bad = 1;
+    out[j] = value;
+    if (policy_p) policy_p[j] = (uint8_t)pp;
+    if (policy_e) policy_e[j] = (uint8_t)pe;
   }
   return bad ? PO_ENONFINITE : 0;
+}
+
+void po_sl_backup_cells(const po_sl_cfg *c, const double *V, size_t count,
+                        const int64_t *cells, double *out, uint8_t *policy_p,
+                        uint8_t *policy_e) {
+  const sl_geom g = geom(c);
+#pragma omp parallel for schedule(dynamic, 4)
+  for (size_t i = 0; i < count; i++) {
+    int pp, pe;
+    out[i] = backup_cell(c, &g, V, (size_t)cells[i], &pp, &pe);
+    if (policy_p) policy_p[i] = (uint8_t)pp;
+    if (policy_e) policy_e[i] = (uint8_t)pe;
+  }
 }
 
 /* Initial fields: TUBE: hypot(x, y) - radius; MINTIME: 0 inside the capture

@@ -86,6 +86,31 @@ class WorldParams(ctypes.Structure):
     ]
 
 
+class SemiLagParams(ctypes.Structure):
+    _fields_ = [
+        ("positions", ctypes.c_int32),
+        ("headings", ctypes.c_int32),
+        ("p_speeds", ctypes.c_int32),
+        ("e_speeds", ctypes.c_int32),
+        ("extent", ctypes.c_double),
+        ("capture_radius", ctypes.c_double),
+        ("p_speed_min", ctypes.c_double),
+        ("p_speed_max", ctypes.c_double),
+        ("p_acceleration", ctypes.c_double),
+        ("p_curvature", ctypes.c_double),
+        ("e_speed_min", ctypes.c_double),
+        ("e_speed_max", ctypes.c_double),
+        ("e_acceleration", ctypes.c_double),
+        ("e_curvature", ctypes.c_double),
+        ("dt", ctypes.c_double),
+        ("mode", ctypes.c_int32),
+        ("device", ctypes.c_int32),
+    ]
+
+
+PE_SL_TUBE = 0
+PE_SL_MINTIME = 1
+
 _P = ctypes.c_void_p
 _I64P = ctypes.POINTER(ctypes.c_int64)
 _DP = ctypes.POINTER(ctypes.c_double)
@@ -137,6 +162,23 @@ SIGNATURES = {
     "pe_world_profile": (ctypes.c_int, [_P, ctypes.c_int]),
     "pe_world_kernel_time": (ctypes.c_int, [_P, _DP, _I64P]),
     "pe_world_destroy": (ctypes.c_int, [_P]),
+    "pe_semilag_dt": (ctypes.c_int, [ctypes.POINTER(SemiLagParams), _DP]),
+    "pe_semilag_create": (ctypes.c_int, [ctypes.POINTER(SemiLagParams),
+                                         ctypes.POINTER(ctypes.c_void_p)]),
+    "pe_semilag_init": (ctypes.c_int, [_P, _P]),
+    "pe_semilag_backup": (ctypes.c_int, [_P, ctypes.c_int]),
+    "pe_semilag_iterate": (ctypes.c_int, [_P, ctypes.c_int64, ctypes.c_double,
+                                          ctypes.c_int32, _I64P, _DP,
+                                          ctypes.POINTER(ctypes.c_int32)]),
+    "pe_semilag_residual": (ctypes.c_int, [_P, _DP]),
+    "pe_semilag_copy_value": (ctypes.c_int, [_P, _P]),
+    "pe_semilag_copy_policy": (ctypes.c_int, [_P, _P, _P]),
+    "pe_semilag_device_value": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_void_p)]),
+    "pe_semilag_iterations": (ctypes.c_int, [_P, _I64P]),
+    "pe_semilag_set_stream": (ctypes.c_int, [_P, _P]),
+    "pe_semilag_profile": (ctypes.c_int, [_P, ctypes.c_int]),
+    "pe_semilag_kernel_time": (ctypes.c_int, [_P, _DP, _I64P]),
+    "pe_semilag_destroy": (ctypes.c_int, [_P]),
 }
 
 _lib = None

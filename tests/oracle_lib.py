@@ -86,6 +86,7 @@ class Oracle:
             "po_sl_interpolate": (ctypes.c_double, [_P, _P, _P]),
             "po_sl_backup": (ctypes.c_int, [_P, _P, _P, _P, _P]),
             "po_sl_init": (None, [_P, _P]),
+            "po_sl_backup_cells": (None, [_P, _P, ctypes.c_size_t, _P, _P, _P, _P]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(lib, name)
@@ -203,6 +204,18 @@ class Oracle:
                                    None if pe is None else pe.ctypes.data)
         assert rc == 0, rc
         return (out, pp, pe) if with_policy else out
+
+    def sl_backup_cells(self, cfg, V, cells):
+        """Backup of the listed flat cells only: (values, policy_p, policy_e)."""
+        V = np.ascontiguousarray(V, dtype=np.float64)
+        cells = np.ascontiguousarray(cells, dtype=np.int64)
+        out = np.zeros(len(cells))
+        pp = np.zeros(len(cells), np.uint8)
+        pe = np.zeros(len(cells), np.uint8)
+        self.lib.po_sl_backup_cells(ctypes.addressof(cfg), V.ctypes.data, len(cells),
+                                    cells.ctypes.data, out.ctypes.data,
+                                    pp.ctypes.data, pe.ctypes.data)
+        return out, pp, pe
 
     def rect_separation(self, p, e, p_body, e_body):
         return self.lib.po_rect_separation(p[0], p[1], p[2], e[0], e[1], e[2],

@@ -1,0 +1,133 @@
+"""Semi-Lagrangian min-max backup on the GPU (float32) against the FP64
+oracle: values within float rounding, optimal action indices equal except
+at ties, convergence of the minimum-time value iteration, warm starts, and
+full-size properties on the 89M-cell grid."""
+
+import numpy as np
+import pytest
+
+from pursuit_evasion_b200 import _native
+from pursuit_evasion_b200.reversible.free_dp import RelativeGrid
+from pursuit_evasion_b200.reversible.semilag import (
+    SemiLagrangianSolver,
+    capture_time,
+    interpolation_cfl_dt,
+)
+from tests import oracle_lib
+from tests.helpers import A3, CONFIG1_GRID, CONFIG2_GRID
+
+pytestmark = pytest.mark.gpu
+
+# float32 value arithmetic vs the FP64 oracle, per backup
+VALUE_ATOL = 2e-5
+# an action index may differ only where the oracle's two candidates are
+# this close (a tie within float rounding)
+TIE_ATOL = 2e-4
+
+
+def oracle_worst(oracle, cfg, V, cell, grid):
+    """Per pursuer action, the max over evader actions (FP64) at one cell."""
+    iv, ie, ip, iy, ix = np.unravel_index(cell, grid.shape)
+    axes = grid.axes(A3)
+    state = (axes[4][ix], axes[3][iy], axes[2][ip], axes[0][iv], axes[1][ie])
+    worst = []
+    for up in range(9):
+        vals = [oracle.sl_interpolate(cfg, V, oracle.sl_successor(cfg, state, up, ue))
+                for ue in range(9)]
+        if cfg.mode == oracle_lib.SL_MINTIME:
+            vals = np.clip(vals, 0, 1)
+        worst.append(max(vals))
+    return np.array(worst)
+
+
+@pytest.mark.parametrize("mode", ["tube", "min_time"])
+def test_single_backup_matches_oracle(oracle, mode):
+    grid = RelativeGrid(13, 12, 7, 7, 3.0)
+    dt = interpolation_cfl_dt(A3, grid)
+    omode = oracle_lib.SL_TUBE if mode == "tube" else oracle_lib.SL_MINTIME
+    cfg = oracle.sl_cfg(A3, grid, dt, omode)
+    rng = np.random.default_rng(5)
+    if mode == "tube":
+        V = oracle.sl_init(cfg, grid.states) + 0.05 * rng.normal(size=grid.states)
+    else:
+        V = rng.uniform(0, 1, grid.states)
+    V32 = V.astype(np.float32)
+    ref, pp, pe = oracle.sl_backup(cfg, V32.astype(np.float64), with_policy=True)
+    with SemiLagrangianSolver(A3, grid, dt=dt, mode=mode) as s:
+        s.initialize(V32)
+        s.backup(with_policy=True)
+        got = s.value().ravel()
+        gp, ge = (a.ravel() for a in s.policy())
+    np.testing.assert_allclose(got, ref, atol=VALUE_ATOL, rtol=0)
+    mismatch = np.flatnonzero(gp != pp)
+    assert len(mismatch) < 0.01 * grid.states
+    for cell in mismatch[:200]:
+        worst = oracle_worst(oracle, cfg, V32.astype(np.float64), cell, grid)
+        assert abs(worst[gp[cell]] - worst[pp[cell]]) <= TIE_ATOL
+    # evader indices agree wherever the pursuer indices do, up to ties
+    same = gp == pp
+    assert np.mean(ge[same] == pe[same]) > 0.98
+
+
+def test_tube_backups_are_monotone_and_track_oracle(oracle):
+    grid = CONFIG1_GRID
+    dt = interpolation_cfl_dt(A3, grid)
+    cfg = oracle.sl_cfg(A3, grid, dt, oracle_lib.SL_TUBE)
+    V = oracle.sl_init(cfg, grid.states)
+    with SemiLagrangianSolver(A3, grid, dt=dt, mode="tube") as s:
+        s.initialize()
+        first = s.value().ravel().copy()
+        np.testing.assert_array_equal(first, V.astype(np.float32))
+        for _ in range(4):
+            V = oracle.sl_backup(cfg, V)
+        iters, residual, _ = s.iterate(4, tol=0.0)
+        got = s.value().ravel()
+    assert iters == 4
+    assert np.all(got <= first)
+    np.testing.assert_allclose(got, V, atol=4 * VALUE_ATOL, rtol=0)
+
+
+def test_min_time_iteration_converges_and_warm_start_is_a_fixed_point(oracle):
+    grid = RelativeGrid(11, 8, 5, 5, 3.0)
+    dt = 0.1
+    cfg = oracle.sl_cfg(A3, grid, dt, oracle_lib.SL_MINTIME)
+    with SemiLagrangianSolver(A3, grid, dt=dt, mode="min_time") as s:
+        s.initialize()
+        iters, residual, converged = s.iterate(2000, tol=1e-5, check_every=1)
+        u = s.value().ravel().copy()
+    assert converged and residual < 1e-5
+    # the oracle, started from the GPU's converged field, barely moves it
+    step = oracle.sl_backup(cfg, u.astype(np.float64))
+    assert np.abs(step - u).max() < 5e-5
+    # captured cells hold 0, capture times are finite and positive elsewhere
+    T = capture_time(u)
+    assert np.all(T[u == 0] == 0)
+    assert np.isfinite(T).mean() > 0.5
+    # a warm start at the fixed point converges at once
+    with SemiLagrangianSolver(A3, grid, dt=dt, mode="min_time") as s:
+        s.initialize(u)
+        iters2, residual2, converged2 = s.iterate(50, tol=1e-5, check_every=1)
+    assert converged2 and iters2 <= 2
+
+
+def test_full_size_backup_spot_checks(oracle):
+    """89,434,800 cells, one tube backup: 400 sampled cells against the FP64
+    oracle, monotone, finite, policy recorded."""
+    grid = CONFIG2_GRID
+    dt = interpolation_cfl_dt(A3, grid)
+    cfg = oracle.sl_cfg(A3, grid, dt, oracle_lib.SL_TUBE)
+    launches = _native.launch_count()
+    with SemiLagrangianSolver(A3, grid, dt=dt, mode="tube") as s:
+        s.initialize()
+        v0 = s.value().ravel().copy()
+        s.backup(with_policy=True)
+        v1 = s.value().ravel()
+        gp, _ = s.policy()
+    assert _native.launch_count() - launches >= 2
+    assert np.isfinite(v1).all() and np.all(v1 <= v0)
+    rng = np.random.default_rng(8)
+    cells = rng.choice(grid.states, size=400, replace=False)
+    ref, pp, _ = oracle.sl_backup_cells(cfg, v0.astype(np.float64), cells)
+    np.testing.assert_allclose(v1[cells], ref, atol=VALUE_ATOL, rtol=0)
+    agree = np.mean(gp.ravel()[cells] == pp)
+    assert agree > 0.95
