@@ -267,6 +267,89 @@ def run_reference_arm(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def world8d_section(steps=200):
+    """The 8D contact game step (config 4): 11^4 positions, 9^2 headings, 7^2
+    speeds (58,110,129 cells), a3 limits, 0.5 x 0.3 m footprints, CFL 0.8,
+    `steps` RK2 steps from the rectangle-contact field; device time."""
+    import torch
+    from pursuit_evasion_b200.reversible.world_dp import WorldGrid, WorldSolver
+
+    grid = WorldGrid(11, 9, 7, 7, 3.0)
+    with WorldSolver(a3_config(), grid, avoid=False) as s:
+        stream = torch.cuda.current_stream()
+        s.set_stream(stream.cuda_stream)
+        s.init_contact((0.5, 0.3), (0.5, 0.3))
+        for _ in range(3):
+            s.step(s.dt_limit)
+        s.init_contact((0.5, 0.3), (0.5, 0.3))
+        s.synchronize()
+        s.profile(True)
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        for _ in range(steps):
+            s.step(s.dt_limit)
+        t1.record(stream)
+        s.synchronize()
+        ms = t0.elapsed_time(t1)
+        kms, launches = s.kernel_time()
+        s.profile(False)
+        residual = s.residual()
+    cells = grid.states
+    peak, _ = measured_peaks()
+    achieved = (8 * cells + 12 * cells) * steps / (kms / 1e3) / 1e9
+    return {"workload": "world8d_contact WorldGrid(11,9,7,7,3.0) a3, 0.5x0.3 m bodies, "
+                        f"CFL 0.8, {steps} RK2 steps, float32 exact order",
+            "cells": cells, "value": cells * 2 * steps / (ms / 1e3),
+            "unit": METRIC, "ms_per_rk2_step": ms / steps,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak},
+            "last_residual": residual}
+
+
+def semilag_section(backups=5):
+    """Relative 5D semi-Lagrangian min-max backups on the 89M-cell grid
+    (tube functional, interpolation-CFL dt): device time per backup."""
+    import torch
+    from pursuit_evasion_b200.reversible.free_dp import RelativeGrid
+    from pursuit_evasion_b200.reversible.semilag import SemiLagrangianSolver
+
+    grid = RelativeGrid(**GRID)
+    with SemiLagrangianSolver(a3_config(), grid, mode="tube") as s:
+        stream = torch.cuda.current_stream()
+        s.set_stream(stream.cuda_stream)
+        s.initialize()
+        s.backup()
+        s.initialize()
+        s.profile(True)
+        s.iterate(backups, tol=0.0, check_every=backups)
+        ms, n = s.kernel_time()
+        s.profile(False)
+        dt = s.dt
+    cells = grid.states
+    peak, _ = measured_peaks()
+    achieved = 8 * cells * n / (ms / 1e3) / 1e9
+    return {"workload": f"semilag5d tube RelativeGrid(65,48,21,21,8.0) a3, dt {dt:.5f} s "
+                        "(interpolation CFL), 9x9 actions, value-only backups",
+            "cells": cells, "value": cells * n / (ms / 1e3), "unit": METRIC,
+            "ms_per_backup": ms / n,
+            "roofline": {"bound": "hbm (gather/FP32-issue bound in practice)",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak}}
+
+
+def converge_section(samples, epochs):
+    """Time to a converged minimum-time table (tol 1e-5): plain vs learned
+    warm start, on the 89M-cell grid with dt = 0.05 s."""
+    from pursuit_evasion_b200.learned.warm_start import time_to_converged
+    from pursuit_evasion_b200.reversible.free_dp import RelativeGrid
+
+    grid = RelativeGrid(**GRID)
+    coarse = RelativeGrid(33, 24, 11, 11, GRID["extent"])
+    result, _ = time_to_converged(a3_config(), grid, dt=0.05, tol=1e-5, samples=samples,
+                                  epochs=epochs, batch=8192, coarse_grid=coarse)
+    return result
+
+
 def run_ours(args, world, rank, local):
     import torch
 
@@ -399,6 +482,17 @@ def run_ours(args, world, rank, local):
         }
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline()
+        if not args.no_sections:
+            for key, fn in (("world8d", world8d_section), ("semilag5d", semilag_section)):
+                try:
+                    line[key] = fn()
+                except Exception as exc:  # report, keep the headline line
+                    line[key] = {"error": repr(exc)}
+            if args.converge:
+                try:
+                    line["converged"] = converge_section(args.samples, args.epochs)
+                except Exception as exc:
+                    line["converged"] = {"error": repr(exc)}
         print(json.dumps(line), flush=True)
     solver.close()
     if world > 1:
@@ -416,6 +510,12 @@ def main():
     parser.add_argument("--precision", choices=["float32", "float64"],
                         default="float32")
     parser.add_argument("--no-cpu-baseline", action="store_true")
+    parser.add_argument("--no-sections", action="store_true",
+                        help="skip the 8D and semi-Lagrangian side measurements")
+    parser.add_argument("--converge", action=argparse.BooleanOptionalAction, default=True,
+                        help="time-to-converged table, plain vs learned warm start")
+    parser.add_argument("--samples", type=int, default=1 << 22)
+    parser.add_argument("--epochs", type=int, default=20)
     args = parser.parse_args()
     # At least three warm-up solves are always run.
     args.warmup = max(args.warmup, 3)

@@ -232,6 +232,9 @@ int pe_semilag_create(const pe_semilag_params *params, pe_semilag **out);
 /* initial == NULL: TUBE hypot(x,y) - r; MINTIME 0 in the capture disk, 1
  * elsewhere.  Otherwise a dense host field (a warm start). */
 int pe_semilag_init(pe_semilag *h, const float *initial);
+/* Initialise from a dense field already on the handle's device (e.g. the
+ * learned surrogate's prediction). */
+int pe_semilag_init_device(pe_semilag *h, const float *device_initial);
 /* One backup sweep; with_policy != 0 also records the optimal pursuer and
  * evader action indices (catalogue order 3*i_a + i_k) of every cell. */
 int pe_semilag_backup(pe_semilag *h, int with_policy);
@@ -243,6 +246,8 @@ int pe_semilag_iterate(pe_semilag *h, int64_t max_iterations, double tol,
                        double *residual, int32_t *converged);
 int pe_semilag_residual(pe_semilag *h, double *residual);
 int pe_semilag_copy_value(pe_semilag *h, float *host_value);
+/* Copy the value field into a dense device array on the handle's device. */
+int pe_semilag_copy_value_device(pe_semilag *h, float *device_value);
 int pe_semilag_copy_policy(pe_semilag *h, uint8_t *host_p, uint8_t *host_e);
 int pe_semilag_device_value(pe_semilag *h, float **device_value);
 int pe_semilag_iterations(const pe_semilag *h, int64_t *iterations);
@@ -250,6 +255,67 @@ int pe_semilag_set_stream(pe_semilag *h, void *cuda_stream);
 int pe_semilag_profile(pe_semilag *h, int enable);
 int pe_semilag_kernel_time(pe_semilag *h, double *total_ms, int64_t *launches);
 int pe_semilag_destroy(pe_semilag *h);
+
+/* ------------------------------------------------------------------------
+ * Learned value surrogate: BF16 tensor-core MLP kernels.
+ *
+ * The reference has no learned warm start for the game tables; the closest
+ * precedent is its SiLU MLP value heads trained by supervised MSE on DP
+ * labels with Adam(W) (pe/local_game/learning.py:14-77 ContactValueNet,
+ * pe/local_game/training.py:39 fit_contact_values, :185-186 optimiser,
+ * :352 loss).  These building blocks run a features -> 4 x 256 SiLU -> 1
+ * network in BF16 with FP32 accumulation and FP32 master weights; the host
+ * side (pursuit_evasion_b200/learned) chains them into training steps that
+ * are captured in one CUDA graph.  Every pointer is a device pointer; bf16
+ * arrays are passed as void*.  All calls are asynchronous on cuda_stream.
+ * ------------------------------------------------------------------------ */
+
+/* C = A x B.  a_mmajor: A stored [K][M] (else [M][K]); b_nmajor: B stored
+ * [K][N] (else [N][K]).  epilogue 0: C32 = acc; 1: C32 = acc + bias (C32 may
+ * be NULL), C16 = bf16(silu(acc + bias)); 2: C32 += acc, split-K over
+ * `splits` CTAs (C32 pre-zeroed); 3: C16 = bf16(acc * silu'(zpre)).
+ * M, N multiples of 128, K a multiple of 32 * splits. */
+int pe_mlp_gemm(const void *A, const void *B, int M, int N, int K, int lda, int ldb,
+                int a_mmajor, int b_nmajor, int epilogue, int splits, float *C32,
+                void *C16, int ldc, const float *bias, const float *zpre,
+                void *cuda_stream);
+/* Adam on n FP32 master weights w (w16, if not NULL, receives their bf16
+ * copy).  corr[0], corr[1] are the bias corrections 1 - beta^t read on the
+ * device, so a captured graph replays with the current step. */
+int pe_mlp_adam(float *w, void *w16, const float *grad, float *m, float *v, int64_t n,
+                float lr, float beta1, float beta2, float eps, const float *corr,
+                float grad_scale, void *cuda_stream);
+/* Output head y = h . w + b over bf16 activations h [rows][width]; with a
+ * target also dy = 2 (y - target) / rows and loss += mean squared error. */
+int pe_mlp_head_forward(const void *h, const float *w, const float *b,
+                        const float *target, float *y, float *dy, float *loss,
+                        int rows, int width, void *cuda_stream);
+/* Head gradients dw, db and dz = dy w * silu'(zprev) (bf16) for the last
+ * hidden layer. */
+int pe_mlp_head_backward(const void *h, const float *zprev, const float *w,
+                         const float *dy, float *dw, float *db, void *dz, int rows,
+                         int width, void *cuda_stream);
+/* out[c] = sum over rows of bf16 x[row][c] (bias gradients). */
+int pe_mlp_colsum(const void *x, float *out, int rows, int cols, void *cuda_stream);
+/* Features of relative 5D grid nodes (flat [vP, vE, psi, y, x] indices idx)
+ * into bf16 rows of width ld (x, y, cos psi, sin psi, vP, vE scaled to
+ * [-1, 1]); with a table also target[i] = table[idx[i]]. */
+int pe_mlp_encode_relative_nodes(const float *table, const int64_t *idx, int n,
+                                 int positions, int headings, int p_speeds,
+                                 int e_speeds, double extent, double p_min,
+                                 double p_max, double e_min, double e_max, void *feat,
+                                 int ld, float *target, void *cuda_stream);
+/* Features of arbitrary relative states [n][5] = (x, y, psi, vP, vE). */
+int pe_mlp_encode_relative_states(const float *states, int n, double extent,
+                                  double p_min, double p_max, double e_min,
+                                  double e_max, void *feat, int ld, void *cuda_stream);
+/* Features of 8D grid nodes [xP, yP, thP, vP, xE, yE, thE, vE] (10 columns:
+ * positions, cos/sin of both headings, both speeds). */
+int pe_mlp_encode_world_nodes(const float *table, const int64_t *idx, int n,
+                              int positions, int headings, int p_speeds, int e_speeds,
+                              double extent, double p_min, double p_max, double e_min,
+                              double e_max, void *feat, int ld, float *target,
+                              void *cuda_stream);
 
 #ifdef __cplusplus
 }

@@ -311,6 +311,20 @@ int pe_semilag_init(pe_semilag *h, const float *initial) {
   return PE_OK;
 }
 
+int pe_semilag_init_device(pe_semilag *h, const float *device_initial) {
+  int rc = enter(h);
+  if (rc) return rc;
+  if (!device_initial) return fail(PE_EINVAL, "device_initial is NULL");
+  PE_CUDA_TRY(cudaMemsetAsync(h->stats, 0, sizeof(pe::SLStats), h->stream));
+  PE_CUDA_TRY(cudaMemcpyAsync(h->a, device_initial, sizeof(float) * (size_t)h->g.n,
+                              cudaMemcpyDeviceToDevice, h->stream));
+  PE_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  h->iterations = 0;
+  h->initialized = true;
+  h->policy_valid = false;
+  return PE_OK;
+}
+
 int pe_semilag_backup(pe_semilag *h, int with_policy) {
   int rc = enter(h);
   if (rc) return rc;
@@ -364,6 +378,15 @@ int pe_semilag_copy_value(pe_semilag *h, float *host_value) {
   if (!host_value) return fail(PE_EINVAL, "host_value is NULL");
   PE_CUDA_TRY(cudaMemcpyAsync(host_value, h->a, sizeof(float) * (size_t)h->g.n,
                               cudaMemcpyDeviceToHost, h->stream));
+  return read_stats(h);
+}
+
+int pe_semilag_copy_value_device(pe_semilag *h, float *device_value) {
+  int rc = enter(h);
+  if (rc) return rc;
+  if (!device_value) return fail(PE_EINVAL, "device_value is NULL");
+  PE_CUDA_TRY(cudaMemcpyAsync(device_value, h->a, sizeof(float) * (size_t)h->g.n,
+                              cudaMemcpyDeviceToDevice, h->stream));
   return read_stats(h);
 }
 

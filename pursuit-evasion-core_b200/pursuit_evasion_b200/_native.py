@@ -166,12 +166,14 @@ SIGNATURES = {
     "pe_semilag_create": (ctypes.c_int, [ctypes.POINTER(SemiLagParams),
                                          ctypes.POINTER(ctypes.c_void_p)]),
     "pe_semilag_init": (ctypes.c_int, [_P, _P]),
+    "pe_semilag_init_device": (ctypes.c_int, [_P, _P]),
     "pe_semilag_backup": (ctypes.c_int, [_P, ctypes.c_int]),
     "pe_semilag_iterate": (ctypes.c_int, [_P, ctypes.c_int64, ctypes.c_double,
                                           ctypes.c_int32, _I64P, _DP,
                                           ctypes.POINTER(ctypes.c_int32)]),
     "pe_semilag_residual": (ctypes.c_int, [_P, _DP]),
     "pe_semilag_copy_value": (ctypes.c_int, [_P, _P]),
+    "pe_semilag_copy_value_device": (ctypes.c_int, [_P, _P]),
     "pe_semilag_copy_policy": (ctypes.c_int, [_P, _P, _P]),
     "pe_semilag_device_value": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_void_p)]),
     "pe_semilag_iterations": (ctypes.c_int, [_P, _I64P]),
@@ -179,6 +181,20 @@ SIGNATURES = {
     "pe_semilag_profile": (ctypes.c_int, [_P, ctypes.c_int]),
     "pe_semilag_kernel_time": (ctypes.c_int, [_P, _DP, _I64P]),
     "pe_semilag_destroy": (ctypes.c_int, [_P]),
+    "pe_mlp_gemm": (ctypes.c_int, [_P, _P] + [ctypes.c_int] * 9 + [_P, _P, ctypes.c_int,
+                                                                   _P, _P, _P]),
+    "pe_mlp_adam": (ctypes.c_int, [_P, _P, _P, _P, _P, ctypes.c_int64, ctypes.c_float,
+                                   ctypes.c_float, ctypes.c_float, ctypes.c_float, _P,
+                                   ctypes.c_float, _P]),
+    "pe_mlp_head_forward": (ctypes.c_int, [_P] * 7 + [ctypes.c_int, ctypes.c_int, _P]),
+    "pe_mlp_head_backward": (ctypes.c_int, [_P] * 7 + [ctypes.c_int, ctypes.c_int, _P]),
+    "pe_mlp_colsum": (ctypes.c_int, [_P, _P, ctypes.c_int, ctypes.c_int, _P]),
+    "pe_mlp_encode_relative_nodes": (ctypes.c_int, [_P, _P] + [ctypes.c_int] * 5
+                                     + [ctypes.c_double] * 5 + [_P, ctypes.c_int, _P, _P]),
+    "pe_mlp_encode_relative_states": (ctypes.c_int, [_P, ctypes.c_int] + [ctypes.c_double] * 5
+                                      + [_P, ctypes.c_int, _P]),
+    "pe_mlp_encode_world_nodes": (ctypes.c_int, [_P, _P] + [ctypes.c_int] * 5
+                                  + [ctypes.c_double] * 5 + [_P, ctypes.c_int, _P, _P]),
 }
 
 _lib = None

@@ -1,0 +1,98 @@
+"""Learned warm start of minimum-time value iteration, and its evaluation.
+
+The plain DP is the reference and the judge: `time_to_converged` solves the
+relative 5D minimum-time game (semi-Lagrangian value iteration, a
+contraction) to a sup-norm residual `tol` from the cold start (u = 1 outside
+the capture disk) and again from a surrogate prediction, and reports the
+iterations, device seconds and the largest difference between the two
+converged tables.  The surrogate is trained by this package's kernels on
+node samples of a solver table: the same problem's table (an amortised
+re-solve) or a coarser grid's table (a multigrid-style cold path, whose cost
+includes that coarse solve and the training).
+"""
+
+from __future__ import annotations
+
+import time
+
+from ..reversible.free_dp import RelativeGrid
+from ..reversible.semilag import SemiLagrangianSolver
+from .mlp import ValueMLP
+from .train import RelativeNodeSampler, predict_nodes, train
+
+
+def converge(config, grid, *, dt, tol, initial=None, max_iterations=20000,
+             check_every=5, device=0):
+    """Minimum-time value iteration to residual < tol.  `initial`: optional
+    dense float32 torch tensor on the device.  Returns (u tensor, info)."""
+    import torch
+
+    dev = torch.device("cuda", device)
+    u = torch.empty(grid.states, device=dev)
+    with SemiLagrangianSolver(config, grid, dt=dt, mode="min_time", device=device) as s:
+        stream = torch.cuda.current_stream(dev)
+        s.set_stream(stream.cuda_stream)
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if initial is not None:
+            s.initialize_device(initial.data_ptr())
+        else:
+            s.initialize()
+        start.record(stream)
+        iters, residual, converged = s.iterate(max_iterations, tol=tol,
+                                               check_every=check_every)
+        end.record(stream)
+        s.value_to_device(u.data_ptr())
+        torch.cuda.synchronize(dev)
+        seconds = start.elapsed_time(end) / 1e3
+    return u, dict(iterations=iters, residual=residual, converged=converged,
+                   seconds=seconds)
+
+
+def surrogate_start(net, config, grid, out):
+    """Surrogate prediction on every node of `grid`, clamped to [0, 1]."""
+    import torch
+
+    predict_nodes(net, RelativeNodeSampler(config, grid), out)
+    out.clamp_(0.0, 1.0)
+    return out
+
+
+def time_to_converged(config, grid, *, dt, tol=1e-5, samples=1 << 22, epochs=20,
+                      batch=8192, coarse_grid=None, seed=0, device=0, log=None):
+    import torch
+
+    dev = torch.device("cuda", device)
+    result = {"grid": grid.to_dict(), "dt": dt, "tol": tol, "samples": samples,
+              "epochs": epochs, "batch": batch}
+    u_plain, plain = converge(config, grid, dt=dt, tol=tol, device=device)
+    result["plain"] = plain
+
+    def warm_from(table_grid, table, label):
+        net = ValueMLP(RelativeNodeSampler.in_features, seed=seed, device=device,
+                       max_batch=batch)
+        losses, train_s = train(net, RelativeNodeSampler(config, table_grid, table),
+                                samples=samples, epochs=epochs, batch=batch, seed=seed,
+                                log=log)
+        t0 = time.perf_counter()
+        u0 = surrogate_start(net, config, grid, torch.empty(grid.states, device=dev))
+        torch.cuda.synchronize(dev)
+        infer_s = time.perf_counter() - t0
+        surrogate_err = float((u0 - u_plain).abs().max())
+        u_warm, warm = converge(config, grid, dt=dt, tol=tol, initial=u0, device=device)
+        warm.update(train_seconds=train_s, final_mse=losses[-1], inference_seconds=infer_s,
+                    surrogate_max_abs_error=surrogate_err,
+                    max_abs_diff_vs_plain=float((u_warm - u_plain).abs().max()),
+                    speedup_iterations=plain["iterations"] / max(warm["iterations"], 1),
+                    speedup_seconds=plain["seconds"] / max(warm["seconds"], 1e-12))
+        result[label] = warm
+        return net
+
+    net = warm_from(grid, u_plain, "warm_same_table")
+    if coarse_grid is not None:
+        u_coarse, coarse = converge(config, coarse_grid, dt=dt, tol=tol, device=device)
+        warm_from(coarse_grid, u_coarse, "warm_coarse_table")
+        result["warm_coarse_table"]["coarse_solve"] = coarse
+        w = result["warm_coarse_table"]
+        w["end_to_end_seconds"] = (coarse["seconds"] + w["train_seconds"]
+                                   + w["inference_seconds"] + w["seconds"])
+    return result, net

@@ -93,6 +93,10 @@ class SemiLagrangianSolver:
             ptr = initial.ctypes.data
         _native.check(self._lib.pe_semilag_init(self._h, ptr))
 
+    def initialize_device(self, device_ptr):
+        """Initialise from a dense float32 field already on this device."""
+        _native.check(self._lib.pe_semilag_init_device(self._h, ctypes.c_void_p(device_ptr)))
+
     def backup(self, with_policy=False):
         _native.check(self._lib.pe_semilag_backup(self._h, int(with_policy)))
 
@@ -113,6 +117,11 @@ class SemiLagrangianSolver:
         out = np.empty(self.cells, np.float32) if out is None else out
         _native.check(self._lib.pe_semilag_copy_value(self._h, out.ctypes.data))
         return out.reshape(self.shape)
+
+    def value_to_device(self, device_ptr):
+        """Copy the value field into a dense float32 array on this device."""
+        _native.check(self._lib.pe_semilag_copy_value_device(self._h,
+                                                             ctypes.c_void_p(device_ptr)))
 
     def policy(self):
         p = np.empty(self.cells, np.uint8)

@@ -1,0 +1,120 @@
+"""Hand-written BF16 tensor-core MLP kernels (pe_mlp_*): GEMM layouts and
+epilogues against PyTorch fp32 matmuls of the same bf16 operands, and the
+forward/backward gradients against PyTorch CPU FP64 autograd on the same
+weights and inputs."""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+def gemm_case(a_mmajor, b_nmajor, epi, M=256, N=256, K=256, splits=1, seed=0):
+    from pursuit_evasion_b200.learned.mlp import ValueMLP
+
+    g = torch.Generator().manual_seed(seed)
+    A = torch.randn(M, K, generator=g).to(torch.bfloat16)
+    B = torch.randn(K, N, generator=g).to(torch.bfloat16)
+    bias = torch.randn(N, generator=g)
+    zpre = torch.randn(M, N, generator=g)
+    ref = A.float() @ B.float()
+    dev = torch.device("cuda", 0)
+    A_st = (A.t() if a_mmajor else A).contiguous().to(dev)   # [K][M] or [M][K]
+    B_st = (B if b_nmajor else B.t()).contiguous().to(dev)   # [K][N] or [N][K]
+    lda = M if a_mmajor else K
+    ldb = N if b_nmajor else K
+    C32 = torch.zeros(M, N, device=dev)
+    C16 = torch.zeros(M, N, dtype=torch.bfloat16, device=dev)
+    net = ValueMLP.__new__(ValueMLP)
+    from pursuit_evasion_b200 import _native
+    net.torch, net.lib, net.dev = torch, _native.library(), dev
+    net._gemm(A_st, B_st, M, N, K, lda, ldb, a_mmajor, b_nmajor, epi, splits=splits,
+              C32=C32 if epi in (0, 1, 2) else None,
+              C16=C16 if epi in (1, 3) else None, ldc=N,
+              bias=bias.to(dev) if epi == 1 else None,
+              zpre=zpre.to(dev) if epi == 3 else None)
+    torch.cuda.synchronize()
+    return ref, bias, zpre, C32.cpu(), C16.float().cpu()
+
+
+@pytest.mark.parametrize("a_mmajor", [False, True])
+@pytest.mark.parametrize("b_nmajor", [False, True])
+def test_gemm_layouts_store_fp32(a_mmajor, b_nmajor):
+    ref, _, _, C32, _ = gemm_case(a_mmajor, b_nmajor, 0)
+    torch.testing.assert_close(C32, ref, rtol=1e-4, atol=1e-3)
+
+
+def test_gemm_split_k_accumulates():
+    ref, _, _, C32, _ = gemm_case(True, True, 2, M=256, N=128, K=2048, splits=8)
+    torch.testing.assert_close(C32, ref, rtol=1e-4, atol=2e-3)
+
+
+def test_gemm_bias_silu_and_dsilu_epilogues():
+    ref, bias, _, C32, C16 = gemm_case(False, False, 1)
+    z = ref + bias
+    torch.testing.assert_close(C32, z, rtol=1e-4, atol=1e-3)
+    torch.testing.assert_close(C16, torch.nn.functional.silu(z), rtol=1e-2, atol=2e-2)
+    ref, _, zpre, _, C16 = gemm_case(False, True, 3)
+    s = torch.sigmoid(zpre)
+    torch.testing.assert_close(C16, ref * s * (1 + zpre * (1 - s)), rtol=1e-2, atol=5e-2)
+
+
+def test_gradients_match_fp64_autograd():
+    from pursuit_evasion_b200.learned.mlp import FEATURES, ValueMLP
+
+    rows = 512
+    net = ValueMLP(6, seed=3, max_batch=rows)
+    g = torch.Generator().manual_seed(1)
+    feat = torch.zeros(rows, FEATURES)
+    feat[:, :6] = torch.rand(rows, 6, generator=g) * 2 - 1
+    target = torch.sin(3 * feat[:, 0]) * feat[:, 1] + 0.5 * feat[:, 4]
+    net.feat.copy_(feat.to(torch.bfloat16))
+    net.target[:rows].copy_(target)
+    net.loss.zero_()
+    net.forward(rows, target=True)
+    net.backward(rows)
+    torch.cuda.synchronize()
+
+    # FP64 autograd on the same (bf16-rounded) weights and inputs
+    x = net.feat.double().cpu()
+    ws = [w.to(torch.bfloat16).double().cpu().requires_grad_() for w in net.w]
+    bs = [b.double().cpu().requires_grad_() for b in net.b]
+    wo = net.w_out.double().cpu().requires_grad_()
+    bo = net.b_out.double().cpu().requires_grad_()
+    h = x
+    for w, b in zip(ws, bs):
+        h = torch.nn.functional.silu(h @ w.t() + b)
+    y = h @ wo + bo
+    loss = ((y - target.double()) ** 2).mean()
+    loss.backward()
+    assert float(net.loss.cpu()) == pytest.approx(float(loss), rel=2e-2)
+    refs = [w.grad for w in ws] + [b.grad for b in bs] + [wo.grad, bo.grad]
+    for ours, ref in zip(net.grads, refs):
+        ours = ours.double().cpu().reshape(ref.shape)
+        rel = (ours - ref).norm() / max(ref.norm(), 1e-12)
+        cos = torch.nn.functional.cosine_similarity(ours.flatten(), ref.flatten(), dim=0)
+        assert rel < 5e-2 and cos > 0.998, (rel, cos)
+
+
+def test_training_reduces_loss():
+    from pursuit_evasion_b200.learned.mlp import FEATURES, ValueMLP
+
+    rows = 1024
+    net = ValueMLP(6, seed=0, max_batch=rows)
+    g = torch.Generator().manual_seed(2)
+    feat = torch.zeros(rows, FEATURES)
+    feat[:, :6] = torch.rand(rows, 6, generator=g) * 2 - 1
+    target = feat[:, 0] ** 2 + 0.5 * torch.cos(2 * feat[:, 1]) - 0.3 * feat[:, 5]
+    net.feat.copy_(feat.to(torch.bfloat16))
+    net.target.copy_(target)
+    losses = []
+    for step in range(1, 301):
+        net.loss.zero_()
+        net.forward(rows, target=True)
+        net.backward(rows)
+        net.set_step(step)
+        net.adam(lr=1e-3)
+        losses.append(float(net.loss.cpu()))
+    assert losses[-1] < 0.05 * losses[0]
