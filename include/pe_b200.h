@@ -147,6 +147,36 @@ int pe_relative_kernel_time(pe_relative *h, int stage, double *total_ms,
 /* Release device memory and the handle. */
 int pe_relative_destroy(pe_relative *h);
 
+/* One RK2 (or RK1, params->order) step of the relative 5D ENO/LF update on
+ * caller-owned device buffers, allocating no device memory.  This entry
+ * point has no counterpart in the reference.  It serves callers that cannot
+ * allocate once they run: a fixed-rate controller cannot afford
+ * cudaMalloc/cudaFree, which may synchronise the device, and a host
+ * application that owns all device memory through its own pool does not
+ * allow allocations behind its back.
+ *
+ * field_in, field_out, arrival: device arrays of pe_relative_cells() floats
+ * in the dense table layout [vP, vE, psi, y, x]; field_out receives the
+ * advanced field and arrival the first-crossing times (NaN where unset).
+ * t is the step's start time.  The arithmetic is the exact path, equal to a
+ * PE_LOCAL_F64 handle's step bit for bit.  *residual (may be NULL) receives
+ * max|field_out - field_in|.  The call synchronises `cuda_stream`.
+ *
+ * Scratch (the intermediate stage field, the heading tables, the reduction
+ * words) lives in one fixed __device__ array of about 16.8 MB that every
+ * GPU loading the library holds until exit; grids above
+ * PE_NOALLOC_MAX_CELLS cells or PE_NOALLOC_MAX_HEADINGS headings are
+ * rejected with PE_EINVAL.  The first call on a device looks up the
+ * array's device address; make that first call before any stream capture.
+ * All calls share the array: calls that overlap on the GPU (other streams,
+ * other host threads) race and must be serialised by the caller. */
+#define PE_NOALLOC_MAX_CELLS 4194304
+#define PE_NOALLOC_MAX_HEADINGS 1024
+int pe_relative_step_noalloc(const pe_relative_params *params,
+                             const float *field_in, float *field_out,
+                             float *arrival, double t, double dt,
+                             void *cuda_stream, double *residual);
+
 /* ------------------------------------------------------------------------
  * Dense 8D game [xP, yP, thP, vP, xE, yE, thE, vE] (vE fastest).
  *

@@ -144,6 +144,9 @@ SIGNATURES = {
     "pe_relative_profile": (ctypes.c_int, [_P, ctypes.c_int]),
     "pe_relative_kernel_time": (ctypes.c_int, [_P, ctypes.c_int, _DP, _I64P]),
     "pe_relative_destroy": (ctypes.c_int, [_P]),
+    "pe_relative_step_noalloc": (ctypes.c_int, [ctypes.POINTER(RelativeParams), _P, _P,
+                                                _P, ctypes.c_double, ctypes.c_double,
+                                                _P, _DP]),
     "pe_world_cells": (ctypes.c_int, [ctypes.POINTER(WorldParams), _I64P]),
     "pe_world_dt_limit": (ctypes.c_int, [ctypes.POINTER(WorldParams), _DP]),
     "pe_world_create": (ctypes.c_int, [ctypes.POINTER(WorldParams),
