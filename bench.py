@@ -358,6 +358,9 @@ def run_ours(args, world, rank, local):
     from pursuit_evasion_b200.reversible.relative_solver import RelativeSolver
 
     torch.cuda.set_device(local)
+    # A stream of our own: the solver handles run on it and the timing
+    # events are recorded on it (the legacy default stream would neither).
+    torch.cuda.set_stream(torch.cuda.Stream(device=local))
     if world > 1:
         import datetime
         import torch.distributed as dist

@@ -25,11 +25,7 @@ struct pe_relative {
   double t = 0;
   int64_t steps = 0;
   bool initialized = false;
-  bool profiling = false;
-  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending[2];
-  std::vector<cudaEvent_t> spare;
-  double prof_ms[2] = {0, 0};
-  int64_t prof_n[2] = {0, 0};
+  pe::LaunchTimer timer;  // per-stage launch times (pe_relative_profile)
 };
 
 namespace {
@@ -123,41 +119,7 @@ void release(pe_relative *h) {
   cudaFree(h->csf);
   cudaFree(h->stats);
   if (h->host_stats) cudaFreeHost(h->host_stats);
-  for (auto &list : h->pending)
-    for (auto &e : list) {
-      cudaEventDestroy(e.first);
-      cudaEventDestroy(e.second);
-    }
-  for (auto e : h->spare) cudaEventDestroy(e);
   if (h->own) cudaStreamDestroy(h->own);
-}
-
-cudaEvent_t take_event(pe_relative *h) {
-  if (!h->spare.empty()) {
-    cudaEvent_t e = h->spare.back();
-    h->spare.pop_back();
-    return e;
-  }
-  cudaEvent_t e = nullptr;
-  cudaEventCreate(&e);
-  return e;
-}
-
-// Sum the elapsed time of recorded stage launches (waits for them).
-int drain_profile(pe_relative *h) {
-  for (int s = 0; s < 2; s++) {
-    for (auto &pr : h->pending[s]) {
-      PE_CUDA_TRY(cudaEventSynchronize(pr.second));
-      float ms = 0;
-      PE_CUDA_TRY(cudaEventElapsedTime(&ms, pr.first, pr.second));
-      h->prof_ms[s] += ms;
-      h->prof_n[s] += 1;
-      h->spare.push_back(pr.first);
-      h->spare.push_back(pr.second);
-    }
-    h->pending[s].clear();
-  }
-  return PE_OK;
 }
 
 int launch_stage(pe_relative *h, int stage, const float *src, float *dst,
@@ -173,24 +135,14 @@ int launch_stage(pe_relative *h, int stage, const float *src, float *dst,
   s.dt = dt;
   s.t = h->t;
   s.stats = h->stats;
-  cudaEvent_t e0 = nullptr, e1 = nullptr;
-  if (h->profiling) {
-    e0 = take_event(h);
-    e1 = take_event(h);
-    PE_CUDA_TRY(cudaEventRecord(e0, h->stream));
-  }
+  cudaEvent_t e0 = h->timer.begin(h->stream);
   const cudaError_t err =
       h->p.precision == PE_LOCAL_F64
           ? pe::rel5_stage_f64(h->g, s, blend, h->stream)
           : pe::rel5_stage_f32(h->g, h->tile, s, blend, h->stream);
   if (err != cudaSuccess) return pe::cuda_fail(err, "relative stage launch");
   pe::count_launches(1);
-  if (h->profiling) {
-    PE_CUDA_TRY(cudaEventRecord(e1, h->stream));
-    h->pending[stage].push_back({e0, e1});
-    if (h->pending[stage].size() > 4096) return drain_profile(h);
-  }
-  return PE_OK;
+  return h->timer.end(h->stream, e0, stage);
 }
 
 int step_impl(pe_relative *h, double dt) {
@@ -483,12 +435,7 @@ int pe_relative_stats(pe_relative *h, double *residual, double *max_increase) {
 int pe_relative_profile(pe_relative *h, int enable) {
   int rc = enter(h);
   if (rc) return rc;
-  rc = drain_profile(h);
-  if (rc) return rc;
-  h->profiling = enable != 0;
-  h->prof_ms[0] = h->prof_ms[1] = 0;
-  h->prof_n[0] = h->prof_n[1] = 0;
-  return PE_OK;
+  return h->timer.reset(enable != 0);
 }
 
 int pe_relative_kernel_time(pe_relative *h, int stage, double *total_ms,
@@ -496,10 +443,10 @@ int pe_relative_kernel_time(pe_relative *h, int stage, double *total_ms,
   int rc = enter(h);
   if (rc) return rc;
   if (stage != 0 && stage != 1) return fail(PE_EINVAL, "stage must be 0 or 1");
-  rc = drain_profile(h);
+  rc = h->timer.harvest(true);
   if (rc) return rc;
-  if (total_ms) *total_ms = h->prof_ms[stage];
-  if (launches) *launches = h->prof_n[stage];
+  if (total_ms) *total_ms = h->timer.ms(stage);
+  if (launches) *launches = h->timer.launches(stage);
   return PE_OK;
 }
 

@@ -25,10 +25,7 @@ struct pe_semilag {
   cudaStream_t own = nullptr, stream = nullptr;
   int64_t iterations = 0;
   bool initialized = false, policy_valid = false;
-  bool profiling = false;
-  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending;
-  double prof_ms = 0;
-  int64_t prof_n = 0;
+  pe::LaunchTimer timer;  // launch times (profile / kernel_time)
 };
 
 namespace {
@@ -97,10 +94,6 @@ void release(pe_semilag *h) {
                     (void *)h->emove, (void *)h->stats})
     cudaFree(ptr);
   if (h->host_stats) cudaFreeHost(h->host_stats);
-  for (auto &e : h->pending) {
-    cudaEventDestroy(e.first);
-    cudaEventDestroy(e.second);
-  }
   if (h->own) cudaStreamDestroy(h->own);
 }
 
@@ -118,20 +111,6 @@ int read_stats(pe_semilag *h) {
   return PE_OK;
 }
 
-int drain(pe_semilag *h) {
-  for (auto &pr : h->pending) {
-    PE_CUDA_TRY(cudaEventSynchronize(pr.second));
-    float ms = 0;
-    PE_CUDA_TRY(cudaEventElapsedTime(&ms, pr.first, pr.second));
-    h->prof_ms += ms;
-    h->prof_n++;
-    cudaEventDestroy(pr.first);
-    cudaEventDestroy(pr.second);
-  }
-  h->pending.clear();
-  return PE_OK;
-}
-
 int backup(pe_semilag *h, bool policy) {
   PE_CUDA_TRY(cudaMemsetAsync(&h->stats->residual, 0, sizeof(unsigned long long),
                               h->stream));
@@ -144,21 +123,12 @@ int backup(pe_semilag *h, bool policy) {
   bk.earc = h->earc;
   bk.emove = h->emove;
   bk.stats = h->stats;
-  cudaEvent_t e0 = nullptr, e1 = nullptr;
-  if (h->profiling) {
-    PE_CUDA_TRY(cudaEventCreate(&e0));
-    PE_CUDA_TRY(cudaEventCreate(&e1));
-    PE_CUDA_TRY(cudaEventRecord(e0, h->stream));
-  }
+  cudaEvent_t e0 = h->timer.begin(h->stream);
   PE_CUDA_TRY(pe::sl_backup(h->g, bk, h->stream));
   pe::count_launches(1);
-  if (h->profiling) {
-    PE_CUDA_TRY(cudaEventRecord(e1, h->stream));
-    h->pending.push_back({e0, e1});
-    if (h->pending.size() > 4096) {
-      int rc = drain(h);
-      if (rc) return rc;
-    }
+  {
+    const int rc = h->timer.end(h->stream, e0, 0);
+    if (rc) return rc;
   }
   std::swap(h->a, h->b);
   h->iterations++;
@@ -426,21 +396,16 @@ int pe_semilag_set_stream(pe_semilag *h, void *cuda_stream) {
 int pe_semilag_profile(pe_semilag *h, int enable) {
   int rc = enter(h);
   if (rc) return rc;
-  rc = drain(h);
-  if (rc) return rc;
-  h->profiling = enable != 0;
-  h->prof_ms = 0;
-  h->prof_n = 0;
-  return PE_OK;
+  return h->timer.reset(enable != 0);
 }
 
 int pe_semilag_kernel_time(pe_semilag *h, double *total_ms, int64_t *launches) {
   int rc = enter(h);
   if (rc) return rc;
-  rc = drain(h);
+  rc = h->timer.harvest(true);
   if (rc) return rc;
-  if (total_ms) *total_ms = h->prof_ms;
-  if (launches) *launches = h->prof_n;
+  if (total_ms) *total_ms = h->timer.ms(0);
+  if (launches) *launches = h->timer.launches(0);
   return PE_OK;
 }
 

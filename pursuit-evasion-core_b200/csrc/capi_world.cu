@@ -22,10 +22,7 @@ struct pe_world {
   double t = 0;
   int64_t steps = 0;
   bool initialized = false;
-  bool profiling = false;
-  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending;
-  double prof_ms = 0;
-  int64_t prof_n = 0;
+  pe::LaunchTimer timer;  // launch times (profile / kernel_time)
 };
 
 namespace {
@@ -101,10 +98,6 @@ void release(pe_world *h) {
                     (void *)h->sdiff, (void *)h->stats})
     cudaFree(ptr);
   if (h->host_stats) cudaFreeHost(h->host_stats);
-  for (auto &e : h->pending) {
-    cudaEventDestroy(e.first);
-    cudaEventDestroy(e.second);
-  }
   if (h->own) cudaStreamDestroy(h->own);
 }
 
@@ -123,20 +116,6 @@ int read_stats(pe_world *h) {
   return PE_OK;
 }
 
-int drain(pe_world *h) {
-  for (auto &pr : h->pending) {
-    PE_CUDA_TRY(cudaEventSynchronize(pr.second));
-    float ms = 0;
-    PE_CUDA_TRY(cudaEventElapsedTime(&ms, pr.first, pr.second));
-    h->prof_ms += ms;
-    h->prof_n += 1;
-    cudaEventDestroy(pr.first);
-    cudaEventDestroy(pr.second);
-  }
-  h->pending.clear();
-  return PE_OK;
-}
-
 int stage(pe_world *h, const float *src, float *dst, const float *base, float dt) {
   pe::World8Stage s{};
   s.src = src;
@@ -151,20 +130,10 @@ int stage(pe_world *h, const float *src, float *dst, const float *base, float dt
   s.dt = dt;
   s.tau = h->t;
   s.stats = h->stats;
-  cudaEvent_t e0 = nullptr, e1 = nullptr;
-  if (h->profiling) {
-    PE_CUDA_TRY(cudaEventCreate(&e0));
-    PE_CUDA_TRY(cudaEventCreate(&e1));
-    PE_CUDA_TRY(cudaEventRecord(e0, h->stream));
-  }
+  cudaEvent_t e0 = h->timer.begin(h->stream);
   PE_CUDA_TRY(pe::world8_stage(h->g, s, h->stream));
   pe::count_launches(1);
-  if (h->profiling) {
-    PE_CUDA_TRY(cudaEventRecord(e1, h->stream));
-    h->pending.push_back({e0, e1});
-    if (h->pending.size() > 4096) return drain(h);
-  }
-  return PE_OK;
+  return h->timer.end(h->stream, e0, 0);
 }
 
 int step_impl(pe_world *h, double dt) {
@@ -409,21 +378,16 @@ int pe_world_set_stream(pe_world *h, void *cuda_stream) {
 int pe_world_profile(pe_world *h, int enable) {
   int rc = enter(h);
   if (rc) return rc;
-  rc = drain(h);
-  if (rc) return rc;
-  h->profiling = enable != 0;
-  h->prof_ms = 0;
-  h->prof_n = 0;
-  return PE_OK;
+  return h->timer.reset(enable != 0);
 }
 
 int pe_world_kernel_time(pe_world *h, double *total_ms, int64_t *launches) {
   int rc = enter(h);
   if (rc) return rc;
-  rc = drain(h);
+  rc = h->timer.harvest(true);
   if (rc) return rc;
-  if (total_ms) *total_ms = h->prof_ms;
-  if (launches) *launches = h->prof_n;
+  if (total_ms) *total_ms = h->timer.ms(0);
+  if (launches) *launches = h->timer.launches(0);
   return PE_OK;
 }
 

@@ -6,7 +6,9 @@
 #include <cstdarg>
 #include <cstdint>
 #include <cstdio>
+#include <deque>
 #include <string>
+#include <vector>
 
 #include "pe_b200.h"
 
@@ -23,6 +25,42 @@ int cuda_fail(cudaError_t err, const char *what);
 
 // Count of kernels this library has launched (pe_launch_count()).
 void count_launches(int64_t n);
+
+// Per-launch device time from CUDA event pairs recorded on the launching
+// stream, summed per slot (e.g. RK2 stage 1 / stage 2).  Finished pairs are
+// harvested without blocking once many are outstanding, so profiling adds
+// no host synchronisation to a long run unless the device falls more than
+// kHardCap launches behind.
+class LaunchTimer {
+ public:
+  static constexpr size_t kSoftCap = 1024, kHardCap = 65536;
+  static constexpr int kSlots = 2;
+
+  ~LaunchTimer();
+  // Event to record before the launch (nullptr when disabled).
+  cudaEvent_t begin(cudaStream_t stream);
+  // Record the end event after the launch and file the pair under `slot`.
+  int end(cudaStream_t stream, cudaEvent_t start, int slot);
+  // Sum finished pairs; wait_all waits for every outstanding pair.
+  int harvest(bool wait_all);
+  // Wait for outstanding pairs, zero the sums and switch on or off.
+  int reset(bool enable);
+  bool enabled() const { return enabled_; }
+  double ms(int slot) const { return ms_[slot]; }
+  int64_t launches(int slot) const { return n_[slot]; }
+
+ private:
+  struct Pair {
+    cudaEvent_t start, stop;
+    int slot;
+  };
+  cudaEvent_t take();
+  bool enabled_ = false;
+  double ms_[kSlots] = {0, 0};
+  int64_t n_[kSlots] = {0, 0};
+  std::deque<Pair> pending_;
+  std::vector<cudaEvent_t> spare_;
+};
 
 }  // namespace pe
 

@@ -118,6 +118,7 @@ def predict_nodes(net, sampler, out, *, chunk=8192):
     torch = net.torch
     dev = net.dev
     n = sampler.cells
+    chunk = min(chunk, net.batch)
     idx = torch.empty(chunk, dtype=torch.int64, device=dev)
     for start in range(0, n, chunk):
         rows = min(chunk, n - start)

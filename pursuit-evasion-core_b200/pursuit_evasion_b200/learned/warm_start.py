@@ -29,8 +29,12 @@ def converge(config, grid, *, dt, tol, initial=None, max_iterations=20000,
 
     dev = torch.device("cuda", device)
     u = torch.empty(grid.states, device=dev)
-    with SemiLagrangianSolver(config, grid, dt=dt, mode="min_time", device=device) as s:
-        stream = torch.cuda.current_stream(dev)
+    # the handle and the timing events share one explicit stream, ordered
+    # after the work that produced `initial`
+    stream = torch.cuda.Stream(device=dev)
+    stream.wait_stream(torch.cuda.current_stream(dev))
+    with SemiLagrangianSolver(config, grid, dt=dt, mode="min_time", device=device) as s, \
+            torch.cuda.stream(stream):
         s.set_stream(stream.cuda_stream)
         start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         if initial is not None:
