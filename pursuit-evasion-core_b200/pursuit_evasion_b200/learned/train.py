@@ -145,4 +145,4 @@ def predict_states(net, config, extent, states):
         float(e.speed_min), float(e.speed_max), _ptr(net.feat), FEATURES, net._stream()))
     if padded > n:
         net.feat[n:padded].zero_()
-    return net.forward(padded)[:n]
+    return net.forward(padded)[:n].clone()  # the network's output buffer is reused

@@ -82,9 +82,11 @@ def time_to_converged(config, grid, *, dt, tol=1e-5, samples=1 << 22, epochs=20,
         torch.cuda.synchronize(dev)
         infer_s = time.perf_counter() - t0
         surrogate_err = float((u0 - u_plain).abs().max())
+        surrogate_mean = float((u0 - u_plain).abs().mean())
         u_warm, warm = converge(config, grid, dt=dt, tol=tol, initial=u0, device=device)
         warm.update(train_seconds=train_s, final_mse=losses[-1], inference_seconds=infer_s,
                     surrogate_max_abs_error=surrogate_err,
+                    surrogate_mean_abs_error=surrogate_mean,
                     max_abs_diff_vs_plain=float((u_warm - u_plain).abs().max()),
                     speedup_iterations=plain["iterations"] / max(warm["iterations"], 1),
                     speedup_seconds=plain["seconds"] / max(warm["seconds"], 1e-12))
