@@ -178,6 +178,60 @@ int pe_relative_step_noalloc(const pe_relative_params *params,
                              void *cuda_stream, double *residual);
 
 /* ------------------------------------------------------------------------
+ * Batched relative 5D solves.
+ *
+ * Many independent free_dp-style solves -- each with its own RelativeGrid,
+ * physics and horizon -- advanced together: every RK2 step of every solve
+ * runs in ONE persistent cooperative kernel launch (recorded once in a
+ * CUDA graph), a grid-wide barrier between stages.  Each solve follows the
+ * reference executable's driver (native_relative.cpp:173-190, steps of
+ * min(cfl_limit, horizon - t)) from the capture field
+ * (native_relative.cpp:91-100); with the exact arithmetic its final field
+ * and arrival times equal a PE_LOCAL_F64 pe_relative handle's (and the
+ * reference executable's run with the same --horizon and --output-dt =
+ * horizon) bit for bit.  The reference has no batched mode: it runs such
+ * solves one executable at a time (free_dp.py:259-261).
+ * ------------------------------------------------------------------------ */
+typedef struct pe_batch pe_batch;
+
+/* params[i].order must be 2 and every solve must have the same precision:
+ * PE_LOCAL_F64 (the exact arithmetic, bit-identical per solve as above) or
+ * PE_LOCAL_F32 (a float32 cell update, within float rounding and ENO
+ * selection ties of the exact one).  params[i].device is ignored (the batch
+ * lives on `device`). */
+int pe_batch_create(const pe_relative_params *params, const double *horizons,
+                    int32_t count, int32_t device, pe_batch **out);
+/* Work-item tile of one solve: `rows` y rows of one (vP, vE, psi) plane.
+ * Results do not depend on the tile. */
+int pe_batch_set_tile(pe_batch *h, int32_t solve, int32_t rows);
+int pe_batch_get_tile(const pe_batch *h, int32_t solve, int32_t *rows);
+int pe_batch_set_stream(pe_batch *h, void *cuda_stream);
+/* Capture field and arrival of every solve at t = 0. */
+int pe_batch_init(pe_batch *h);
+/* All steps of all solves: one graph launch holding one cooperative kernel.
+ * Enqueues the work; init must precede every run. */
+int pe_batch_run(pe_batch *h);
+/* Wait; PE_ETIMEOUT if a barrier wait gave up, PE_ENONFINITE if any update
+ * was not finite. */
+int pe_batch_synchronize(pe_batch *h);
+/* Cells, RK2 steps to the horizon and the CFL step limit of one solve. */
+int pe_batch_solve_info(const pe_batch *h, int32_t solve, int64_t *cells,
+                        int64_t *steps, double *dt_limit);
+/* Dense [vP, vE, psi, y, x] field / arrival times of one solve (host). */
+int pe_batch_copy_field(pe_batch *h, int32_t solve, float *host_field);
+int pe_batch_copy_arrival(pe_batch *h, int32_t solve, float *host_arrival);
+/* Sup-norm change of the solve's last step and its largest increase. */
+int pe_batch_stats(pe_batch *h, int32_t solve, double *residual,
+                   double *max_increase);
+/* CTAs and threads of the persistent launch, the longest solve's steps and
+ * the batch's cell-stage updates per run (2 x cells x steps, summed). */
+int pe_batch_launch_info(const pe_batch *h, int32_t *ctas, int32_t *threads,
+                         int32_t *max_steps, int64_t *total_cell_stages);
+int pe_batch_profile(pe_batch *h, int enable);
+int pe_batch_kernel_time(pe_batch *h, double *total_ms, int64_t *launches);
+int pe_batch_destroy(pe_batch *h);
+
+/* ------------------------------------------------------------------------
  * Dense 8D game [xP, yP, thP, vP, xE, yE, thE, vE] (vE fastest).
  *
  * Replaces the reference executable native_world.cpp (argv options
@@ -282,6 +336,18 @@ int pe_semilag_copy_policy(pe_semilag *h, uint8_t *host_p, uint8_t *host_e);
 int pe_semilag_device_value(pe_semilag *h, float **device_value);
 int pe_semilag_iterations(const pe_semilag *h, int64_t *iterations);
 int pe_semilag_set_stream(pe_semilag *h, void *cuda_stream);
+/* Kernel of value-only backups.  PE_SL_KERNEL_TILED stages speed-blended
+ * heading planes of a tile in shared memory and prunes pursuer actions
+ * (needs positions + 4 <= 72 and successors within 1.99 cells and one
+ * heading plane, true at the interpolation-CFL dt); PE_SL_KERNEL_GENERIC
+ * gathers from global memory; PE_SL_KERNEL_AUTO (default) picks the tiled
+ * kernel where it applies and the grid gives at least 8 of its work items
+ * ((vP, vE) pairs x row tiles) per SM.  Backups that record the policy always use the
+ * generic kernel.  Both give the same values up to float rounding. */
+enum { PE_SL_KERNEL_AUTO = 0, PE_SL_KERNEL_GENERIC = 1, PE_SL_KERNEL_TILED = 2 };
+int pe_semilag_set_kernel(pe_semilag *h, int kernel);
+/* The kernel value-only backups use now (GENERIC or TILED). */
+int pe_semilag_kernel(const pe_semilag *h, int32_t *kernel);
 int pe_semilag_profile(pe_semilag *h, int enable);
 int pe_semilag_kernel_time(pe_semilag *h, double *total_ms, int64_t *launches);
 int pe_semilag_destroy(pe_semilag *h);

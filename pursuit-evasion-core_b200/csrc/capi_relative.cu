@@ -10,6 +10,7 @@
 
 #include "pe_internal.h"
 #include "relative5d.cuh"
+#include "relative5d_host.h"
 
 struct pe_relative {
   pe_relative_params p{};
@@ -31,82 +32,10 @@ struct pe_relative {
 namespace {
 
 using pe::fail;
+using pe::rel5host::cfl_limit;
+using pe::rel5host::make_grid;
+using pe::rel5host::validate;
 
-bool finite_all(std::initializer_list<double> values) {
-  for (double v : values)
-    if (!std::isfinite(v)) return false;
-  return true;
-}
-
-int validate(const pe_relative_params *p) {
-  if (!p) return fail(PE_EINVAL, "params is NULL");
-  if (p->positions < 3 || p->headings < 4 || p->p_speeds < 3 ||
-      p->e_speeds < 3)
-    return fail(PE_EINVAL,
-                "Invalid solver options: grid needs positions>=3, headings>=4, "
-                "speeds>=3");
-  if (p->order != 1 && p->order != 2)
-    return fail(PE_EINVAL, "Invalid solver options: order must be 1 or 2");
-  if (p->scheme != PE_SCHEME_ENO_LF)
-    return fail(PE_EINVAL, "Invalid solver options: unknown scheme %d",
-                p->scheme);
-  if (p->precision != PE_LOCAL_F32 && p->precision != PE_LOCAL_F64)
-    return fail(PE_EINVAL, "Invalid solver options: unknown precision %d",
-                p->precision);
-  if (!finite_all({p->extent, p->capture_radius, p->p_speed_min,
-                   p->p_speed_max, p->p_acceleration, p->p_curvature,
-                   p->e_speed_min, p->e_speed_max, p->e_acceleration,
-                   p->e_curvature, p->cfl}))
-    return fail(PE_EINVAL, "Invalid solver options: non-finite value");
-  if (p->extent <= p->capture_radius || p->capture_radius <= 0 ||
-      p->cfl <= 0 || p->cfl > 1 || p->p_acceleration <= 0 ||
-      p->e_acceleration <= 0 || p->p_curvature <= 0 || p->e_curvature <= 0 ||
-      p->p_speed_min >= p->p_speed_max || p->e_speed_min >= p->e_speed_max)
-    return fail(PE_EINVAL, "Invalid solver options");
-  if ((int64_t)p->p_speeds * p->e_speeds > 65535 || p->headings > 65535 ||
-      (int64_t)p->positions * p->positions > (1 << 30))
-    return fail(PE_EINVAL, "Invalid solver options: grid too large");
-  return PE_OK;
-}
-
-pe::Rel5Grid make_grid(const pe_relative_params *p) {
-  pe::Rel5Grid g{};
-  const double pi = std::acos(-1.0);
-  g.nx = p->positions;
-  g.nh = p->headings;
-  g.nvp = p->p_speeds;
-  g.nve = p->e_speeds;
-  g.order = p->order;
-  g.xp = (g.nx + 3) / 4 * 4;  // rows padded to 16 bytes
-  g.sy = g.xp;
-  g.sp = (int64_t)g.nx * g.xp;
-  g.se = g.sp * g.nh;
-  g.sv = g.se * g.nve;
-  g.n_padded = g.sv * g.nvp;
-  g.n = (int64_t)g.nx * g.nx * g.nh * g.nve * g.nvp;
-  g.extent = p->extent;
-  g.dx = 2 * p->extent / (p->positions - 1);
-  g.dphi = 2 * pi / p->headings;
-  g.dvp = (p->p_speed_max - p->p_speed_min) / (p->p_speeds - 1);
-  g.dve = (p->e_speed_max - p->e_speed_min) / (p->e_speeds - 1);
-  g.vp_lo = p->p_speed_min;
-  g.ve_lo = p->e_speed_min;
-  g.acc_p = p->p_acceleration;
-  g.acc_e = p->e_acceleration;
-  g.curv_p = p->p_curvature;
-  g.curv_e = p->e_curvature;
-  return g;
-}
-
-double cfl_limit(const pe_relative_params *p, const pe::Rel5Grid &g) {
-  const double VP = std::max(std::abs(p->p_speed_min), std::abs(p->p_speed_max));
-  const double VE = std::max(std::abs(p->e_speed_min), std::abs(p->e_speed_max));
-  const double rate = (VP + VE + VP * p->p_curvature * p->extent) / g.dx +
-                      (VE + VP * p->p_curvature * p->extent) / g.dx +
-                      (VP * p->p_curvature + VE * p->e_curvature) / g.dphi +
-                      p->p_acceleration / g.dvp + p->e_acceleration / g.dve;
-  return p->cfl / rate;
-}
 
 void release(pe_relative *h) {
   cudaFree(h->a);

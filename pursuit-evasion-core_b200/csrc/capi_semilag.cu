@@ -5,6 +5,7 @@
 // displacement in the pursuer frame for every heading, then drives the
 // min-max backups (semilag5d.cu) and the value-iteration loop with a
 // sup-norm stopping test.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -22,6 +23,13 @@ struct pe_semilag {
   pe::SLEvaderArc *earc = nullptr;
   pe::SLEvaderMove *emove = nullptr;
   pe::SLStats *stats = nullptr, *host_stats = nullptr;
+  // tiled value-only kernel (semilag5d_tiled.cu), when the grid allows it
+  pe::SLSpeedStep *pstep = nullptr, *estep = nullptr;
+  uint8_t *hint = nullptr;
+  pe::SLTiledPlan plan{};
+  bool tiled_ok = false;    // the tiled kernel applies to this grid and dt
+  bool tiled_auto = false;  // ... and has enough work items to be the faster one
+  int kernel = PE_SL_KERNEL_AUTO;
   cudaStream_t own = nullptr, stream = nullptr;
   int64_t iterations = 0;
   bool initialized = false, policy_valid = false;
@@ -49,6 +57,58 @@ void chord_turn(double d, double k, double *chord, double *turn) {
   const double t = k * d, half = 0.5 * t;
   *turn = t;
   *chord = std::fabs(half) < 1e-12 ? d : d * std::sin(half) / half;
+}
+
+// Speed interpolation steps of one car (SLSpeedStep) from its arc table
+// fv[level * 9 + action]; false if a successor leaves the three slabs
+// around its level or the speed depends on the steering.
+template <typename Arc>
+bool speed_steps(const std::vector<Arc> &arc, int levels, std::vector<pe::SLSpeedStep> *out) {
+  out->resize(levels);
+  for (int lv = 0; lv < levels; lv++) {
+    pe::SLSpeedStep &st = (*out)[lv];
+    st.base = std::min(std::max(lv - 1, 0), levels - 3);
+    for (int a = 0; a < 3; a++) {
+      const float fv = arc[lv * 9 + 3 * a + 1].fv;
+      if (arc[lv * 9 + 3 * a].fv != fv || arc[lv * 9 + 3 * a + 2].fv != fv) return false;
+      int j = (int)std::floor(fv);
+      j = std::min(std::max(j, 0), levels - 2);
+      const int slot = j - st.base;
+      if (slot < 0 || slot > 1) return false;
+      st.slot[a] = slot;
+      st.w[a] = fv - (float)j;
+    }
+  }
+  return true;
+}
+
+// The tiled kernel stages two halo cells around a tile and one heading
+// plane on each side: every successor must stay within 1.99 cells in x and
+// y and below one heading spacing.  The displacement is affine in the cell
+// position, so its extremes sit at the corners of the position box.
+bool tiled_geometry_ok(const pe::SLGrid &g, const std::vector<pe::SLPursuerArc> &parc,
+                       const std::vector<pe::SLEvaderArc> &earc,
+                       const std::vector<pe::SLEvaderMove> &emove) {
+  const double center = 0.5 * (g.nx - 1), ihx = g.ihx;
+  double reach = 0, turn = 0;
+  for (int iv = 0; iv < g.nvp; iv++)
+    for (int up = 0; up < 9; up++) {
+      const pe::SLPursuerArc &pa = parc[iv * 9 + up];
+      const double rot = (std::fabs(pa.c - 1.0) + std::fabs(pa.s)) * center;
+      for (int ie = 0; ie < g.nve; ie++)
+        for (int ue = 0; ue < 9; ue++) {
+          turn = std::max(turn, std::fabs((double)earc[ie * 9 + ue].turn_idx -
+                                          (double)pa.turn_idx));
+          for (int ip = 0; ip < g.nh; ip++) {
+            const pe::SLEvaderMove &em = emove[((size_t)ip * g.nve + ie) * 9 + ue];
+            const double dxp = (double)em.ex - pa.px, dyp = (double)em.ey - pa.py;
+            const double ox = std::fabs(pa.c * dxp + pa.s * dyp) * ihx;
+            const double oy = std::fabs(pa.c * dyp - pa.s * dxp) * ihx;
+            reach = std::max(reach, rot + std::max(ox, oy));
+          }
+        }
+    }
+  return reach <= 1.99 && turn < 0.999;
 }
 
 int validate(const pe_semilag_params *p) {
@@ -91,7 +151,8 @@ double interpolation_cfl_dt(const pe_semilag_params *p) {
 void release(pe_semilag *h) {
   for (void *ptr : {(void *)h->a, (void *)h->b, (void *)h->plane, (void *)h->pol_p,
                     (void *)h->pol_e, (void *)h->parc, (void *)h->earc,
-                    (void *)h->emove, (void *)h->stats})
+                    (void *)h->emove, (void *)h->stats, (void *)h->pstep,
+                    (void *)h->estep, (void *)h->hint})
     cudaFree(ptr);
   if (h->host_stats) cudaFreeHost(h->host_stats);
   if (h->own) cudaStreamDestroy(h->own);
@@ -111,6 +172,17 @@ int read_stats(pe_semilag *h) {
   return PE_OK;
 }
 
+bool use_tiled(const pe_semilag *h) {
+  if (h->kernel == PE_SL_KERNEL_TILED) return h->tiled_ok;
+  return h->kernel == PE_SL_KERNEL_AUTO && h->tiled_auto;
+}
+
+// Reset the per-cell action hints of the tiled kernel (neutral pair).
+int reset_hints(pe_semilag *h) {
+  if (h->hint) PE_CUDA_TRY(cudaMemsetAsync(h->hint, 0x44, (size_t)h->g.n, h->stream));
+  return PE_OK;
+}
+
 int backup(pe_semilag *h, bool policy) {
   PE_CUDA_TRY(cudaMemsetAsync(&h->stats->residual, 0, sizeof(unsigned long long),
                               h->stream));
@@ -124,7 +196,12 @@ int backup(pe_semilag *h, bool policy) {
   bk.emove = h->emove;
   bk.stats = h->stats;
   cudaEvent_t e0 = h->timer.begin(h->stream);
-  PE_CUDA_TRY(pe::sl_backup(h->g, bk, h->stream));
+  if (!policy && use_tiled(h)) {
+    const pe::SLTiled tl{h->pstep, h->estep, h->hint};
+    PE_CUDA_TRY(pe::sl_backup_tiled(h->g, bk, tl, h->plan, h->stream));
+  } else {
+    PE_CUDA_TRY(pe::sl_backup(h->g, bk, h->stream));
+  }
   pe::count_launches(1);
   {
     const int rc = h->timer.end(h->stream, e0, 0);
@@ -215,6 +292,22 @@ int pe_semilag_create(const pe_semilag_params *params, pe_semilag **out) {
         m.ey = (float)(chord * std::sin(psi + 0.5 * turn));
       }
     }
+  // tiled value-only kernel: speed steps, geometry and a shared-memory plan
+  std::vector<pe::SLSpeedStep> pstep, estep;
+  {
+    int optin = 0;
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin,
+                           params->device);
+    h->tiled_ok = speed_steps(parc, g.nvp, &pstep) && speed_steps(earc, g.nve, &estep) &&
+                  tiled_geometry_ok(g, parc, earc, emove) &&
+                  pe::sl_tiled_plan(g, optin - 1024, &h->plan);
+    // one CTA per SM: with fewer than ~8 items per SM the tail of the last
+    // wave and the per-item ring warm-up outweigh the gain (measured on a
+    // 33x24x11x11 grid: 1.46 ms tiled vs 0.81 ms generic per backup)
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, params->device);
+    h->tiled_auto = h->tiled_ok && h->plan.items >= 8 * (int64_t)sms;
+  }
   cudaError_t err = cudaSuccess;
   auto take = [&](cudaError_t e) {
     if (err == cudaSuccess) err = e;
@@ -240,6 +333,17 @@ int pe_semilag_create(const pe_semilag_params *params, pe_semilag **out) {
     take(cudaMemcpy(h->emove, emove.data(), sizeof(pe::SLEvaderMove) * emove.size(),
                     cudaMemcpyHostToDevice));
     take(cudaMemset(h->stats, 0, sizeof(pe::SLStats)));
+  }
+  if (err == cudaSuccess && h->tiled_ok) {
+    take(cudaMalloc(&h->pstep, sizeof(pe::SLSpeedStep) * pstep.size()));
+    take(cudaMalloc(&h->estep, sizeof(pe::SLSpeedStep) * estep.size()));
+    take(cudaMalloc(&h->hint, (size_t)g.n));
+    if (err == cudaSuccess) {
+      take(cudaMemcpy(h->pstep, pstep.data(), sizeof(pe::SLSpeedStep) * pstep.size(),
+                      cudaMemcpyHostToDevice));
+      take(cudaMemcpy(h->estep, estep.data(), sizeof(pe::SLSpeedStep) * estep.size(),
+                      cudaMemcpyHostToDevice));
+    }
   }
   if (err != cudaSuccess) {
     rc = pe::cuda_fail(err, "pe_semilag_create");
@@ -274,6 +378,8 @@ int pe_semilag_init(pe_semilag *h, const float *initial) {
     PE_CUDA_TRY(pe::sl_init(h->g, h->plane, h->a, h->stream));
     pe::count_launches(1);
   }
+  rc = reset_hints(h);
+  if (rc) return rc;
   PE_CUDA_TRY(cudaStreamSynchronize(h->stream));
   h->iterations = 0;
   h->initialized = true;
@@ -288,6 +394,8 @@ int pe_semilag_init_device(pe_semilag *h, const float *device_initial) {
   PE_CUDA_TRY(cudaMemsetAsync(h->stats, 0, sizeof(pe::SLStats), h->stream));
   PE_CUDA_TRY(cudaMemcpyAsync(h->a, device_initial, sizeof(float) * (size_t)h->g.n,
                               cudaMemcpyDeviceToDevice, h->stream));
+  rc = reset_hints(h);
+  if (rc) return rc;
   PE_CUDA_TRY(cudaStreamSynchronize(h->stream));
   h->iterations = 0;
   h->initialized = true;
@@ -390,6 +498,24 @@ int pe_semilag_set_stream(pe_semilag *h, void *cuda_stream) {
   int rc = enter(h);
   if (rc) return rc;
   h->stream = cuda_stream ? (cudaStream_t)cuda_stream : h->own;
+  return PE_OK;
+}
+
+int pe_semilag_set_kernel(pe_semilag *h, int kernel) {
+  int rc = enter(h);
+  if (rc) return rc;
+  if (kernel != PE_SL_KERNEL_AUTO && kernel != PE_SL_KERNEL_GENERIC &&
+      kernel != PE_SL_KERNEL_TILED)
+    return fail(PE_EINVAL, "unknown backup kernel %d", kernel);
+  if (kernel == PE_SL_KERNEL_TILED && !h->tiled_ok)
+    return fail(PE_EINVAL, "the tiled backup kernel does not apply to this grid and dt");
+  h->kernel = kernel;
+  return PE_OK;
+}
+
+int pe_semilag_kernel(const pe_semilag *h, int32_t *kernel) {
+  if (!h || !kernel) return fail(PE_EINVAL, "handle or kernel is NULL");
+  *kernel = use_tiled(h) ? PE_SL_KERNEL_TILED : PE_SL_KERNEL_GENERIC;
   return PE_OK;
 }
 

@@ -6,74 +6,10 @@
 //
 // One thread per cell of the padded layout.  blockIdx.z enumerates (vP, vE),
 // blockIdx.y the heading, and the x dimension covers the (y, x) plane.
-#include "relative5d.cuh"
+#include "relative5d_exact.cuh"
 
 namespace pe {
 namespace {
-
-struct Slopes {
-  double lo, hi;
-};
-
-// One-axis ENO slopes at node j (native_relative.cpp:38-67).
-template <int ORDER>
-__device__ __forceinline__ Slopes eno_axis(const float *__restrict__ s,
-                                           int64_t j, int64_t stride, int pos,
-                                           int n, double h, bool periodic) {
-  Slopes r;
-  const double v = s[j];
-  if (!periodic && pos == 0) {
-    r.lo = r.hi = ((double)s[j + stride] - v) / h;
-    return r;
-  }
-  if (!periodic && pos == n - 1) {
-    r.lo = r.hi = (v - (double)s[j - stride]) / h;
-    return r;
-  }
-  // Offsets of the neighbours, wrapped on the periodic axis.
-  const int64_t wrap = (int64_t)n * stride;
-  const int64_t om1 = (periodic && pos < 1) ? wrap - stride : -stride;
-  const int64_t op1 = (periodic && pos + 1 >= n) ? stride - wrap : stride;
-  const double vm = s[j + om1];
-  const double vp = s[j + op1];
-  r.lo = (v - vm) / h;
-  r.hi = (vp - v) / h;
-  if (ORDER == 1) return r;
-  const double hh = h * h;
-  const double c2 = (vp - 2 * v + vm) / hh;
-  double l2 = c2, r2 = c2;
-  if (periodic || pos >= 2) {
-    const int64_t om2 = (periodic && pos < 2) ? wrap - 2 * stride : -2 * stride;
-    l2 = (v - 2 * vm + (double)s[j + om2]) / hh;
-  }
-  if (periodic || pos + 2 < n) {
-    const int64_t op2 =
-        (periodic && pos + 2 >= n) ? 2 * stride - wrap : 2 * stride;
-    r2 = ((double)s[j + op2] - 2 * vp + v) / hh;
-  }
-  r.lo += .5 * h * (fabs(l2) < fabs(c2) ? l2 : c2);
-  r.hi -= .5 * h * (fabs(c2) < fabs(r2) ? c2 : r2);
-  return r;
-}
-
-__device__ __forceinline__ void atomic_max_nonneg(unsigned long long *word,
-                                                  double value) {
-  // Non-negative doubles order like their bit patterns.
-  if (value > 0) atomicMax(word, (unsigned long long)__double_as_longlong(value));
-}
-
-// Block maximum of a non-negative double (blockDim.x = 128).
-__device__ __forceinline__ double block_max(double v, double *scratch) {
-  for (int off = 16; off > 0; off >>= 1)
-    v = fmax(v, __shfl_xor_sync(0xffffffffu, v, off));
-  if ((threadIdx.x & 31) == 0) scratch[threadIdx.x >> 5] = v;
-  __syncthreads();
-  double m = 0;
-  if (threadIdx.x == 0)
-    for (int w = 0; w < (int)(blockDim.x >> 5); w++) m = fmax(m, scratch[w]);
-  __syncthreads();
-  return m;
-}
 
 template <int ORDER, int BLEND>
 __global__ void __launch_bounds__(128)
@@ -88,62 +24,17 @@ __global__ void __launch_bounds__(128)
     const int ie = blockIdx.z % g.nve, iv = blockIdx.z / g.nve;
     const int64_t j = (int64_t)blockIdx.z * g.se + (int64_t)ip * g.sp +
                       (int64_t)iy * g.sy + ix;
-    const float *__restrict__ src = s.src;
-
-    const double x = -g.extent + ix * g.dx;
-    const double y = -g.extent + iy * g.dx;
-    const double vp = g.vp_lo + iv * g.dvp, ve = g.ve_lo + ie * g.dve;
-    const double wp = fabs(vp) * g.curv_p, we = fabs(ve) * g.curv_e;
-    const double bx = ve * s.cs[ip] - vp, by = ve * s.sn[ip];
-
-    const Slopes sx = eno_axis<ORDER>(src, j, 1, ix, g.nx, g.dx, false);
-    const Slopes sy = eno_axis<ORDER>(src, j, g.sy, iy, g.nx, g.dx, false);
-    const Slopes sp = eno_axis<ORDER>(src, j, g.sp, ip, g.nh, g.dphi, true);
-    const Slopes sv = eno_axis<ORDER>(src, j, g.sv, iv, g.nvp, g.dvp, false);
-    const Slopes se = eno_axis<ORDER>(src, j, g.se, ie, g.nve, g.dve, false);
-
-    const double gx = .5 * (sx.lo + sx.hi), gy = .5 * (sy.lo + sy.hi),
-                 gp = .5 * (sp.lo + sp.hi), gv = .5 * (sv.lo + sv.hi),
-                 ge = .5 * (se.lo + se.hi);
-    const double pl = iv == 0 ? 0 : -g.acc_p, ph = iv == g.nvp - 1 ? 0 : g.acc_p;
-    const double el = ie == 0 ? 0 : -g.acc_e, eh = ie == g.nve - 1 ? 0 : g.acc_e;
-    const double pv_lo = pl * gv, pv_hi = ph * gv;
-    const double ev_lo = el * ge, ev_hi = eh * ge;
-    const double p_best = (pv_hi < pv_lo) ? pv_hi : pv_lo;  // std::min order
-    const double e_best = (ev_lo < ev_hi) ? ev_hi : ev_lo;  // std::max order
-    double H = bx * gx + by * gy - wp * fabs(y * gx - x * gy - gp) +
-               we * fabs(gp) + p_best + e_best;
-    H += .5 * ((fabs(bx) + wp * fabs(y)) * (sx.hi - sx.lo) +
-               (fabs(by) + wp * fabs(x)) * (sy.hi - sy.lo) +
-               (wp + we) * (sp.hi - sp.lo) + g.acc_p * (sv.hi - sv.lo) +
-               g.acc_e * (se.hi - se.lo));
-
-    const double old = src[j];
-    const double prev = BLEND ? (double)s.dst[j] : old;
-    double value = old + s.dt * (H < 0. ? H : 0.);
-    if (BLEND) value = .5 * (prev + value);
-    if (!isfinite(value)) {
-      bad = true;
-    } else {
-      const float stored = (float)value;
-      s.dst[j] = stored;
-      if (BLEND || ORDER == 1) {
-        const double change = (double)stored - prev;
-        change_abs = fabs(change);
-        change_up = change > 0 ? change : 0;
-        if (prev > 0 && stored <= 0 && isnan(s.arrival[j]))
-          s.arrival[j] = (float)(s.t + s.dt * prev / (prev - (double)stored));
-      }
-    }
+    exact::cell_update<ORDER, BLEND>(g, s, ix, iy, ip, iv, ie, j, change_abs, change_up,
+                                     bad);
   }
   if (__syncthreads_or(bad) && threadIdx.x == 0)
     atomicOr(&s.stats->nonfinite, 1u);
   if (BLEND || ORDER == 1) {
-    const double m_abs = block_max(change_abs, scratch);
-    const double m_up = block_max(change_up, scratch);
+    const double m_abs = exact::block_max(change_abs, scratch);
+    const double m_up = exact::block_max(change_up, scratch);
     if (threadIdx.x == 0) {
-      atomic_max_nonneg(&s.stats->residual, m_abs);
-      atomic_max_nonneg(&s.stats->increase, m_up);
+      exact::atomic_max_nonneg(&s.stats->residual, m_abs);
+      exact::atomic_max_nonneg(&s.stats->increase, m_up);
     }
   }
 }

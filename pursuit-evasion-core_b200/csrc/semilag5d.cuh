@@ -51,6 +51,42 @@ struct SLBackup {
 
 cudaError_t sl_backup(const SLGrid &g, const SLBackup &b, cudaStream_t stream);
 
+// ---- shared-memory tiled backup (semilag5d_tiled.cu), value only ----------
+
+#define SL_TILED_MAX_THREADS 512
+
+// Speed interpolation of one car's successors from one speed level: the
+// three staged slabs are base, base+1, base+2; acceleration index a blends
+// slab base+slot[a] and the next one with upper weight w[a].
+struct SLSpeedStep {
+  int base;
+  int slot[3];
+  float w[3];
+};
+
+struct SLTiled {
+  const SLSpeedStep *pstep;  // [nvp]
+  const SLSpeedStep *estep;  // [nve]
+  uint8_t *hint;             // [cells]: (pursuer action << 4) | evader reply of
+                             // the previous backup; 0x44 before the first
+};
+
+struct SLTiledPlan {
+  int rows;        // cell rows of a tile (full x width)
+  int tiles_y;
+  int psi_chunk, psi_chunks;
+  int threads;
+  int64_t items;   // nvp * nve * tiles_y * psi_chunks
+  size_t smem;     // dynamic shared memory per CTA
+};
+
+// Tile plan for grid g within max_smem bytes of dynamic shared memory;
+// false if the grid's width does not fit the tiled kernel.
+bool sl_tiled_plan(const SLGrid &g, int max_smem, SLTiledPlan *plan);
+
+cudaError_t sl_backup_tiled(const SLGrid &g, const SLBackup &b, const SLTiled &t,
+                            const SLTiledPlan &plan, cudaStream_t stream);
+
 // Initial field: TUBE hypot(x, y) - radius; MINTIME 0 inside the capture
 // disk and 1 elsewhere.  plane: dense (y, x) values computed on the host.
 cudaError_t sl_init(const SLGrid &g, const float *plane, float *field,

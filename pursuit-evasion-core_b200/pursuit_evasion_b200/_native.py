@@ -108,6 +108,7 @@ class SemiLagParams(ctypes.Structure):
     ]
 
 
+PE_SL_KERNEL_AUTO, PE_SL_KERNEL_GENERIC, PE_SL_KERNEL_TILED = 0, 1, 2
 PE_SL_TUBE = 0
 PE_SL_MINTIME = 1
 
@@ -147,6 +148,23 @@ SIGNATURES = {
     "pe_relative_step_noalloc": (ctypes.c_int, [ctypes.POINTER(RelativeParams), _P, _P,
                                                 _P, ctypes.c_double, ctypes.c_double,
                                                 _P, _DP]),
+    "pe_batch_create": (ctypes.c_int, [ctypes.POINTER(RelativeParams), _DP, ctypes.c_int32,
+                                       ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p)]),
+    "pe_batch_set_tile": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32]),
+    "pe_batch_get_tile": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]),
+    "pe_batch_set_stream": (ctypes.c_int, [_P, _P]),
+    "pe_batch_init": (ctypes.c_int, [_P]),
+    "pe_batch_run": (ctypes.c_int, [_P]),
+    "pe_batch_synchronize": (ctypes.c_int, [_P]),
+    "pe_batch_solve_info": (ctypes.c_int, [_P, ctypes.c_int32, _I64P, _I64P, _DP]),
+    "pe_batch_copy_field": (ctypes.c_int, [_P, ctypes.c_int32, _P]),
+    "pe_batch_copy_arrival": (ctypes.c_int, [_P, ctypes.c_int32, _P]),
+    "pe_batch_stats": (ctypes.c_int, [_P, ctypes.c_int32, _DP, _DP]),
+    "pe_batch_launch_info": (ctypes.c_int, [_P] + [ctypes.POINTER(ctypes.c_int32)] * 3
+                             + [_I64P]),
+    "pe_batch_profile": (ctypes.c_int, [_P, ctypes.c_int]),
+    "pe_batch_kernel_time": (ctypes.c_int, [_P, _DP, _I64P]),
+    "pe_batch_destroy": (ctypes.c_int, [_P]),
     "pe_world_cells": (ctypes.c_int, [ctypes.POINTER(WorldParams), _I64P]),
     "pe_world_dt_limit": (ctypes.c_int, [ctypes.POINTER(WorldParams), _DP]),
     "pe_world_create": (ctypes.c_int, [ctypes.POINTER(WorldParams),
@@ -181,6 +199,8 @@ SIGNATURES = {
     "pe_semilag_device_value": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_void_p)]),
     "pe_semilag_iterations": (ctypes.c_int, [_P, _I64P]),
     "pe_semilag_set_stream": (ctypes.c_int, [_P, _P]),
+    "pe_semilag_set_kernel": (ctypes.c_int, [_P, ctypes.c_int]),
+    "pe_semilag_kernel": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int32)]),
     "pe_semilag_profile": (ctypes.c_int, [_P, ctypes.c_int]),
     "pe_semilag_kernel_time": (ctypes.c_int, [_P, _DP, _I64P]),
     "pe_semilag_destroy": (ctypes.c_int, [_P]),

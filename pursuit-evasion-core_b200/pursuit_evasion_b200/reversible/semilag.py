@@ -27,6 +27,8 @@ import numpy as np
 from .. import _native
 
 MODES = {"tube": _native.PE_SL_TUBE, "min_time": _native.PE_SL_MINTIME}
+KERNELS = {"auto": _native.PE_SL_KERNEL_AUTO, "generic": _native.PE_SL_KERNEL_GENERIC,
+           "tiled": _native.PE_SL_KERNEL_TILED}
 
 
 def semilag_params(config, grid, *, dt=0.0, mode="tube", device=0):
@@ -137,6 +139,18 @@ class SemiLagrangianSolver:
 
     def set_stream(self, stream_ptr):
         _native.check(self._lib.pe_semilag_set_stream(self._h, stream_ptr))
+
+    def set_kernel(self, kernel):
+        """Value-only backup kernel: "auto" (default), "generic" or "tiled"."""
+        if kernel not in KERNELS:
+            raise ValueError("kernel must be 'auto', 'generic' or 'tiled'")
+        _native.check(self._lib.pe_semilag_set_kernel(self._h, KERNELS[kernel]))
+
+    @property
+    def kernel(self):
+        k = ctypes.c_int32()
+        _native.check(self._lib.pe_semilag_kernel(self._h, ctypes.byref(k)))
+        return "tiled" if k.value == _native.PE_SL_KERNEL_TILED else "generic"
 
     def profile(self, enable=True):
         _native.check(self._lib.pe_semilag_profile(self._h, int(enable)))

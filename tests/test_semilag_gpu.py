@@ -69,6 +69,57 @@ def test_single_backup_matches_oracle(oracle, mode):
     assert np.mean(ge[same] == pe[same]) > 0.98
 
 
+@pytest.mark.parametrize("mode", ["tube", "min_time"])
+@pytest.mark.parametrize("grid", [RelativeGrid(13, 12, 7, 7, 3.0),
+                                  RelativeGrid(21, 16, 5, 9, 5.0)])
+def test_tiled_value_backup_matches_oracle(oracle, mode, grid):
+    """The shared-memory tiled kernel (value-only backups) on random fields."""
+    dt = interpolation_cfl_dt(A3, grid)
+    omode = oracle_lib.SL_TUBE if mode == "tube" else oracle_lib.SL_MINTIME
+    cfg = oracle.sl_cfg(A3, grid, dt, omode)
+    rng = np.random.default_rng(11)
+    if mode == "tube":
+        V = oracle.sl_init(cfg, grid.states) + 0.05 * rng.normal(size=grid.states)
+    else:
+        V = rng.uniform(0, 1, grid.states)
+    V32 = V.astype(np.float32)
+    ref = oracle.sl_backup(cfg, V32.astype(np.float64))
+    with SemiLagrangianSolver(A3, grid, dt=dt, mode=mode) as s:
+        s.set_kernel("tiled")
+        assert s.kernel == "tiled"
+        s.initialize(V32)
+        s.backup()
+        got = s.value().ravel()
+        residual = s.residual()
+    np.testing.assert_allclose(got, ref, atol=VALUE_ATOL, rtol=0)
+    assert residual == pytest.approx(float(np.abs(got - V32).max()), rel=1e-6, abs=1e-12)
+
+
+@pytest.mark.parametrize("mode", ["tube", "min_time"])
+def test_tiled_and_generic_kernels_agree_over_iterations(mode):
+    """Ten value-only backups with the tiled kernel (pruned, hint-ordered)
+    and with the generic kernel: the same fields up to float rounding."""
+    grid = RelativeGrid(33, 24, 7, 7, 6.0)
+    out = {}
+    for kernel in ("tiled", "generic"):
+        with SemiLagrangianSolver(A3, grid, mode=mode) as s:
+            s.set_kernel(kernel)
+            assert s.kernel == kernel
+            s.initialize()
+            s.iterate(10, tol=0.0, check_every=10)
+            out[kernel] = s.value().ravel().copy()
+    np.testing.assert_allclose(out["tiled"], out["generic"], atol=10 * VALUE_ATOL, rtol=0)
+
+
+def test_tiled_kernel_refused_where_it_does_not_apply():
+    grid = RelativeGrid(13, 12, 7, 7, 3.0)
+    big_dt = 4 * interpolation_cfl_dt(A3, grid)  # successors several cells away
+    with SemiLagrangianSolver(A3, grid, dt=big_dt, mode="tube") as s:
+        assert s.kernel == "generic"
+        with pytest.raises(ValueError):
+            s.set_kernel("tiled")
+
+
 def test_tube_backups_are_monotone_and_track_oracle(oracle):
     grid = CONFIG1_GRID
     dt = interpolation_cfl_dt(A3, grid)
@@ -131,3 +182,27 @@ def test_full_size_backup_spot_checks(oracle):
     np.testing.assert_allclose(v1[cells], ref, atol=VALUE_ATOL, rtol=0)
     agree = np.mean(gp.ravel()[cells] == pp)
     assert agree > 0.95
+
+
+def test_full_size_tiled_backup_spot_checks(oracle):
+    """89,434,800 cells, two value-only backups with the tiled kernel (the
+    second one pruned with the first one's hints): sampled cells against the
+    FP64 oracle."""
+    grid = CONFIG2_GRID
+    dt = interpolation_cfl_dt(A3, grid)
+    cfg = oracle.sl_cfg(A3, grid, dt, oracle_lib.SL_TUBE)
+    rng = np.random.default_rng(9)
+    cells = rng.choice(grid.states, size=300, replace=False)
+    with SemiLagrangianSolver(A3, grid, dt=dt, mode="tube") as s:
+        assert s.kernel == "tiled"
+        s.initialize()
+        s.backup()
+        v1 = s.value().ravel().copy()
+        s.backup()
+        v2 = s.value().ravel()
+    v0 = oracle.sl_init(cfg, grid.states)
+    ref1, _, _ = oracle.sl_backup_cells(cfg, v0, cells)
+    np.testing.assert_allclose(v1[cells], ref1, atol=VALUE_ATOL, rtol=0)
+    ref2, _, _ = oracle.sl_backup_cells(cfg, v1.astype(np.float64), cells)
+    np.testing.assert_allclose(v2[cells], ref2, atol=VALUE_ATOL, rtol=0)
+    assert np.isfinite(v2).all() and np.all(v2 <= v1)
