@@ -80,6 +80,11 @@ class ValueMLP:
         self.dy = torch.empty(batch, device=self.dev)
         self.target = torch.empty(batch, device=self.dev)
 
+    def set_batch(self, batch):
+        """Reallocate the activation buffers for `batch` rows (for instance
+        large inference chunks after training); weights are kept."""
+        self._alloc(int(batch))
+
     # ----------------------------------------------------------- kernels
     def _stream(self):
         return ctypes.c_void_p(self.torch.cuda.current_stream(self.dev).cuda_stream)

@@ -21,6 +21,9 @@ from .mlp import ValueMLP
 from .train import RelativeNodeSampler, predict_nodes, train
 
 
+INFER_CHUNK = 1 << 17  # rows per inference launch sequence
+
+
 def converge(config, grid, *, dt, tol, initial=None, max_iterations=20000,
              check_every=5, device=0):
     """Minimum-time value iteration to residual < tol.  `initial`: optional
@@ -56,7 +59,7 @@ def surrogate_start(net, config, grid, out):
     """Surrogate prediction on every node of `grid`, clamped to [0, 1]."""
     import torch
 
-    predict_nodes(net, RelativeNodeSampler(config, grid), out)
+    predict_nodes(net, RelativeNodeSampler(config, grid), out, chunk=net.batch)
     out.clamp_(0.0, 1.0)
     return out
 
@@ -77,6 +80,7 @@ def time_to_converged(config, grid, *, dt, tol=1e-5, samples=1 << 22, epochs=20,
         losses, train_s = train(net, RelativeNodeSampler(config, table_grid, table),
                                 samples=samples, epochs=epochs, batch=batch, seed=seed,
                                 log=log)
+        net.set_batch(INFER_CHUNK)  # inference in large chunks
         t0 = time.perf_counter()
         u0 = surrogate_start(net, config, grid, torch.empty(grid.states, device=dev))
         torch.cuda.synchronize(dev)
