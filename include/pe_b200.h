@@ -253,6 +253,9 @@ typedef struct pe_world_params {
   int32_t linear_speed_boundary; /* --linear-speed-boundary */
   int32_t avoid_mode;            /* 0: none; 1: max(|xP|,|yP|) - arena + 1e-6 */
   int32_t device;
+  int32_t fast; /* 0 (default): float32 in the reference's order, bit for bit
+                   native_world.cpp; 1: reciprocal spacings and multiply-add
+                   contraction (equal to float rounding and ENO2 flips) */
 } pe_world_params;
 
 typedef struct pe_world pe_world;
@@ -375,6 +378,18 @@ int pe_mlp_gemm(const void *A, const void *B, int M, int N, int K, int lda, int 
                 int a_mmajor, int b_nmajor, int epilogue, int splits, float *C32,
                 void *C16, int ldc, const float *bias, const float *zpre,
                 void *cuda_stream);
+/* The same product on the 5th-generation tensor cores (tcgen05.mma with the
+ * accumulator in tensor memory, TMA-fed 128B-swizzled shared memory), for
+ * the case of both operands K-major: A [M][K] (row pitch lda) and B [N][K]
+ * (row pitch ldb), C = A B^T.  Epilogues 0, 1 and 3 as pe_mlp_gemm.  M, N
+ * multiples of 128, K a multiple of 64, operands 16-byte aligned with lda,
+ * ldb multiples of 8. */
+int pe_mlp_gemm_tc(const void *A, const void *B, int M, int N, int K, int lda, int ldb,
+                   int epilogue, float *C32, void *C16, int ldc, const float *bias,
+                   const float *zpre, void *cuda_stream);
+/* Number of pe_mlp_gemm_tc launches whose bounded waits timed out since the
+ * last call (then cleared).  Synchronises the device. */
+int pe_mlp_gemm_tc_timeouts(int32_t *count);
 /* Adam on n FP32 master weights w (w16, if not NULL, receives their bf16
  * copy).  corr[0], corr[1] are the bias corrections 1 - beta^t read on the
  * device, so a captured graph replays with the current step. */
@@ -391,6 +406,9 @@ int pe_mlp_head_forward(const void *h, const float *w, const float *b,
 int pe_mlp_head_backward(const void *h, const float *zprev, const float *w,
                          const float *dy, float *dw, float *db, void *dz, int rows,
                          int width, void *cuda_stream);
+/* dst[c][r] = src[r][c] for a bf16 matrix of rows x cols (the transposed
+ * weight copy the tensor-core activation-gradient GEMM reads). */
+int pe_mlp_transpose(const void *src, void *dst, int rows, int cols, void *cuda_stream);
 /* out[c] = sum over rows of bf16 x[row][c] (bias gradients). */
 int pe_mlp_colsum(const void *x, float *out, int rows, int cols, void *cuda_stream);
 /* Features of relative 5D grid nodes (flat [vP, vE, psi, y, x] indices idx)

@@ -107,7 +107,6 @@ def build(verbose: bool = False) -> Path:
         "-o",
         str(tmp),
         *map(str, objects),
-        "-lcuda",
     ]
     result = subprocess.run(cmd, capture_output=True, text=True)
     if result.returncode != 0:

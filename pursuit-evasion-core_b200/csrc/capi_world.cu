@@ -45,7 +45,7 @@ int validate(const pe_world_params *p) {
       p->p_speed_min >= p->p_speed_max || p->e_speed_min >= p->e_speed_max ||
       p->p_acceleration <= 0 || p->e_acceleration <= 0 || p->p_curvature <= 0 ||
       p->e_curvature <= 0 || p->extent <= 0 ||
-      (p->avoid_mode != 0 && p->avoid_mode != 1))
+      (p->avoid_mode != 0 && p->avoid_mode != 1) || (p->fast != 0 && p->fast != 1))
     return fail(PE_EINVAL, "Invalid arguments");
   return PE_OK;
 }
@@ -75,6 +75,7 @@ pe::World8Grid make_grid(const pe_world_params *p) {
   for (int k = 0; k < 8; k++) {
     g.shape[k] = shape[k];
     g.spacing[k] = spacing[k];
+    g.inv_spacing[k] = 1.f / spacing[k];
   }
   g.stride[7] = 1;
   for (int k = 6; k >= 0; k--) g.stride[k] = g.stride[k + 1] * shape[k + 1];
@@ -131,7 +132,8 @@ int stage(pe_world *h, const float *src, float *dst, const float *base, float dt
   s.tau = h->t;
   s.stats = h->stats;
   cudaEvent_t e0 = h->timer.begin(h->stream);
-  PE_CUDA_TRY(pe::world8_stage(h->g, s, h->stream));
+  PE_CUDA_TRY(h->p.fast ? pe::world8_stage_fast(h->g, s, h->stream)
+                        : pe::world8_stage(h->g, s, h->stream));
   pe::count_launches(1);
   return h->timer.end(h->stream, e0, 0);
 }

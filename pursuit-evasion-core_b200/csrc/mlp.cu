@@ -292,6 +292,23 @@ __global__ void head_backward_kernel(const __nv_bfloat16 *h, const float *zprev,
   if (col == 0) atomicAdd(db, accb);
 }
 
+// dst[c][r] = src[r][c] (bf16, rows x cols), through a 32 x 33 shared tile.
+__global__ void transpose_kernel(const __nv_bfloat16 *src, __nv_bfloat16 *dst, int rows,
+                                 int cols) {
+  __shared__ __nv_bfloat16 tile[32][33];
+  const int c = blockIdx.x * 32 + threadIdx.x;
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    const int r = blockIdx.y * 32 + k;
+    if (r < rows && c < cols) tile[k][threadIdx.x] = src[(int64_t)r * cols + c];
+  }
+  __syncthreads();
+  const int r = blockIdx.y * 32 + threadIdx.x;
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    const int cc = blockIdx.x * 32 + k;
+    if (r < rows && cc < cols) dst[(int64_t)cc * rows + r] = tile[threadIdx.x][k];
+  }
+}
+
 // Column sums of a bf16 matrix (bias gradients): out[c] += sum_r x[r][c].
 __global__ void colsum_kernel(const __nv_bfloat16 *x, float *out, int rows, int cols) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -567,6 +584,18 @@ int pe_mlp_encode_world_nodes(const float *table, const int64_t *idx, int n,
       feature_scale((float)extent, (float)p_min, (float)p_max, (float)e_min, (float)e_max),
       static_cast<__nv_bfloat16 *>(feat), ld, target);
   PE_CUDA_TRY(cudaGetLastError());
+  pe::count_launches(1);
+  return PE_OK;
+}
+
+int pe_mlp_transpose(const void *src, void *dst, int rows, int cols, void *cuda_stream) {
+  if (!src || !dst || rows <= 0 || cols <= 0)
+    return pe::fail(PE_EINVAL, "transpose: invalid arguments");
+  const dim3 grid((cols + 31) / 32, (rows + 31) / 32), block(32, 8);
+  pe::transpose_kernel<<<grid, block, 0, static_cast<cudaStream_t>(cuda_stream)>>>(
+      static_cast<const __nv_bfloat16 *>(src), static_cast<__nv_bfloat16 *>(dst), rows, cols);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return pe::cuda_fail(e, "pe_mlp_transpose");
   pe::count_launches(1);
   return PE_OK;
 }

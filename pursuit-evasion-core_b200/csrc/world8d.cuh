@@ -18,6 +18,7 @@ struct World8Grid {
   int64_t stride[8];
   int shape[8];
   float spacing[8];
+  float inv_spacing[8];  // 1 / spacing (fast variant)
   float extent, arena, ap, ae, kp, ke;
 };
 
@@ -43,6 +44,12 @@ struct World8Stage {
 // equal native_world.cpp's bit for bit.
 cudaError_t world8_stage(const World8Grid &g, const World8Stage &s,
                          cudaStream_t stream);
+
+// The same stage with reciprocal spacings and multiply-add contraction:
+// equal to the exact stage up to float rounding (and the ENO2 selections
+// rounding can flip).
+cudaError_t world8_stage_fast(const World8Grid &g, const World8Stage &s,
+                              cudaStream_t stream);
 
 // Capture field of the 8D contact game: the oriented-rectangle separation of
 // the two footprints at every grid pose, in double, stored as float; arrival

@@ -83,6 +83,7 @@ class WorldParams(ctypes.Structure):
         ("linear_speed_boundary", ctypes.c_int32),
         ("avoid_mode", ctypes.c_int32),
         ("device", ctypes.c_int32),
+        ("fast", ctypes.c_int32),
     ]
 
 
@@ -206,11 +207,15 @@ SIGNATURES = {
     "pe_semilag_destroy": (ctypes.c_int, [_P]),
     "pe_mlp_gemm": (ctypes.c_int, [_P, _P] + [ctypes.c_int] * 9 + [_P, _P, ctypes.c_int,
                                                                    _P, _P, _P]),
+    "pe_mlp_gemm_tc": (ctypes.c_int, [_P, _P] + [ctypes.c_int] * 6 + [_P, _P, ctypes.c_int,
+                                                                     _P, _P, _P]),
+    "pe_mlp_gemm_tc_timeouts": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int32)]),
     "pe_mlp_adam": (ctypes.c_int, [_P, _P, _P, _P, _P, ctypes.c_int64, ctypes.c_float,
                                    ctypes.c_float, ctypes.c_float, ctypes.c_float, _P,
                                    ctypes.c_float, _P]),
     "pe_mlp_head_forward": (ctypes.c_int, [_P] * 7 + [ctypes.c_int, ctypes.c_int, _P]),
     "pe_mlp_head_backward": (ctypes.c_int, [_P] * 7 + [ctypes.c_int, ctypes.c_int, _P]),
+    "pe_mlp_transpose": (ctypes.c_int, [_P, _P, ctypes.c_int, ctypes.c_int, _P]),
     "pe_mlp_colsum": (ctypes.c_int, [_P, _P, ctypes.c_int, ctypes.c_int, _P]),
     "pe_mlp_encode_relative_nodes": (ctypes.c_int, [_P, _P] + [ctypes.c_int] * 5
                                      + [ctypes.c_double] * 5 + [_P, ctypes.c_int, _P, _P]),

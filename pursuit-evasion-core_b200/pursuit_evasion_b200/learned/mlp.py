@@ -5,9 +5,11 @@ Architecture (BF16 weights and activations, FP32 accumulation):
 The features of a relative 5D state [x, y, psi, vP, vE] are
 [x/e, y/e, cos psi, sin psi, vP~, vE~] (speeds mapped to [-1, 1]); of an 8D
 state, the same per car.  Every forward, backward and Adam kernel is
-hand-written (csrc/mlp.cu, C ABI pe_mlp_*); PyTorch only provides device
-memory, the stream, random numbers for minibatches and, in the tests, the
-FP64 autograd that checks the gradients.  The reference's precedent is a
+hand-written (csrc/mlp.cu, csrc/mlp_tc.cu, C ABI pe_mlp_*): the layer and
+activation-gradient GEMMs run on the tensor cores with tcgen05.mma and the
+accumulator in tensor memory, the split-K weight-gradient GEMM on mma.sync.
+PyTorch only provides device memory, the stream, random numbers for
+minibatches and, in the tests, the FP64 autograd that checks the gradients.  The reference's precedent is a
 SiLU MLP trained with Adam on MSE against DP labels
 (local_game/learning.py:32-38, training.py:185-186, :352).
 """
@@ -59,6 +61,10 @@ class ValueMLP:
         self.w_out = ((torch.rand(hidden, generator=gen) * 2 - 1) / math.sqrt(hidden)).to(self.dev)
         self.b_out = torch.zeros(1, device=self.dev)
         self.w16 = [w.to(torch.bfloat16).contiguous() for w in self.w]
+        # transposed bf16 copies [in][out]: the K-major operand of the
+        # activation-gradient GEMM on the tensor cores
+        self.w16t = [torch.empty(w.shape[1], w.shape[0], dtype=torch.bfloat16, device=self.dev)
+                     for w in self.w]
         self.params = self.w + self.b + [self.w_out, self.b_out]
         self.m = [torch.zeros_like(p) for p in self.params]
         self.v = [torch.zeros_like(p) for p in self.params]
@@ -66,6 +72,7 @@ class ValueMLP:
         self.corr = torch.ones(2, device=self.dev)
         self.loss = torch.zeros(1, device=self.dev)
         self._alloc(max_batch)
+        self._transpose_weights()
 
     def _alloc(self, batch):
         torch = self.torch
@@ -97,14 +104,26 @@ class ValueMLP:
                                   opt(bias), opt(zpre), self._stream())
         _native.check(rc)
 
+    def _gemm_tc(self, A, B, M, N, K, epi, *, C32=None, C16=None, bias=None, zpre=None):
+        """C = A B^T on the tensor cores (tcgen05); A [M][K], B [N][K]."""
+        opt = lambda t: None if t is None else _ptr(t)
+        _native.check(self.lib.pe_mlp_gemm_tc(_ptr(A), _ptr(B), M, N, K, A.shape[1],
+                                              B.shape[1], epi, opt(C32), opt(C16), N,
+                                              opt(bias), opt(zpre), self._stream()))
+
+    def _transpose_weights(self):
+        for w, wt in zip(self.w16, self.w16t):
+            _native.check(self.lib.pe_mlp_transpose(_ptr(w), _ptr(wt), w.shape[0], w.shape[1],
+                                                    self._stream()))
+
     def forward(self, rows, *, target=False):
         """Forward over self.feat[:rows]; with target=True also the MSE loss
         (accumulated into self.loss) and dy."""
         x = self.feat
         for l in range(self.layers):
             K = FEATURES if l == 0 else self.hidden
-            self._gemm(x, self.w16[l], rows, self.hidden, K, K, K, False, False, 1,
-                       C32=self.z[l], C16=self.h[l], ldc=self.hidden, bias=self.b[l])
+            self._gemm_tc(x, self.w16[l], rows, self.hidden, K, 1, C32=self.z[l],
+                          C16=self.h[l], bias=self.b[l])
             x = self.h[l]
         _native.check(self.lib.pe_mlp_head_forward(
             _ptr(self.h[-1]), _ptr(self.w_out), _ptr(self.b_out),
@@ -137,9 +156,8 @@ class ValueMLP:
                                                  self.hidden, self._stream()))
             if l > 0:
                 # dz_{l-1} = (dz_l W_l) * silu'(z_{l-1})
-                self._gemm(self.dz[l], self.w16[l], rows, self.hidden, self.hidden,
-                           self.hidden, self.hidden, False, True, 3, C16=self.dz[l - 1],
-                           ldc=self.hidden, zpre=self.z[l - 1])
+                self._gemm_tc(self.dz[l], self.w16t[l], rows, self.hidden, self.hidden, 3,
+                              C16=self.dz[l - 1], zpre=self.z[l - 1])
 
     def adam(self, lr=1e-3, beta1=0.9, beta2=0.999, eps=1e-8):
         """One Adam update; the bias corrections are read from self.corr on
@@ -149,6 +167,7 @@ class ValueMLP:
             _native.check(self.lib.pe_mlp_adam(_ptr(p), w16, _ptr(g), _ptr(m), _ptr(v),
                                                p.numel(), lr, beta1, beta2, eps,
                                                _ptr(self.corr), 1.0, self._stream()))
+        self._transpose_weights()
 
     def set_step(self, step, beta1=0.9, beta2=0.999):
         self.corr.copy_(self.torch.tensor([1 - beta1 ** step, 1 - beta2 ** step],

@@ -90,7 +90,7 @@ def output_times(horizon, output_dt):
         np.arange(int(np.ceil(horizon / output_dt)) + 1) * output_dt, horizon))
 
 
-def _params(config, grid, *, order, cfl, speed_boundary, avoid, device):
+def _params(config, grid, *, order, cfl, speed_boundary, avoid, device, fast=False):
     p, e = config.pursuer, config.evader
     return _native.WorldParams(
         positions=grid.positions, headings=grid.headings,
@@ -103,14 +103,17 @@ def _params(config, grid, *, order, cfl, speed_boundary, avoid, device):
         e_acceleration=float(e.acceleration), e_curvature=float(e.max_curvature),
         cfl=float(cfl), order=int(order),
         linear_speed_boundary=int(speed_boundary == "linear"),
-        avoid_mode=1 if avoid else 0, device=int(device))
+        avoid_mode=1 if avoid else 0, device=int(device), fast=int(bool(fast)))
 
 
 class WorldSolver:
-    """Owning handle of one device-resident 8D field (pe_world_*)."""
+    """Owning handle of one device-resident 8D field (pe_world_*).  `fast`
+    selects the stage with reciprocal spacings and multiply-add contraction
+    instead of the reference's operation order (bit for bit
+    native_world.cpp)."""
 
     def __init__(self, config, grid, *, order=2, cfl=0.8, speed_boundary="linear",
-                 avoid=True, device=0):
+                 avoid=True, device=0, fast=False):
         if speed_boundary not in ("linear", "legacy_signed"):
             raise ValueError("Speed boundary must be linear or legacy_signed.")
         if order not in (1, 2) or not 0 < cfl <= 1:
@@ -121,7 +124,7 @@ class WorldSolver:
         self.cells = grid.states
         self._params = _params(config, grid, order=order, cfl=cfl,
                                speed_boundary=speed_boundary, avoid=avoid,
-                               device=device)
+                               device=device, fast=fast)
         handle = ctypes.c_void_p()
         _native.check(self._lib.pe_world_create(ctypes.byref(self._params),
                                                 ctypes.byref(handle)))

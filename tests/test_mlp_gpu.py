@@ -118,3 +118,50 @@ def test_training_reduces_loss():
         net.adam(lr=1e-3)
         losses.append(float(net.loss.cpu()))
     assert losses[-1] < 0.05 * losses[0]
+
+
+def gemm_tc_case(epi, M=256, N=256, K=256, seed=0):
+    import ctypes
+
+    from pursuit_evasion_b200 import _native
+
+    g = torch.Generator().manual_seed(seed)
+    A = torch.randn(M, K, generator=g).to(torch.bfloat16)
+    B = torch.randn(N, K, generator=g).to(torch.bfloat16)  # [N][K]: a Linear weight
+    bias = torch.randn(N, generator=g)
+    zpre = torch.randn(M, N, generator=g)
+    ref = A.float() @ B.float().t()
+    dev = torch.device("cuda", 0)
+    Ad, Bd = A.to(dev), B.to(dev)
+    C32 = torch.zeros(M, N, device=dev)
+    C16 = torch.zeros(M, N, dtype=torch.bfloat16, device=dev)
+    biasd, zd = bias.to(dev), zpre.to(dev)
+    lib = _native.library()
+    p = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+    _native.check(lib.pe_mlp_gemm_tc(p(Ad), p(Bd), M, N, K, K, K, epi,
+                                     p(C32) if epi in (0, 1) else None,
+                                     p(C16) if epi in (1, 3) else None, N,
+                                     p(biasd) if epi == 1 else None,
+                                     p(zd) if epi == 3 else None,
+                                     ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+    torch.cuda.synchronize()
+    timeouts = ctypes.c_int32()
+    _native.check(lib.pe_mlp_gemm_tc_timeouts(ctypes.byref(timeouts)))
+    assert timeouts.value == 0
+    return ref, bias, zpre, C32.cpu(), C16.float().cpu()
+
+
+@pytest.mark.parametrize("M, N, K", [(128, 128, 64), (256, 256, 256), (1024, 256, 128)])
+def test_tensor_core_gemm_matches_fp32_reference(M, N, K):
+    ref, _, _, C32, _ = gemm_tc_case(0, M=M, N=N, K=K)
+    torch.testing.assert_close(C32, ref, rtol=1e-4, atol=1e-3)
+
+
+def test_tensor_core_gemm_epilogues():
+    ref, bias, _, C32, C16 = gemm_tc_case(1)
+    z = ref + bias
+    torch.testing.assert_close(C32, z, rtol=1e-4, atol=1e-3)
+    torch.testing.assert_close(C16, torch.nn.functional.silu(z), rtol=1e-2, atol=2e-2)
+    ref, _, zpre, _, C16 = gemm_tc_case(3)
+    s = torch.sigmoid(zpre)
+    torch.testing.assert_close(C16, ref * s * (1 + zpre * (1 - s)), rtol=1e-2, atol=5e-2)
