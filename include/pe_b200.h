@@ -349,6 +349,13 @@ int pe_semilag_set_stream(pe_semilag *h, void *cuda_stream);
  * generic kernel.  Both give the same values up to float rounding. */
 enum { PE_SL_KERNEL_AUTO = 0, PE_SL_KERNEL_GENERIC = 1, PE_SL_KERNEL_TILED = 2 };
 int pe_semilag_set_kernel(pe_semilag *h, int kernel);
+/* Tile of the tiled kernel: about `rows` cell rows at full width per work
+ * item (0 restores the default); smaller tiles use less shared memory, so
+ * two CTAs can share an SM, at a larger halo cost.  Results do not depend
+ * on the tile. */
+int pe_semilag_set_tile(pe_semilag *h, int32_t rows);
+int pe_semilag_get_tile(const pe_semilag *h, int32_t *rows, int32_t *threads,
+                        int64_t *items);
 /* The kernel value-only backups use now (GENERIC or TILED). */
 int pe_semilag_kernel(const pe_semilag *h, int32_t *kernel);
 int pe_semilag_profile(pe_semilag *h, int enable);
@@ -430,6 +437,37 @@ int pe_mlp_encode_world_nodes(const float *table, const int64_t *idx, int n,
                               double extent, double p_min, double p_max, double e_min,
                               double e_max, void *feat, int ld, float *target,
                               void *cuda_stream);
+
+/* ------------------------------------------------------------------------
+ * Queries of a completed relative table, resident on the GPU.
+ *
+ * Replaces RelativeTable.field / RelativeTable.value of
+ * reversible/relative_table.py:76-161 for batches of states: 32-corner
+ * multilinear stencil over [vP, vE, psi, y, x] with periodic heading, the
+ * signed field at a budget (linear in time between frames), and the capture
+ * time as the first zero crossing found by bisection over frames.  Results
+ * equal the reference reader's in double precision (summation order
+ * aside), including its batch-wide bisection: a state whose earliest frame
+ * is already inside is resolved as the reference resolves it in a batch
+ * of the same states.
+ * ------------------------------------------------------------------------ */
+typedef struct pe_table pe_table;
+
+/* host_frames: [frames][cells] float32 in storage order [vP, vE, psi, y, x]
+ * (fields.f32 of a table directory); times: the output times; shape,
+ * axis_lo, axis_hi, spacing per storage axis (the metadata's axes: first,
+ * last and second-minus-first value); speed_limits = {vP min, vP max, vE
+ * min, vE max}. */
+int pe_table_create(const float *host_frames, int32_t frames, const double *times,
+                    const int32_t shape[5], const double axis_lo[5], const double axis_hi[5],
+                    const double spacing[5], double capture_radius,
+                    const double speed_limits[4], int32_t device, pe_table **out);
+/* Capture times of n states [n][5] = (x, y, psi, vP, vE) (host arrays). */
+int pe_table_value(pe_table *h, const double *host_states, int64_t n, double *host_out);
+/* Signed field of n states at budgets[n] (host arrays). */
+int pe_table_field(pe_table *h, const double *host_states, const double *host_budgets,
+                   int64_t n, double *host_out);
+int pe_table_destroy(pe_table *h);
 
 #ifdef __cplusplus
 }

@@ -27,6 +27,7 @@ struct pe_semilag {
   pe::SLSpeedStep *pstep = nullptr, *estep = nullptr;
   uint8_t *hint = nullptr;
   pe::SLTiledPlan plan{};
+  int smem_limit = 0;  // dynamic shared memory available to the tiled kernel
   bool tiled_ok = false;    // the tiled kernel applies to this grid and dt
   bool tiled_auto = false;  // ... and has enough work items to be the faster one
   int kernel = PE_SL_KERNEL_AUTO;
@@ -298,9 +299,10 @@ int pe_semilag_create(const pe_semilag_params *params, pe_semilag **out) {
     int optin = 0;
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin,
                            params->device);
+    h->smem_limit = optin - 1024;
     h->tiled_ok = speed_steps(parc, g.nvp, &pstep) && speed_steps(earc, g.nve, &estep) &&
                   tiled_geometry_ok(g, parc, earc, emove) &&
-                  pe::sl_tiled_plan(g, optin - 1024, &h->plan);
+                  pe::sl_tiled_plan(g, optin - 1024, 0, &h->plan);
     // one CTA per SM: with fewer than ~8 items per SM the tail of the last
     // wave and the per-item ring warm-up outweigh the gain (measured on a
     // 33x24x11x11 grid: 1.46 ms tiled vs 0.81 ms generic per backup)
@@ -510,6 +512,27 @@ int pe_semilag_set_kernel(pe_semilag *h, int kernel) {
   if (kernel == PE_SL_KERNEL_TILED && !h->tiled_ok)
     return fail(PE_EINVAL, "the tiled backup kernel does not apply to this grid and dt");
   h->kernel = kernel;
+  return PE_OK;
+}
+
+int pe_semilag_set_tile(pe_semilag *h, int32_t rows) {
+  int rc = enter(h);
+  if (rc) return rc;
+  if (!h->tiled_ok) return fail(PE_EINVAL, "the tiled backup kernel does not apply");
+  pe::SLTiledPlan plan{};
+  if (rows < 0 || !pe::sl_tiled_plan(h->g, h->smem_limit, rows, &plan))
+    return fail(PE_EINVAL, "tile of %d rows does not fit the tiled kernel", rows);
+  PE_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  h->plan = plan;
+  return PE_OK;
+}
+
+int pe_semilag_get_tile(const pe_semilag *h, int32_t *rows, int32_t *threads,
+                        int64_t *items) {
+  if (!h) return fail(PE_EINVAL, "handle is NULL");
+  if (rows) *rows = h->tiled_ok ? h->plan.rows : 0;
+  if (threads) *threads = h->tiled_ok ? h->plan.threads : 0;
+  if (items) *items = h->tiled_ok ? h->plan.items : 0;
   return PE_OK;
 }
 

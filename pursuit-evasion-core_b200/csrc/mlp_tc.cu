@@ -197,10 +197,14 @@ __global__ void __launch_bounds__(THREADS, 1)
   }
   __syncwarp();
 
-  // epilogue: thread (warp w, lane l) owns tile row 32 w + l
+  // epilogue: warp w reads accumulator lanes (tile rows) 32w..32w+31, 32
+  // columns at a time (thread l holds row 32w + l), turns the 32 x 32 block
+  // around in shared memory (the operand ring is idle once `done` fired)
+  // and stores it row by row, lane l on column l: coalesced loads of the
+  // pre-activation and coalesced stores
   const bool have = mbar_wait(done, 0, g.error);
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  const int row = m0 + warp * 32 + lane;
+  float *stage = reinterpret_cast<float *>(sA) + warp * 32 * 33;
 #pragma unroll 1
   for (int c0 = 0; c0 < TN; c0 += 32) {
     uint32_t r[32];
@@ -217,32 +221,29 @@ __global__ void __launch_bounds__(THREADS, 1)
           "=r"(r[31])
         : "r"(taddr));
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-    if (!have || row >= g.M) continue;
-    const int n = n0 + c0;
-    const size_t o = (size_t)row * g.ldc + n;
-    if (EPI == 0) {
 #pragma unroll
-      for (int j = 0; j < 32; j += 4)
-        *reinterpret_cast<float4 *>(g.C32 + o + j) =
-            make_float4(__uint_as_float(r[j]), __uint_as_float(r[j + 1]),
-                        __uint_as_float(r[j + 2]), __uint_as_float(r[j + 3]));
-    } else if (EPI == 1) {
-#pragma unroll
-      for (int j = 0; j < 32; j += 2) {
-        const float z0 = __uint_as_float(r[j]) + g.bias[n + j];
-        const float z1 = __uint_as_float(r[j + 1]) + g.bias[n + j + 1];
-        if (g.C32) *reinterpret_cast<float2 *>(g.C32 + o + j) = make_float2(z0, z1);
-        *reinterpret_cast<__nv_bfloat162 *>(g.C16 + o + j) =
-            __floats2bfloat162_rn(silu(z0), silu(z1));
-      }
-    } else {
-#pragma unroll
-      for (int j = 0; j < 32; j += 2) {
-        const float2 z = *reinterpret_cast<const float2 *>(g.zpre + o + j);
-        *reinterpret_cast<__nv_bfloat162 *>(g.C16 + o + j) = __floats2bfloat162_rn(
-            __uint_as_float(r[j]) * silu_grad(z.x), __uint_as_float(r[j + 1]) * silu_grad(z.y));
+    for (int j = 0; j < 32; j++) stage[lane * 33 + j] = __uint_as_float(r[j]);
+    __syncwarp();
+    if (have) {
+      const int n = n0 + c0 + lane;
+      const float bn = EPI == 1 ? g.bias[n] : 0.f;
+#pragma unroll 4
+      for (int rr = 0; rr < 32; rr++) {
+        const int row = m0 + warp * 32 + rr;
+        const size_t o = (size_t)row * g.ldc + n;
+        const float acc = stage[rr * 33 + lane];
+        if (EPI == 0) {
+          g.C32[o] = acc;
+        } else if (EPI == 1) {
+          const float z = acc + bn;
+          if (g.C32) g.C32[o] = z;
+          g.C16[o] = __float2bfloat16_rn(silu(z));
+        } else {
+          g.C16[o] = __float2bfloat16_rn(acc * silu_grad(g.zpre[o]));
+        }
       }
     }
+    __syncwarp();
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();

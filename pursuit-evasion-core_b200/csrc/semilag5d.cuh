@@ -80,9 +80,10 @@ struct SLTiledPlan {
   size_t smem;     // dynamic shared memory per CTA
 };
 
-// Tile plan for grid g within max_smem bytes of dynamic shared memory;
-// false if the grid's width does not fit the tiled kernel.
-bool sl_tiled_plan(const SLGrid &g, int max_smem, SLTiledPlan *plan);
+// Tile plan for grid g within max_smem bytes of dynamic shared memory
+// (want_rows > 0: about that many cell rows per tile, else the default);
+// false if the grid's width or the tile does not fit the tiled kernel.
+bool sl_tiled_plan(const SLGrid &g, int max_smem, int want_rows, SLTiledPlan *plan);
 
 cudaError_t sl_backup_tiled(const SLGrid &g, const SLBackup &b, const SLTiled &t,
                             const SLTiledPlan &plan, cudaStream_t stream);

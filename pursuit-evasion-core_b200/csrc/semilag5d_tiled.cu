@@ -26,6 +26,9 @@
 // are described at minmax_cell; min and max are exact, so the value does
 // not depend on the visiting order.
 //
+// The grid holds as many CTAs as fit on the SMs at once (one for the
+// default tile, two for tiles of about 6 rows).
+//
 // Preconditions (checked on the host): nx + 4 <= 72, every successor within
 // 1.99 cells of its cell in x and y, heading shifts below one plane, and
 // speed successors inside the three staged slabs.
@@ -431,18 +434,23 @@ cudaError_t launch(const SLGrid &g, const SLBackup &b, const SLTiled &t,
   if (err != cudaSuccess) return err;
   err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   if (err != cudaSuccess) return err;
-  const int64_t grid = plan.items < sms ? plan.items : sms;
+  int resident = 0;
+  err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, kernel, plan.threads,
+                                                      plan.smem);
+  if (err != cudaSuccess) return err;
+  const int64_t slots = (int64_t)sms * (resident > 0 ? resident : 1);
+  const int64_t grid = plan.items < slots ? plan.items : slots;
   kernel<<<(unsigned)grid, plan.threads, plan.smem, stream>>>(g, b, t, plan);
   return cudaGetLastError();
 }
 
 }  // namespace
 
-bool sl_tiled_plan(const SLGrid &g, int max_smem, SLTiledPlan *plan) {
+bool sl_tiled_plan(const SLGrid &g, int max_smem, int want_rows, SLTiledPlan *plan) {
   const int nx = g.nx;
   if (nx + 2 * kHalo > kPitch || g.nvp < 3 || g.nve < 3) return false;
   // rows per tile: about 864 cells (432 threads), at most 16 rows, equal tiles
-  int rows = 864 / nx;
+  int rows = want_rows > 0 ? want_rows : 864 / nx;
   rows = rows < 1 ? 1 : (rows > 16 ? 16 : rows);
   const int tiles = (nx + rows - 1) / rows;
   rows = (nx + tiles - 1) / tiles;

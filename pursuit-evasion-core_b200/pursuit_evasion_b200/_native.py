@@ -166,6 +166,12 @@ SIGNATURES = {
     "pe_batch_profile": (ctypes.c_int, [_P, ctypes.c_int]),
     "pe_batch_kernel_time": (ctypes.c_int, [_P, _DP, _I64P]),
     "pe_batch_destroy": (ctypes.c_int, [_P]),
+    "pe_table_create": (ctypes.c_int, [_P, ctypes.c_int32, _DP, ctypes.POINTER(ctypes.c_int32),
+                                       _DP, _DP, _DP, ctypes.c_double, _DP, ctypes.c_int32,
+                                       ctypes.POINTER(ctypes.c_void_p)]),
+    "pe_table_value": (ctypes.c_int, [_P, _DP, ctypes.c_int64, _DP]),
+    "pe_table_field": (ctypes.c_int, [_P, _DP, _DP, ctypes.c_int64, _DP]),
+    "pe_table_destroy": (ctypes.c_int, [_P]),
     "pe_world_cells": (ctypes.c_int, [ctypes.POINTER(WorldParams), _I64P]),
     "pe_world_dt_limit": (ctypes.c_int, [ctypes.POINTER(WorldParams), _DP]),
     "pe_world_create": (ctypes.c_int, [ctypes.POINTER(WorldParams),
@@ -202,6 +208,9 @@ SIGNATURES = {
     "pe_semilag_set_stream": (ctypes.c_int, [_P, _P]),
     "pe_semilag_set_kernel": (ctypes.c_int, [_P, ctypes.c_int]),
     "pe_semilag_kernel": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int32)]),
+    "pe_semilag_set_tile": (ctypes.c_int, [_P, ctypes.c_int32]),
+    "pe_semilag_get_tile": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int32),
+                                           ctypes.POINTER(ctypes.c_int32), _I64P]),
     "pe_semilag_profile": (ctypes.c_int, [_P, ctypes.c_int]),
     "pe_semilag_kernel_time": (ctypes.c_int, [_P, _DP, _I64P]),
     "pe_semilag_destroy": (ctypes.c_int, [_P]),

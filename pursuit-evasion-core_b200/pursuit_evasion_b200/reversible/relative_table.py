@@ -10,6 +10,7 @@ this package (or by the reference) can be read without the reference:
     * signed field at a budget             relative_table.py:104-117
     * capture time = first zero crossing
       by bisection over frames             relative_table.py:119-161
+`DeviceRelativeTable` answers the same queries with the table on the GPU.
 """
 
 from __future__ import annotations
@@ -150,3 +151,75 @@ class RelativeTable:
         out = self.times[lo] + np.clip(frac, 0, 1) * (self.times[hi] - self.times[lo])
         out = np.where(valid, out, np.nan)
         return np.where(captured & self._physical(flat), 0, out).reshape(batch)
+
+
+class DeviceRelativeTable:
+    """A completed table resident on a CUDA device (pe_table_*): the same
+    `field` and `value` queries as RelativeTable, for batches of states,
+    evaluated by GPU kernels in double precision."""
+
+    def __init__(self, table, device=0):
+        import ctypes
+
+        from .. import _native
+
+        self._ctypes = ctypes
+        self._native = _native
+        self._lib = _native.library()
+        self.table = table
+        frames = np.ascontiguousarray(table.fields, dtype=np.float32)
+        times = np.ascontiguousarray(table.times, dtype=np.float64)
+        shape = (ctypes.c_int32 * 5)(*table.shape)
+        lo = (ctypes.c_double * 5)(*[float(a[0]) for a in table.axes])
+        hi = (ctypes.c_double * 5)(*[float(a[-1]) for a in table.axes])
+        h = (ctypes.c_double * 5)(*[float(x) for x in table.spacings])
+        ph = table.physics
+        limits = (ctypes.c_double * 4)(ph["pursuer"]["speed_min"], ph["pursuer"]["speed_max"],
+                                       ph["evader"]["speed_min"], ph["evader"]["speed_max"])
+        handle = ctypes.c_void_p()
+        _native.check(self._lib.pe_table_create(
+            frames.ctypes.data, len(times), times.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+            shape, lo, hi, h, float(ph["capture_radius"]), limits, int(device),
+            ctypes.byref(handle)))
+        self._h = handle
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.pe_table_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _states(self, states):
+        states = np.asarray(states, dtype=np.float64)
+        if states.ndim < 1 or states.shape[-1] != 5:
+            raise ValueError("Relative states must end in [x,y,psi,vP,vE]")
+        return np.ascontiguousarray(states.reshape(-1, 5)), states.shape[:-1]
+
+    def value(self, states):
+        flat, batch = self._states(states)
+        out = np.empty(len(flat), np.float64)
+        if len(flat):
+            dp = self._ctypes.POINTER(self._ctypes.c_double)
+            self._native.check(self._lib.pe_table_value(
+                self._h, flat.ctypes.data_as(dp), len(flat), out.ctypes.data_as(dp)))
+        return out.reshape(batch)
+
+    def field(self, states, budget):
+        flat, batch = self._states(states)
+        tau = np.ascontiguousarray(
+            np.broadcast_to(np.asarray(budget, dtype=np.float64), batch).reshape(-1))
+        out = np.empty(len(flat), np.float64)
+        if len(flat):
+            dp = self._ctypes.POINTER(self._ctypes.c_double)
+            self._native.check(self._lib.pe_table_field(
+                self._h, flat.ctypes.data_as(dp), tau.ctypes.data_as(dp), len(flat),
+                out.ctypes.data_as(dp)))
+        return out.reshape(batch)

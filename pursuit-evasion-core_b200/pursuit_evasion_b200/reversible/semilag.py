@@ -146,6 +146,17 @@ class SemiLagrangianSolver:
             raise ValueError("kernel must be 'auto', 'generic' or 'tiled'")
         _native.check(self._lib.pe_semilag_set_kernel(self._h, KERNELS[kernel]))
 
+    def set_tile(self, rows):
+        """About `rows` cell rows per tiled-kernel work item (0: default)."""
+        _native.check(self._lib.pe_semilag_set_tile(self._h, int(rows)))
+
+    @property
+    def tile(self):
+        r, t, n = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int64()
+        _native.check(self._lib.pe_semilag_get_tile(self._h, ctypes.byref(r), ctypes.byref(t),
+                                                    ctypes.byref(n)))
+        return dict(rows=r.value, threads=t.value, items=n.value)
+
     @property
     def kernel(self):
         k = ctypes.c_int32()
