@@ -11,10 +11,13 @@
 // SiLU (FP32 pre-activation optional, BF16 activation), 3 product with
 // SiLU'(pre-activation) to BF16.
 //
-// CTA tile 128 x 128 x 64, 4 pipeline stages, 128 threads: warp 0 lane 0
-// issues the TMA loads, warp 1 lane 0 the MMAs (4 of K=16 per stage); all
-// four warps run the epilogue, warp w on accumulator lanes 32w..32w+31
-// (= tile rows).  Every mbarrier wait is bounded; a timed-out wait sets the
+// CTA tile 128 x TN x 64 (TN = 256 where N allows, else 128), 2 pipeline
+// stages (the surrogate's K is 128 or 256; 97 KB of shared memory and 256
+// tensor-memory columns let two CTAs share an SM, so one's epilogue
+// overlaps the other's loads and MMAs), 128 threads: warp 0 lane 0 issues
+// the TMA loads, warp 1 lane 0 the MMAs (4 of K=16 per stage); all four
+// warps run the epilogue, warp w on accumulator lanes 32w..32w+31 (= tile
+// rows).  Every mbarrier wait is bounded; a timed-out wait sets the
 // error flag and the CTA still releases its tensor memory.
 #include <cuda.h>
 #include <cuda_bf16.h>
@@ -24,9 +27,8 @@
 namespace pe {
 namespace {
 
-constexpr int TM = 128, TN = 128, TK = 64, STAGES = 4, THREADS = 128;
-constexpr int A_BYTES = TM * TK * 2, B_BYTES = TN * TK * 2;  // 16 KB each
-constexpr uint32_t TMEM_COLS = 128;
+constexpr int TM = 128, TK = 64, STAGES = 2, THREADS = 128;
+constexpr int A_BYTES = TM * TK * 2;  // 16 KB
 constexpr uint32_t WAIT_LIMIT = 1u << 24;
 
 __device__ __forceinline__ float silu(float z) { return z / (1.f + __expf(-z)); }
@@ -93,19 +95,23 @@ __device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t addr) {
   return d;
 }
 
-// Instruction descriptor: BF16 x BF16 -> FP32, both K-major, M = 128, N = 128.
-constexpr uint32_t kIdesc = (1u << 4)            // D format FP32
-                            | (1u << 7)          // A format BF16
-                            | (1u << 10)         // B format BF16
-                            | ((uint32_t)(TN >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
+// Instruction descriptor: BF16 x BF16 -> FP32, both K-major, M = 128, N = TN.
+template <int TN>
+__host__ __device__ constexpr uint32_t idesc() {
+  return (1u << 4)      // D format FP32
+         | (1u << 7)    // A format BF16
+         | (1u << 10)   // B format BF16
+         | ((uint32_t)(TN >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
+}
 
+template <int TN>
 __device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db,
                                          uint32_t accumulate) {
   asm volatile(
       "{\n .reg .pred p;\n"
       " setp.ne.b32 p, %4, 0;\n"
       " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}" ::"r"(tmem_d),
-      "l"(da), "l"(db), "r"(kIdesc), "r"(accumulate)
+      "l"(da), "l"(db), "r"(idesc<TN>()), "r"(accumulate)
       : "memory");
 }
 
@@ -124,10 +130,12 @@ struct TcArgs {
   unsigned *error;
 };
 
-template <int EPI>
+template <int EPI, int TN>
 __global__ void __launch_bounds__(THREADS, 1)
     gemm_tc_kernel(const __grid_constant__ CUtensorMap tma_a,
                    const __grid_constant__ CUtensorMap tma_b, const TcArgs g) {
+  constexpr int B_BYTES = TN * TK * 2;
+  constexpr uint32_t TMEM_COLS = TN;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   // 1024-byte alignment of every tile (the swizzle atom)
   uint8_t *base = reinterpret_cast<uint8_t *>(
@@ -189,8 +197,8 @@ __global__ void __launch_bounds__(THREADS, 1)
       const uint32_t a0 = smem_u32(sA + s * A_BYTES), b0 = smem_u32(sB + s * B_BYTES);
 #pragma unroll
       for (int kk = 0; kk < TK / 16; kk++)  // K = 16 per instruction: 32 bytes along a row
-        mma_bf16(tmem, smem_desc_sw128(a0 + kk * 32), smem_desc_sw128(b0 + kk * 32),
-                 (k | kk) != 0);
+        mma_bf16<TN>(tmem, smem_desc_sw128(a0 + kk * 32), smem_desc_sw128(b0 + kk * 32),
+                     (k | kk) != 0);
       mma_commit(&empty[s]);  // frees the stage when these MMAs complete
     }
     mma_commit(done);  // the accumulator is complete (or the loop stopped early)
@@ -253,10 +261,13 @@ __global__ void __launch_bounds__(THREADS, 1)
                  : "memory");
 }
 
-constexpr size_t kSmemBytes = 1024 + STAGES * (A_BYTES + B_BYTES) + (2 * STAGES + 1) * 8 + 16;
+template <int TN>
+__host__ __device__ constexpr size_t smem_bytes() {
+  return 1024 + STAGES * (A_BYTES + TN * TK * 2) + (2 * STAGES + 1) * 8 + 16;
+}
 
 // 2D tensor map of a K-major bf16 matrix [rows][K] with row pitch ld
-// elements, box 64 (K) x 128 (rows), 128-byte swizzle.
+// elements, box 64 (K) x box_rows, 128-byte swizzle.
 // The driver's tensor-map encoder, fetched through the runtime so that the
 // library does not link libcuda (it loads on machines without a driver).
 using EncodeTiled = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
@@ -277,10 +288,10 @@ EncodeTiled encoder() {
   return fn;
 }
 
-CUresult make_map(CUtensorMap *map, const void *ptr, int rows, int K, int ld) {
+CUresult make_map(CUtensorMap *map, const void *ptr, int rows, int K, int ld, int box_rows) {
   const cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
   const cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
-  const cuuint32_t box[2] = {TK, 128};
+  const cuuint32_t box[2] = {TK, (cuuint32_t)box_rows};
   const cuuint32_t elem[2] = {1, 1};
   EncodeTiled encode = encoder();
   if (!encode) return CUDA_ERROR_NOT_FOUND;
@@ -298,15 +309,24 @@ unsigned *error_word() {
   return word;
 }
 
-template <int EPI>
+template <int EPI, int TN>
 cudaError_t launch(const CUtensorMap &a, const CUtensorMap &b, const TcArgs &g,
                    cudaStream_t stream) {
-  auto kernel = gemm_tc_kernel<EPI>;
+  auto kernel = gemm_tc_kernel<EPI, TN>;
+  constexpr size_t smem = smem_bytes<TN>();
   cudaError_t e =
-      cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes);
+      cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  kernel<<<dim3(g.N / TN, g.M / TM), THREADS, kSmemBytes, stream>>>(a, b, g);
+  kernel<<<dim3(g.N / TN, g.M / TM), THREADS, smem, stream>>>(a, b, g);
   return cudaGetLastError();
+}
+
+template <int TN>
+cudaError_t launch_epi(int epilogue, const CUtensorMap &a, const CUtensorMap &b,
+                       const TcArgs &g, cudaStream_t s) {
+  return epilogue == 0   ? launch<0, TN>(a, b, g, s)
+         : epilogue == 1 ? launch<1, TN>(a, b, g, s)
+                         : launch<3, TN>(a, b, g, s);
 }
 
 }  // namespace
@@ -318,7 +338,7 @@ int pe_mlp_gemm_tc(const void *A, const void *B, int M, int N, int K, int lda, i
                    int epilogue, float *C32, void *C16, int ldc, const float *bias,
                    const float *zpre, void *cuda_stream) {
   using namespace pe;
-  if (!A || !B || M <= 0 || N <= 0 || K <= 0 || M % TM || N % TN || K % TK)
+  if (!A || !B || M <= 0 || N <= 0 || K <= 0 || M % TM || N % 128 || K % TK)
     return fail(PE_EINVAL, "gemm_tc: M, N multiples of 128, K a multiple of 64");
   if ((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(B)) % 16 || lda % 8 ||
       ldb % 8 || lda < K || ldb < K)
@@ -330,15 +350,18 @@ int pe_mlp_gemm_tc(const void *A, const void *B, int M, int N, int K, int lda, i
   if (epilogue == 1 && !bias) return fail(PE_EINVAL, "gemm_tc: bias required");
   if (epilogue == 3 && !zpre) return fail(PE_EINVAL, "gemm_tc: zpre required");
   if (ldc % 4) return fail(PE_EINVAL, "gemm_tc: ldc must be a multiple of 4");
+  // a CTA covers 128 x 256 of C where N allows and that still gives two
+  // CTAs per SM of the device (148 SMs: 296), else 128 x 128
+  const int tn = N % 256 == 0 && (int64_t)(M / TM) * (N / 256) >= 296 ? 256 : 128;
   CUtensorMap ma, mb;
-  if (make_map(&ma, A, M, K, lda) != CUDA_SUCCESS || make_map(&mb, B, N, K, ldb) != CUDA_SUCCESS)
+  if (make_map(&ma, A, M, K, lda, TM) != CUDA_SUCCESS ||
+      make_map(&mb, B, N, K, ldb, tn) != CUDA_SUCCESS)
     return fail(PE_EINVAL, "gemm_tc: tensor map encoding failed");
   TcArgs g{M, N, K, ldc, C32, static_cast<__nv_bfloat16 *>(C16), bias, zpre, error_word()};
   if (!g.error) return fail(PE_ENOMEM, "gemm_tc: error word");
   cudaStream_t s = static_cast<cudaStream_t>(cuda_stream);
-  cudaError_t e = epilogue == 0   ? launch<0>(ma, mb, g, s)
-                  : epilogue == 1 ? launch<1>(ma, mb, g, s)
-                                  : launch<3>(ma, mb, g, s);
+  cudaError_t e = tn == 256 ? launch_epi<256>(epilogue, ma, mb, g, s)
+                            : launch_epi<128>(epilogue, ma, mb, g, s);
   if (e != cudaSuccess) return cuda_fail(e, "pe_mlp_gemm_tc");
   count_launches(1);
   return PE_OK;

@@ -116,14 +116,16 @@ class ValueMLP:
             _native.check(self.lib.pe_mlp_transpose(_ptr(w), _ptr(wt), w.shape[0], w.shape[1],
                                                     self._stream()))
 
-    def forward(self, rows, *, target=False):
+    def forward(self, rows, *, target=False, inference=False):
         """Forward over self.feat[:rows]; with target=True also the MSE loss
-        (accumulated into self.loss) and dy."""
+        (accumulated into self.loss) and dy.  inference=True skips storing
+        the FP32 pre-activations, which only backward() reads."""
         x = self.feat
         for l in range(self.layers):
             K = FEATURES if l == 0 else self.hidden
-            self._gemm_tc(x, self.w16[l], rows, self.hidden, K, 1, C32=self.z[l],
-                          C16=self.h[l], bias=self.b[l])
+            self._gemm_tc(x, self.w16[l], rows, self.hidden, K, 1,
+                          C32=None if inference else self.z[l], C16=self.h[l],
+                          bias=self.b[l])
             x = self.h[l]
         _native.check(self.lib.pe_mlp_head_forward(
             _ptr(self.h[-1]), _ptr(self.w_out), _ptr(self.b_out),

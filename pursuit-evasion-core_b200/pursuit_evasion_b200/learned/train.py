@@ -126,7 +126,7 @@ def predict_nodes(net, sampler, out, *, chunk=8192):
         torch.arange(start, start + padded, out=idx[:padded], device=dev)
         idx[:padded].clamp_(max=n - 1)
         sampler.encode(net, idx, padded, False)
-        y = net.forward(padded)
+        y = net.forward(padded, inference=True)
         out[start:start + rows].copy_(y[:rows])
     return out
 
@@ -145,4 +145,5 @@ def predict_states(net, config, extent, states):
         float(e.speed_min), float(e.speed_max), _ptr(net.feat), FEATURES, net._stream()))
     if padded > n:
         net.feat[n:padded].zero_()
-    return net.forward(padded)[:n].clone()  # the network's output buffer is reused
+    # the network's output buffer is reused: copy the answers out
+    return net.forward(padded, inference=True)[:n].clone()

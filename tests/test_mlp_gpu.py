@@ -151,17 +151,20 @@ def gemm_tc_case(epi, M=256, N=256, K=256, seed=0):
     return ref, bias, zpre, C32.cpu(), C16.float().cpu()
 
 
-@pytest.mark.parametrize("M, N, K", [(128, 128, 64), (256, 256, 256), (1024, 256, 128)])
+# the last shape takes the 128 x 256 tiles (enough rows for two CTAs per SM)
+@pytest.mark.parametrize("M, N, K", [(128, 128, 64), (256, 256, 256), (1024, 256, 128),
+                                     (38016, 256, 128)])
 def test_tensor_core_gemm_matches_fp32_reference(M, N, K):
     ref, _, _, C32, _ = gemm_tc_case(0, M=M, N=N, K=K)
     torch.testing.assert_close(C32, ref, rtol=1e-4, atol=1e-3)
 
 
-def test_tensor_core_gemm_epilogues():
-    ref, bias, _, C32, C16 = gemm_tc_case(1)
+@pytest.mark.parametrize("M", [256, 38016])
+def test_tensor_core_gemm_epilogues(M):
+    ref, bias, _, C32, C16 = gemm_tc_case(1, M=M)
     z = ref + bias
     torch.testing.assert_close(C32, z, rtol=1e-4, atol=1e-3)
     torch.testing.assert_close(C16, torch.nn.functional.silu(z), rtol=1e-2, atol=2e-2)
-    ref, _, zpre, _, C16 = gemm_tc_case(3)
+    ref, _, zpre, _, C16 = gemm_tc_case(3, M=M)
     s = torch.sigmoid(zpre)
     torch.testing.assert_close(C16, ref * s * (1 + zpre * (1 - s)), rtol=1e-2, atol=5e-2)
