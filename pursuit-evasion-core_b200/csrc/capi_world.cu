@@ -47,6 +47,11 @@ int validate(const pe_world_params *p) {
       p->e_curvature <= 0 || p->extent <= 0 ||
       (p->avoid_mode != 0 && p->avoid_mode != 1) || (p->fast != 0 && p->fast != 1))
     return fail(PE_EINVAL, "Invalid arguments");
+  // each car's block of cells is indexed with 32-bit integers on the device
+  const int64_t block_p = (int64_t)p->positions * p->positions * p->headings * p->p_speeds;
+  const int64_t block_e = (int64_t)p->positions * p->positions * p->headings * p->e_speeds;
+  if (block_p >= (int64_t)1 << 31 || block_e >= (int64_t)1 << 31)
+    return fail(PE_EINVAL, "Invalid arguments: grid too large");
   return PE_OK;
 }
 

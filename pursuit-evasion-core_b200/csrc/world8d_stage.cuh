@@ -18,8 +18,8 @@ __device__ __forceinline__ float ghost(const float *__restrict__ v, int64_t j,
                                        int64_t stride, int pos, int n,
                                        int offset, bool periodic) {
   int q = pos + offset;
-  if (periodic) {
-    q = (q % n + n) % n;
+  if (periodic) {  // |offset| <= 2 <= n: one wrap at most
+    q = q < 0 ? q + n : (q >= n ? q - n : q);
     return v[j + (int64_t)(q - pos) * stride];
   }
   if (q < 0) {
@@ -80,23 +80,23 @@ template <bool FAST>
 __global__ void __launch_bounds__(256)
     world8_stage_kernel(const World8Grid g, const World8Stage s) {
   __shared__ float warp_max[8];
-  const int64_t inner = (int64_t)g.shape[4] * g.shape[5] * g.shape[6] * g.shape[7];
-  const int64_t outer = g.cells / inner;
+  const int inner = g.shape[4] * g.shape[5] * g.shape[6] * g.shape[7];
+  const int outer = g.shape[0] * g.shape[1] * g.shape[2] * g.shape[3];
   const int e_cell = blockIdx.x * blockDim.x + threadIdx.x;
   float change_max = 0.f;
   bool bad = false;
-  for (int64_t o = blockIdx.y; o < outer; o += gridDim.y) {
+  for (int o = blockIdx.y; o < outer; o += gridDim.y) {
     if (e_cell < inner) {
-      const int64_t j = o * inner + e_cell;
+      const int64_t j = (int64_t)o * inner + e_cell;
       int q[8];
       {
-        int64_t rest = o;
-        q[3] = (int)(rest % g.shape[3]);
+        int rest = o;
+        q[3] = rest % g.shape[3];
         rest /= g.shape[3];
-        q[2] = (int)(rest % g.shape[2]);
+        q[2] = rest % g.shape[2];
         rest /= g.shape[2];
-        q[1] = (int)(rest % g.shape[1]);
-        q[0] = (int)(rest / g.shape[1]);
+        q[1] = rest % g.shape[1];
+        q[0] = rest / g.shape[1];
         int e = e_cell;
         q[7] = e % g.shape[7];
         e /= g.shape[7];
