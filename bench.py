@@ -667,7 +667,7 @@ def main():
     parser.add_argument("--no-cpu-baseline", action="store_true")
     parser.add_argument("--no-sections", action="store_true",
                         help="skip the 8D and semi-Lagrangian side measurements")
-    parser.add_argument("--converge", action=argparse.BooleanOptionalAction, default=False,
+    parser.add_argument("--converge", action=argparse.BooleanOptionalAction, default=True,
                         help="time-to-converged table, plain vs learned warm start")
     parser.add_argument("--samples", type=int, default=1 << 22)
     parser.add_argument("--epochs", type=int, default=20)
