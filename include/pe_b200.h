@@ -469,6 +469,85 @@ int pe_table_field(pe_table *h, const double *host_states, const double *host_bu
                    int64_t n, double *host_out);
 int pe_table_destroy(pe_table *h);
 
+/* ------------------------------------------------------------------------
+ * Compact eight-state semi-Lagrangian contact game (local pair game).
+ *
+ * Replaces the CuPy RawKernels and host loops of
+ * src/pursuit_evasion/local_game/grid_game.py:
+ *   gpu_arrays / initialize_gpu / backup_gpu            :226-333 (dense)
+ *   packed_gpu_arrays / initialize_packed / backup_packed :424-581 (pairs
+ *                                                        within the exit radius)
+ * and the packed query of local_game/reference.py:122-134 (query_field).
+ *
+ * Each car has n legal four-dimensional states (x, y, heading, speed) and
+ * n_actions held controls; a control's successor is a 16-vertex
+ * interpolation stencil (ids, weights) over the car's own states.  One
+ * backup sets, for every pair (ip, ie) of the domain,
+ *   V'(ip, ie) = min(V, min_{u allowed} max_{a allowed}
+ *                sum_q we[q] sum_k wp[k] V(idp[k], ide[q]))
+ * (the reference's factorized product interpolation; its early exit
+ * `worst >= best` is kept).  The dense layout is [n_p][n_e]; pairs farther
+ * apart than the exit radius keep their value.  The packed layout stores
+ * only the domain's pairs (PairDomain, grid_game.py:336-381); a vertex
+ * outside the domain, or an evader state beyond the pursuer's reach, reads
+ * the exit value.  Unlike the reference, one launch performs a whole backup
+ * with the field resident on the device (no per-chunk launches, no host
+ * round trip of the output tiles).
+ * ------------------------------------------------------------------------ */
+typedef struct pe_compact pe_compact;
+
+/* One car's grid (VehicleGrid, grid_game.py:21-30); host arrays, copied. */
+typedef struct pe_vehicle_grid {
+  int32_t states;          /* n */
+  int32_t actions;         /* n_actions */
+  const float *pose;       /* [n][4] x, y, heading, speed */
+  const int32_t *ids;      /* [n][n_actions][16] successor vertex ids */
+  const float *weights;    /* [n][n_actions][16] vertex weights (<= 0: unused) */
+  const uint8_t *allowed;  /* [n][n_actions] */
+} pe_vehicle_grid;
+
+/* PairDomain (grid_game.py:336-381); host arrays, copied. */
+typedef struct pe_pair_domain {
+  int32_t positions;         /* distinct pursuer positions */
+  int32_t max_count;         /* row length of e_indices */
+  const int32_t *p_position; /* [n_p] position index of each pursuer state */
+  const int32_t *lookup;     /* [positions][n_e] rank of an evader state, -1 outside */
+  const int32_t *e_indices;  /* [positions][max_count] evader states in range */
+  const int32_t *counts;     /* [positions] */
+  const int64_t *offsets;    /* [n_p + 1] first pair of each pursuer state */
+} pe_pair_domain;
+
+/* domain == NULL: dense layout.  exit_radius: the domain's radius (packed)
+ * or the capture field's exit radius (dense). */
+int pe_compact_create(const pe_vehicle_grid *p, const pe_vehicle_grid *e,
+                      const pe_pair_domain *domain, double exit_radius,
+                      int32_t device, pe_compact **out);
+/* Number of stored pairs (n_p * n_e dense, offsets[n_p] packed). */
+int pe_compact_cells(const pe_compact *h, int64_t *out);
+/* Capture field: oriented-rectangle separation of the two footprints in
+ * float32 (grid_game.py:193-201 / :364-372); dense pairs beyond the exit
+ * radius get the exit radius. */
+int pe_compact_init(pe_compact *h, double p_length, double p_width, double e_length,
+                    double e_width);
+int pe_compact_set_field(pe_compact *h, const float *host, int64_t n);
+/* `count` backups, each one kernel launch on the handle's stream. */
+int pe_compact_backup(pe_compact *h, int32_t count);
+int pe_compact_copy_field(pe_compact *h, float *host, int64_t n);
+/* Device pointer of the current field (valid until the next backup). */
+int pe_compact_field_device(pe_compact *h, void **out);
+/* n queries, each a product of a pursuer and an evader 16-vertex stencil
+ * (host arrays [n][16]); packed handles read the exit value outside the
+ * domain (reference.py:122-134). */
+int pe_compact_query(pe_compact *h, int32_t n, const int32_t *p_ids,
+                     const float *p_weights, const int32_t *e_ids,
+                     const float *e_weights, float *host_out);
+int pe_compact_set_stream(pe_compact *h, void *cuda_stream);
+int pe_compact_synchronize(pe_compact *h);
+/* Device time of the backups since profiling was switched on. */
+int pe_compact_profile(pe_compact *h, int32_t enable);
+int pe_compact_kernel_time(pe_compact *h, double *ms, int64_t *launches);
+int pe_compact_destroy(pe_compact *h);
+
 #ifdef __cplusplus
 }
 #endif

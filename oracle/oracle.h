@@ -52,6 +52,10 @@ void po_w8_init_contact(const po_w8_cfg *c, double p_len, double p_wid,
                         double e_len, double e_wid, float *a, float *arrival);
 int po_w8_stage(const po_w8_cfg *c, const float *src, float *dst,
                 const float *base, float *arrival, float dt, double tau);
+/* The same stage in double precision on double fields (no arrival): the
+ * rounding-free reference for float32 variants of the step. */
+int po_w8_stage_f64(const po_w8_cfg *c, const double *src, double *dst,
+                    const double *base, double dt);
 
 /* Relative 5D semi-Lagrangian backup (FP64). */
 #define PO_SL_TUBE 0

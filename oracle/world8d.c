@@ -296,3 +296,128 @@ int po_w8_stage(const po_w8_cfg *c, const float *src, float *dst,
   w8_free(&g);
   return bad ? PO_ENONFINITE : 0;
 }
+
+/* ------------------------------------------------------------------------
+ * The same stage in double precision (double fields, the float32 grid axes
+ * and spacings promoted to double): the rounding-free reference against
+ * which float32 variants of the step are measured.  Same formulas and
+ * order as po_w8_stage. */
+static inline double ghost_f64(const double *v, size_t j, size_t stride,
+                               int pos, int n, int offset, int periodic) {
+  int q = pos + offset;
+  if (periodic) {
+    q = (q % n + n) % n;
+    return v[(ptrdiff_t)j + (ptrdiff_t)(q - pos) * (ptrdiff_t)stride];
+  }
+  if (q < 0) {
+    const size_t edge = j - (size_t)pos * stride;
+    const double a = v[edge], b = v[edge + stride];
+    return a + (-q) * fabs(b - a) * ((a > 0) - (a < 0));
+  }
+  if (q >= n) {
+    const size_t edge = j + (size_t)(n - 1 - pos) * stride;
+    const double a = v[edge], b = v[edge - stride];
+    return a + (q - n + 1) * fabs(a - b) * ((a > 0) - (a < 0));
+  }
+  return v[(ptrdiff_t)j + (ptrdiff_t)offset * (ptrdiff_t)stride];
+}
+
+static inline void w8_slopes_f64(const double *v, size_t j, size_t stride,
+                                 int pos, int n, double h, int periodic,
+                                 int inward, int order, double *lo,
+                                 double *hi) {
+  if (inward && pos == 0) {
+    *lo = *hi = (v[j + stride] - v[j]) / h;
+    return;
+  }
+  if (inward && pos == n - 1) {
+    *lo = *hi = (v[j] - v[j - stride]) / h;
+    return;
+  }
+  const double f = v[j];
+  const double fm = ghost_f64(v, j, stride, pos, n, -1, periodic);
+  const double fp = ghost_f64(v, j, stride, pos, n, 1, periodic);
+  double l = (f - fm) / h, r = (fp - f) / h;
+  if (order == 2) {
+    const double dc = (fp - 2 * f + fm) / (h * h);
+    const double dl =
+        inward && pos < 2
+            ? dc
+            : (f - 2 * fm + ghost_f64(v, j, stride, pos, n, -2, periodic)) / (h * h);
+    const double dr =
+        inward && pos + 2 >= n
+            ? dc
+            : (ghost_f64(v, j, stride, pos, n, 2, periodic) - 2 * fp + f) / (h * h);
+    l += .5 * h * (fabs(dl) <= fabs(dc) ? dl : dc);
+    r -= .5 * h * (fabs(dc) <= fabs(dr) ? dc : dr);
+  }
+  *lo = l;
+  *hi = r;
+}
+
+int po_w8_stage_f64(const po_w8_cfg *c, const double *src, double *dst,
+                    const double *base, double dt) {
+  w8_geom g;
+  w8_make(c, &g);
+  const size_t inner = (size_t)c->nh * c->ne;
+  const size_t blocks = g.n / inner;
+  int bad = 0;
+#pragma omp parallel for schedule(static) reduction(| : bad)
+  for (size_t block = 0; block < blocks; block++) {
+    const size_t begin = block * inner;
+    int q[8];
+    for (int k = 0; k < 8; k++) q[k] = (int)((begin / g.stride[k]) % g.shape[k]);
+    const double vp = g.pv[q[3]];
+    const double ap = c->ap, ae = c->ae;
+    const double palo = q[3] == 0 ? 0 : -ap;
+    const double pahi = q[3] == c->np - 1 ? 0 : ap;
+    const double fpx = vp * g.cs[q[2]], fpy = vp * g.sn[q[2]];
+    const double wp = fabs(vp) * c->kp;
+    const double avoid =
+        c->avoid_square
+            ? fmax(fabs((double)g.x[q[0]]), fabs((double)g.x[q[1]])) - c->arena + 1e-6
+            : -INFINITY;
+    for (int eh = 0; eh < c->nh; eh++) {
+      q[6] = eh;
+      for (int iv = 0; iv < c->ne; iv++) {
+        q[7] = iv;
+        const size_t j = begin + (size_t)eh * c->ne + iv;
+        const double ve = g.ev[iv], we = fabs(ve) * c->ke;
+        const double ealo = iv == 0 ? 0 : -ae;
+        const double eahi = iv == c->ne - 1 ? 0 : ae;
+        const double flow[8] = {fpx, fpy, 0, 0, ve * g.cs[eh], ve * g.sn[eh], 0, 0};
+        double grad[8], H = 0, diss = 0;
+        for (int k = 0; k < 8; k++) {
+          double lm, rp;
+          w8_slopes_f64(src, j, g.stride[k], q[k], g.shape[k], g.spacing[k],
+                        k == 2 || k == 6, c->linear_speed && (k == 3 || k == 7),
+                        c->order, &lm, &rp);
+          grad[k] = .5 * (lm + rp);
+          const double alpha = k == 2   ? wp
+                               : k == 3 ? ap
+                               : k == 6 ? we
+                               : k == 7 ? ae
+                                        : fabs(flow[k]);
+          H += flow[k] * grad[k];
+          diss += .5 * alpha * (rp - lm);
+        }
+        const double p_lo_term = palo * grad[3], p_hi_term = pahi * grad[3];
+        const double e_lo_term = ealo * grad[7], e_hi_term = eahi * grad[7];
+        H += -wp * fabs(grad[2]) + we * fabs(grad[6]) +
+             (p_hi_term < p_lo_term ? p_hi_term : p_lo_term) +
+             (e_lo_term < e_hi_term ? e_hi_term : e_lo_term);
+        double value = src[j] + dt * (H + diss);
+        if (base) value = .5 * (base[j] + value);
+        if (c->order == 1 || base) {
+          const double previous = base ? base[j] : src[j];
+          const double tube = previous < value ? previous : value;
+          value = tube < avoid ? avoid : tube;
+        }
+        if (!isfinite(value)) bad = 1;
+        dst[j] = value;
+      }
+    }
+  }
+  w8_free(&g);
+  return bad ? PO_ENONFINITE : 0;
+}

@@ -1,0 +1,621 @@
+// Compact eight-state semi-Lagrangian contact game: capture field, fused
+// min-max backup and product-stencil queries, for the dense pair layout and
+// the pair-packed domain (src/pursuit_evasion/local_game/grid_game.py,
+// local_game/reference.py:122-134).
+//
+// Backup.  The reference runs, per chunk of 256 pursuer states and per
+// pursuer action u, one launch that interpolates the pursuer successor of
+// every (ip, ie') pair into a temporary [chunk][n_e] array and one launch
+// that reduces over the evader replies (grid_game.py:286-333, :384-421), and
+// in the packed memory-saving mode copies every output tile to the host.
+// Here one persistent launch does the whole backup: a CTA takes a pursuer
+// state ip, and for each allowed u builds the interpolated row
+//   g[ie'] = sum_k wp[ip,u,k] V(idp[ip,u,k], ie')
+// in shared memory (coalesced reads of 16 field rows), then every thread
+// reduces its cells (ip, ie) over the evader replies with 16 shared-memory
+// gathers per reply, keeping the running minimum over u in the output
+// array.  The reference's early exit (a reply at least as bad as the best
+// value so far drops the action) is kept, so the values equal the
+// reference's.  Rows longer than the shared-memory budget go to a
+// per-CTA scratch row in global memory (L2-resident).
+#include <cmath>
+#include <vector>
+
+#include "pe_internal.h"
+
+namespace pe {
+namespace {
+
+constexpr int kThreads = 512;
+constexpr int kStencil = 16;
+constexpr int kMaxRowBytes = 192 * 1024;
+
+struct CompactDev {
+  int np, ne, npa, nea;
+  const float4 *p_pose, *e_pose;
+  const int *p_ids, *e_ids;
+  const float *p_w, *e_w;
+  const uint8_t *p_allowed, *e_allowed;
+  // pair-packed domain
+  const int *p_position, *lookup, *e_indices, *counts;
+  const long long *offsets;
+  int positions, max_count;
+  float exit_value;  // exit radius
+  float reach;       // exit radius + evader stencil reach (packed rows)
+};
+
+// Oriented-rectangle separating-axis value of two footprints in float32
+// (geometry.py:15-36 as evaluated by the reference's CUDA initializer,
+// grid_game.py:193-201): the largest of the gaps along both bodies' axes.
+__device__ __forceinline__ float contact_value(float4 a, float4 b, float pl, float pw,
+                                               float el, float ew) {
+  const float dx = b.x - a.x, dy = b.y - a.y;
+  const float rel = b.z - a.z;
+  const float ca = fabsf(cosf(rel)), sa = fabsf(sinf(rel));
+  const float cp = cosf(a.z), sp = sinf(a.z), ce = cosf(b.z), se = sinf(b.z);
+  // gaps along the pursuer's axes, then along the evader's
+  const float gpx = fabsf(dx * cp + dy * sp) - .5f * (pl + el * ca + ew * sa);
+  const float gpy = fabsf(-dx * sp + dy * cp) - .5f * (pw + el * sa + ew * ca);
+  const float gex = fabsf(dx * ce + dy * se) - .5f * (el + pl * ca + pw * sa);
+  const float gey = fabsf(-dx * se + dy * ce) - .5f * (ew + pl * sa + pw * ca);
+  return fmaxf(fmaxf(gpx, gpy), fmaxf(gex, gey));
+}
+
+__global__ void init_dense_kernel(CompactDev d, float *f, float pl, float pw, float el,
+                                  float ew) {
+  const long long n = (long long)d.np * d.ne;
+  for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n;
+       j += (long long)gridDim.x * blockDim.x) {
+    const int ip = (int)(j / d.ne), ie = (int)(j - (long long)ip * d.ne);
+    const float4 a = d.p_pose[ip], b = d.e_pose[ie];
+    const float dx = b.x - a.x, dy = b.y - a.y;
+    f[j] = dx * dx + dy * dy > d.exit_value * d.exit_value
+               ? d.exit_value
+               : contact_value(a, b, pl, pw, el, ew);
+  }
+}
+
+__global__ void init_packed_kernel(CompactDev d, float *f, float pl, float pw, float el,
+                                   float ew) {
+  for (int ip = blockIdx.x; ip < d.np; ip += gridDim.x) {
+    const int pos = d.p_position[ip];
+    const int count = d.counts[pos];
+    const float4 a = d.p_pose[ip];
+    for (int k = threadIdx.x; k < count; k += blockDim.x) {
+      const int ie = d.e_indices[(long long)pos * d.max_count + k];
+      f[d.offsets[ip] + k] = contact_value(a, d.e_pose[ie], pl, pw, el, ew);
+    }
+  }
+}
+
+// Value of the pursuer successor vertex `nxt` paired with evader state ie
+// in the packed layout (grid_game.py:403-411).
+__device__ __forceinline__ float packed_at(const CompactDev &d, const float *__restrict__ f,
+                                           int nxt, int ie) {
+  const int rank = __ldg(d.lookup + (long long)__ldg(d.p_position + nxt) * d.ne + ie);
+  return rank < 0 ? d.exit_value : __ldg(f + __ldg(d.offsets + nxt) + rank);
+}
+
+template <bool PACKED, bool SMEM>
+__global__ void __launch_bounds__(kThreads)
+    backup_kernel(const CompactDev d, const float *__restrict__ cur, float *__restrict__ out,
+                  float *__restrict__ scratch) {
+  extern __shared__ float row_smem[];
+  __shared__ int s_ids[kStencil];
+  __shared__ float s_w[kStencil];
+  float *g = SMEM ? row_smem : scratch + (size_t)blockIdx.x * d.ne;
+  const int tid = threadIdx.x;
+  const float r2 = d.exit_value * d.exit_value, reach2 = d.reach * d.reach;
+
+  for (int ip = blockIdx.x; ip < d.np; ip += gridDim.x) {
+    int count, pos = 0;
+    long long base;
+    if (PACKED) {
+      pos = d.p_position[ip];
+      count = d.counts[pos];
+      base = d.offsets[ip];
+    } else {
+      count = d.ne;
+      base = (long long)ip * d.ne;
+    }
+    const int *cell_e = PACKED ? d.e_indices + (long long)pos * d.max_count : nullptr;
+    const float4 pp = d.p_pose[ip];
+    // the running minimum starts at the current value; every cell is owned
+    // by the same thread for the whole pose
+    for (int k = tid; k < count; k += kThreads) out[base + k] = cur[base + k];
+
+    for (int u = 0; u < d.npa; u++) {
+      if (!d.p_allowed[(long long)ip * d.npa + u]) continue;
+      __syncthreads();  // the previous row's readers are done
+      if (tid < kStencil) {
+        const long long s = ((long long)ip * d.npa + u) * kStencil + tid;
+        s_ids[tid] = d.p_ids[s];
+        s_w[tid] = d.p_w[s];
+      }
+      __syncthreads();
+      // interpolated pursuer successor against every evader state
+      for (int ie = tid; ie < d.ne; ie += kThreads) {
+        float v = 0.f;
+        if (PACKED) {
+          const float4 ep = d.e_pose[ie];
+          const float dx = pp.x - ep.x, dy = pp.y - ep.y;
+          if (dx * dx + dy * dy > reach2) {
+            v = d.exit_value;
+          } else {
+#pragma unroll
+            for (int k = 0; k < kStencil; k++)
+              if (s_w[k] > 0.f) v = fmaf(s_w[k], packed_at(d, cur, s_ids[k], ie), v);
+          }
+        } else {
+#pragma unroll
+          for (int k = 0; k < kStencil; k++)
+            if (s_w[k] > 0.f) v = fmaf(s_w[k], __ldg(cur + (long long)s_ids[k] * d.ne + ie), v);
+        }
+        g[ie] = v;
+      }
+      __syncthreads();
+      // evader replies: max with early exit against the running minimum
+      for (int k = tid; k < count; k += kThreads) {
+        const int ie = PACKED ? cell_e[k] : k;
+        if (!PACKED) {
+          const float4 ep = d.e_pose[ie];
+          const float dx = pp.x - ep.x, dy = pp.y - ep.y;
+          if (dx * dx + dy * dy > r2) continue;  // outside the local game
+        }
+        const float best = out[base + k];
+        float worst = -1e30f;
+        bool dropped = false;
+        for (int a = 0; a < d.nea; a++) {
+          if (!d.e_allowed[(long long)ie * d.nea + a]) continue;
+          const long long s = ((long long)ie * d.nea + a) * kStencil;
+          const int4 *ids4 = reinterpret_cast<const int4 *>(d.e_ids + s);
+          const float4 *w4 = reinterpret_cast<const float4 *>(d.e_w + s);
+          float value = 0.f;
+#pragma unroll
+          for (int q = 0; q < kStencil / 4; q++) {
+            const int4 i = __ldg(ids4 + q);
+            const float4 w = __ldg(w4 + q);
+            if (w.x > 0.f) value = fmaf(w.x, g[i.x], value);
+            if (w.y > 0.f) value = fmaf(w.y, g[i.y], value);
+            if (w.z > 0.f) value = fmaf(w.z, g[i.z], value);
+            if (w.w > 0.f) value = fmaf(w.w, g[i.w], value);
+          }
+          worst = fmaxf(worst, value);
+          if (worst >= best) {
+            dropped = true;
+            break;
+          }
+        }
+        if (!dropped) out[base + k] = fminf(best, worst);
+      }
+    }
+    __syncthreads();  // g and s_ids are reused by the next pose
+  }
+}
+
+template <bool PACKED>
+__global__ void query_kernel(CompactDev d, const float *__restrict__ f, int n,
+                             const int *__restrict__ pi, const float *__restrict__ pw,
+                             const int *__restrict__ ei, const float *__restrict__ ew,
+                             float *__restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float total = 0.f;
+  for (int a = 0; a < kStencil; a++) {
+    const float wa = pw[kStencil * i + a];
+    if (!(wa > 0.f)) continue;
+    const int p = pi[kStencil * i + a];
+    float value = 0.f;
+    for (int b = 0; b < kStencil; b++) {
+      const float wb = ew[kStencil * i + b];
+      if (!(wb > 0.f)) continue;
+      const int e = ei[kStencil * i + b];
+      const float x = PACKED ? packed_at(d, f, p, e) : f[(long long)p * d.ne + e];
+      value = fmaf(wb, x, value);
+    }
+    total = fmaf(wa, value, total);
+  }
+  out[i] = total;
+}
+
+template <typename T>
+int upload(const T *host, size_t count, T **dev) {
+  *dev = nullptr;
+  if (count == 0) return PE_OK;
+  PE_CUDA_TRY(cudaMalloc(dev, count * sizeof(T)));
+  PE_CUDA_TRY(cudaMemcpy(*dev, host, count * sizeof(T), cudaMemcpyHostToDevice));
+  return PE_OK;
+}
+
+}  // namespace
+}  // namespace pe
+
+struct pe_compact {
+  int device = 0;
+  bool packed = false;
+  pe::CompactDev d{};
+  int64_t cells = 0;
+  std::vector<void *> owned;  // device arrays of the grids and the domain
+  float *field = nullptr, *next = nullptr, *scratch = nullptr;
+  int grid = 0;
+  size_t smem = 0;
+  bool smem_row = true;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  bool initialized = false;
+  pe::LaunchTimer timer;
+};
+
+namespace {
+
+using pe::fail;
+
+int check_grid(const pe_vehicle_grid *g, const char *role) {
+  if (!g || !g->pose || !g->ids || !g->weights || !g->allowed)
+    return fail(PE_EINVAL, "%s grid: NULL array", role);
+  if (g->states < 1 || g->actions < 1 || g->actions > 64)
+    return fail(PE_EINVAL, "%s grid: %d states, %d actions", role, g->states, g->actions);
+  const size_t n = (size_t)g->states * g->actions * pe::kStencil;
+  for (size_t i = 0; i < n; i++) {
+    const float w = g->weights[i];
+    if (!std::isfinite(w)) return fail(PE_EINVAL, "%s grid: non-finite weight", role);
+    if (w > 0 && (g->ids[i] < 0 || g->ids[i] >= g->states))
+      return fail(PE_EINVAL, "%s grid: vertex id %d out of range", role, g->ids[i]);
+  }
+  for (size_t i = 0; i < (size_t)g->states * 4; i++)
+    if (!std::isfinite(g->pose[i])) return fail(PE_EINVAL, "%s grid: non-finite state", role);
+  return PE_OK;
+}
+
+int check_domain(const pe_pair_domain *dm, int np, int ne) {
+  if (!dm->p_position || !dm->lookup || !dm->e_indices || !dm->counts || !dm->offsets)
+    return fail(PE_EINVAL, "pair domain: NULL array");
+  if (dm->positions < 1 || dm->max_count < 0 || dm->max_count > ne)
+    return fail(PE_EINVAL, "pair domain: %d positions, %d max count", dm->positions,
+                dm->max_count);
+  for (int i = 0; i < dm->positions; i++) {
+    const int c = dm->counts[i];
+    if (c < 0 || c > dm->max_count) return fail(PE_EINVAL, "pair domain: bad count");
+    for (int k = 0; k < c; k++) {
+      const int ie = dm->e_indices[(size_t)i * dm->max_count + k];
+      if (ie < 0 || ie >= ne || dm->lookup[(size_t)i * ne + ie] != k)
+        return fail(PE_EINVAL, "pair domain: e_indices and lookup disagree");
+    }
+    for (int ie = 0; ie < ne; ie++) {
+      const int r = dm->lookup[(size_t)i * ne + ie];
+      if (r < -1 || r >= c) return fail(PE_EINVAL, "pair domain: lookup rank out of range");
+    }
+  }
+  if (dm->offsets[0] != 0) return fail(PE_EINVAL, "pair domain: offsets[0] != 0");
+  for (int ip = 0; ip < np; ip++) {
+    const int pos = dm->p_position[ip];
+    if (pos < 0 || pos >= dm->positions)
+      return fail(PE_EINVAL, "pair domain: p_position out of range");
+    if (dm->offsets[ip + 1] - dm->offsets[ip] != dm->counts[pos])
+      return fail(PE_EINVAL, "pair domain: offsets disagree with counts");
+  }
+  return PE_OK;
+}
+
+// Largest centre displacement of an evader interpolation vertex with a
+// positive weight, plus 1e-4 (grid_game.py:456-466).
+double evader_reach(const pe_vehicle_grid *e) {
+  double reach = 0;
+  const size_t rows = (size_t)e->states * e->actions;
+  for (size_t r = 0; r < rows; r++) {
+    const size_t state = r / e->actions;
+    for (int q = 0; q < pe::kStencil; q++) {
+      const size_t s = r * pe::kStencil + q;
+      if (!(e->weights[s] > 0)) continue;
+      const int v = e->ids[s];
+      const double dx = (double)e->pose[4 * v] - e->pose[4 * state];
+      const double dy = (double)e->pose[4 * v + 1] - e->pose[4 * state + 1];
+      reach = std::fmax(reach, std::sqrt(dx * dx + dy * dy));
+    }
+  }
+  return reach + 1e-4;
+}
+
+void release(pe_compact *h) {
+  cudaSetDevice(h->device);
+  for (void *p : h->owned) cudaFree(p);
+  cudaFree(h->field);
+  cudaFree(h->next);
+  cudaFree(h->scratch);
+  if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+}
+
+template <typename T>
+int own(pe_compact *h, const T *host, size_t count, const T **dev) {
+  T *p = nullptr;
+  const int rc = pe::upload(host, count, &p);
+  if (p) h->owned.push_back(p);
+  *dev = p;
+  return rc;
+}
+
+int upload_grid(pe_compact *h, const pe_vehicle_grid *g, const float4 **pose,
+                const int **ids, const float **w, const uint8_t **allowed) {
+  const size_t n = g->states, rows = n * g->actions;
+  const float *pose_f = nullptr;
+  int rc = own(h, g->pose, n * 4, &pose_f);
+  if (rc) return rc;
+  *pose = reinterpret_cast<const float4 *>(pose_f);
+  if ((rc = own(h, g->ids, rows * pe::kStencil, ids))) return rc;
+  if ((rc = own(h, g->weights, rows * pe::kStencil, w))) return rc;
+  return own(h, g->allowed, rows, allowed);
+}
+
+int configure_launch(pe_compact *h) {
+  int sms = 0;
+  PE_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
+  const size_t row = (size_t)h->d.ne * sizeof(float);
+  h->smem_row = row <= (size_t)pe::kMaxRowBytes;
+  h->smem = h->smem_row ? row : 0;
+  const void *kernel =
+      h->packed ? (h->smem_row ? (const void *)pe::backup_kernel<true, true>
+                               : (const void *)pe::backup_kernel<true, false>)
+                : (h->smem_row ? (const void *)pe::backup_kernel<false, true>
+                               : (const void *)pe::backup_kernel<false, false>);
+  PE_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)h->smem));
+  int resident = 0;
+  PE_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, kernel, pe::kThreads,
+                                                            h->smem));
+  if (resident < 1) return fail(PE_EINVAL, "compact backup: no resident CTA fits");
+  const int64_t slots = (int64_t)sms * resident;
+  h->grid = (int)(h->d.np < slots ? h->d.np : slots);
+  if (!h->smem_row)
+    PE_CUDA_TRY(cudaMalloc(&h->scratch, (size_t)h->grid * row));
+  return PE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pe_compact_create(const pe_vehicle_grid *p, const pe_vehicle_grid *e,
+                      const pe_pair_domain *domain, double exit_radius, int32_t device,
+                      pe_compact **out) {
+  if (!out) return fail(PE_EINVAL, "out is NULL");
+  *out = nullptr;
+  int rc = check_grid(p, "pursuer");
+  if (rc) return rc;
+  if ((rc = check_grid(e, "evader"))) return rc;
+  if (!std::isfinite(exit_radius) || exit_radius <= 0)
+    return fail(PE_EINVAL, "exit radius must be positive");
+  if ((int64_t)p->states * e->states >= ((int64_t)1 << 40))
+    return fail(PE_EINVAL, "pair space too large");
+  if (domain && (rc = check_domain(domain, p->states, e->states))) return rc;
+  int count = 0;
+  PE_CUDA_TRY(cudaGetDeviceCount(&count));
+  if (device < 0 || device >= count) return fail(PE_EINVAL, "no CUDA device %d", device);
+  PE_CUDA_TRY(cudaSetDevice(device));
+
+  pe_compact *h = new pe_compact;
+  h->device = device;
+  h->packed = domain != nullptr;
+  pe::CompactDev &d = h->d;
+  d.np = p->states;
+  d.ne = e->states;
+  d.npa = p->actions;
+  d.nea = e->actions;
+  d.exit_value = (float)exit_radius;
+  d.reach = (float)(exit_radius + evader_reach(e));
+  rc = upload_grid(h, p, &d.p_pose, &d.p_ids, &d.p_w, &d.p_allowed);
+  if (!rc) rc = upload_grid(h, e, &d.e_pose, &d.e_ids, &d.e_w, &d.e_allowed);
+  if (!rc && domain) {
+    d.positions = domain->positions;
+    d.max_count = domain->max_count;
+    rc = own(h, domain->p_position, (size_t)d.np, &d.p_position);
+    if (!rc) rc = own(h, domain->lookup, (size_t)d.positions * d.ne, &d.lookup);
+    if (!rc) rc = own(h, domain->e_indices, (size_t)d.positions * d.max_count, &d.e_indices);
+    if (!rc) rc = own(h, domain->counts, (size_t)d.positions, &d.counts);
+    if (!rc)
+      rc = own(h, reinterpret_cast<const long long *>(domain->offsets), (size_t)d.np + 1,
+               &d.offsets);
+    h->cells = domain->offsets[d.np];
+  } else {
+    h->cells = (int64_t)d.np * d.ne;
+  }
+  if (!rc && h->cells > 0) {
+    const cudaError_t err1 = cudaMalloc(&h->field, (size_t)h->cells * sizeof(float));
+    const cudaError_t err2 =
+        err1 == cudaSuccess ? cudaMalloc(&h->next, (size_t)h->cells * sizeof(float)) : err1;
+    if (err2 != cudaSuccess) rc = pe::cuda_fail(err2, "compact field");
+  }
+  if (!rc) rc = configure_launch(h);
+  if (!rc) {
+    const cudaError_t err = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+    if (err != cudaSuccess) rc = pe::cuda_fail(err, "cudaStreamCreate");
+    h->own_stream = err == cudaSuccess;
+  }
+  if (rc) {
+    release(h);
+    delete h;
+    return rc;
+  }
+  *out = h;
+  return PE_OK;
+}
+
+int pe_compact_cells(const pe_compact *h, int64_t *out) {
+  if (!h || !out) return fail(PE_EINVAL, "NULL argument");
+  *out = h->cells;
+  return PE_OK;
+}
+
+int pe_compact_init(pe_compact *h, double p_length, double p_width, double e_length,
+                    double e_width) {
+  if (!h) return fail(PE_EINVAL, "handle is NULL");
+  const double dims[4] = {p_length, p_width, e_length, e_width};
+  for (double v : dims)
+    if (!std::isfinite(v) || v <= 0) return fail(PE_EINVAL, "footprints must be positive");
+  PE_CUDA_TRY(cudaSetDevice(h->device));
+  if (h->cells > 0) {
+    if (h->packed)
+      pe::init_packed_kernel<<<148 * 8, 256, 0, h->stream>>>(
+          h->d, h->field, (float)p_length, (float)p_width, (float)e_length, (float)e_width);
+    else
+      pe::init_dense_kernel<<<148 * 8, 256, 0, h->stream>>>(
+          h->d, h->field, (float)p_length, (float)p_width, (float)e_length, (float)e_width);
+    PE_CUDA_TRY(cudaGetLastError());
+    pe::count_launches(1);
+  }
+  h->initialized = true;
+  return PE_OK;
+}
+
+int pe_compact_set_field(pe_compact *h, const float *host, int64_t n) {
+  if (!h || !host) return fail(PE_EINVAL, "NULL argument");
+  if (n != h->cells) return fail(PE_EINVAL, "field has %lld values, expected %lld",
+                                 (long long)n, (long long)h->cells);
+  for (int64_t i = 0; i < n; i++)
+    if (!std::isfinite(host[i])) return fail(PE_EINVAL, "non-finite field value");
+  PE_CUDA_TRY(cudaSetDevice(h->device));
+  PE_CUDA_TRY(cudaMemcpyAsync(h->field, host, (size_t)n * sizeof(float),
+                              cudaMemcpyHostToDevice, h->stream));
+  PE_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  h->initialized = true;
+  return PE_OK;
+}
+
+int pe_compact_backup(pe_compact *h, int32_t count) {
+  if (!h) return fail(PE_EINVAL, "handle is NULL");
+  if (count < 0) return fail(PE_EINVAL, "negative backup count");
+  if (!h->initialized) return fail(PE_ESTATE, "backup before init");
+  PE_CUDA_TRY(cudaSetDevice(h->device));
+  for (int32_t i = 0; i < count && h->cells > 0; i++) {
+    cudaEvent_t t0 = h->timer.begin(h->stream);
+    if (h->packed) {
+      if (h->smem_row)
+        pe::backup_kernel<true, true><<<h->grid, pe::kThreads, h->smem, h->stream>>>(
+            h->d, h->field, h->next, h->scratch);
+      else
+        pe::backup_kernel<true, false><<<h->grid, pe::kThreads, 0, h->stream>>>(
+            h->d, h->field, h->next, h->scratch);
+    } else {
+      if (h->smem_row)
+        pe::backup_kernel<false, true><<<h->grid, pe::kThreads, h->smem, h->stream>>>(
+            h->d, h->field, h->next, h->scratch);
+      else
+        pe::backup_kernel<false, false><<<h->grid, pe::kThreads, 0, h->stream>>>(
+            h->d, h->field, h->next, h->scratch);
+    }
+    PE_CUDA_TRY(cudaGetLastError());
+    pe::count_launches(1);
+    const int rc = h->timer.end(h->stream, t0, 0);
+    if (rc) return rc;
+    std::swap(h->field, h->next);
+  }
+  return PE_OK;
+}
+
+int pe_compact_copy_field(pe_compact *h, float *host, int64_t n) {
+  if (!h || !host) return fail(PE_EINVAL, "NULL argument");
+  if (n != h->cells) return fail(PE_EINVAL, "buffer has %lld values, expected %lld",
+                                 (long long)n, (long long)h->cells);
+  PE_CUDA_TRY(cudaSetDevice(h->device));
+  PE_CUDA_TRY(cudaMemcpyAsync(host, h->field, (size_t)n * sizeof(float),
+                              cudaMemcpyDeviceToHost, h->stream));
+  PE_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return PE_OK;
+}
+
+int pe_compact_field_device(pe_compact *h, void **out) {
+  if (!h || !out) return fail(PE_EINVAL, "NULL argument");
+  *out = h->field;
+  return PE_OK;
+}
+
+int pe_compact_query(pe_compact *h, int32_t n, const int32_t *p_ids,
+                     const float *p_weights, const int32_t *e_ids, const float *e_weights,
+                     float *host_out) {
+  if (!h || !p_ids || !p_weights || !e_ids || !e_weights || !host_out)
+    return fail(PE_EINVAL, "NULL argument");
+  if (n < 0) return fail(PE_EINVAL, "negative query count");
+  if (n == 0) return PE_OK;
+  const size_t m = (size_t)n * pe::kStencil;
+  for (size_t i = 0; i < m; i++) {
+    if (p_weights[i] > 0 && (p_ids[i] < 0 || p_ids[i] >= h->d.np))
+      return fail(PE_EINVAL, "query: pursuer vertex out of range");
+    if (e_weights[i] > 0 && (e_ids[i] < 0 || e_ids[i] >= h->d.ne))
+      return fail(PE_EINVAL, "query: evader vertex out of range");
+  }
+  PE_CUDA_TRY(cudaSetDevice(h->device));
+  int32_t *pi = nullptr, *ei = nullptr;
+  float *pw = nullptr, *ew = nullptr, *out = nullptr;
+  int rc = pe::upload(p_ids, m, &pi);
+  if (!rc) rc = pe::upload(p_weights, m, &pw);
+  if (!rc) rc = pe::upload(e_ids, m, &ei);
+  if (!rc) rc = pe::upload(e_weights, m, &ew);
+  if (!rc) {
+    const cudaError_t err = cudaMalloc(&out, (size_t)n * sizeof(float));
+    if (err != cudaSuccess) rc = pe::cuda_fail(err, "query output");
+  }
+  if (!rc) {
+    const int blocks = (n + 255) / 256;
+    if (h->packed)
+      pe::query_kernel<true><<<blocks, 256, 0, h->stream>>>(h->d, h->field, n, pi, pw, ei,
+                                                            ew, out);
+    else
+      pe::query_kernel<false><<<blocks, 256, 0, h->stream>>>(h->d, h->field, n, pi, pw, ei,
+                                                             ew, out);
+    cudaError_t err = cudaGetLastError();
+    if (err == cudaSuccess) {
+      pe::count_launches(1);
+      err = cudaMemcpyAsync(host_out, out, (size_t)n * sizeof(float),
+                            cudaMemcpyDeviceToHost, h->stream);
+    }
+    if (err == cudaSuccess) err = cudaStreamSynchronize(h->stream);
+    if (err != cudaSuccess) rc = pe::cuda_fail(err, "compact query");
+  }
+  cudaFree(pi);
+  cudaFree(pw);
+  cudaFree(ei);
+  cudaFree(ew);
+  cudaFree(out);
+  return rc;
+}
+
+int pe_compact_set_stream(pe_compact *h, void *cuda_stream) {
+  if (!h) return fail(PE_EINVAL, "handle is NULL");
+  PE_CUDA_TRY(cudaSetDevice(h->device));
+  PE_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  if (h->own_stream) PE_CUDA_TRY(cudaStreamDestroy(h->stream));
+  h->stream = static_cast<cudaStream_t>(cuda_stream);
+  h->own_stream = false;
+  return PE_OK;
+}
+
+int pe_compact_synchronize(pe_compact *h) {
+  if (!h) return fail(PE_EINVAL, "handle is NULL");
+  PE_CUDA_TRY(cudaSetDevice(h->device));
+  PE_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return PE_OK;
+}
+
+int pe_compact_profile(pe_compact *h, int32_t enable) {
+  if (!h) return fail(PE_EINVAL, "handle is NULL");
+  PE_CUDA_TRY(cudaSetDevice(h->device));
+  return h->timer.reset(enable != 0);
+}
+
+int pe_compact_kernel_time(pe_compact *h, double *ms, int64_t *launches) {
+  if (!h || !ms || !launches) return fail(PE_EINVAL, "NULL argument");
+  PE_CUDA_TRY(cudaSetDevice(h->device));
+  const int rc = h->timer.harvest(true);
+  if (rc) return rc;
+  *ms = h->timer.ms(0);
+  *launches = h->timer.launches(0);
+  return PE_OK;
+}
+
+int pe_compact_destroy(pe_compact *h) {
+  if (!h) return PE_OK;
+  release(h);
+  delete h;
+  return PE_OK;
+}
+
+}  // extern "C"

@@ -1,12 +1,339 @@
-// Dense 8D ENO/Lax-Friedrichs stage, fast variant: the shared stage kernel
-// (world8d_stage.cuh) with reciprocal spacings and multiply-add contraction.
+// Dense 8D ENO/Lax-Friedrichs stage, fast variant (float32, multiply-add
+// contraction, reciprocal spacings): the update of native_world.cpp:261-314
+// equal to the exact stage up to float rounding and the ENO2 selections that
+// rounding can flip.
+//
+// Layout [xP, yP, thP, vP | xE, yE, thE, vE]: the cells of one pursuer pose
+// (xP, yP, thP, vP) form a contiguous "evader block" (11*11*9*7 = 7,623 cells
+// on the 8D contact grid).  A CTA walks the pursuer poses o = blockIdx.x,
+// blockIdx.x + gridDim.x, ...; for each it stages the evader block in shared
+// memory (cp.async, double-buffered so the next block loads while this one
+// computes).  The four evader-axis stencils read shared memory; the four
+// pursuer-axis stencils read the same cell of the neighbouring blocks, one
+// coalesced load per neighbour, from L2.
+//
+// Ghost values beyond a non-periodic end (native_world.cpp:44-58) are rebuilt
+// from the clamped 5-value window: every ghost the reference forms is the end
+// value pushed by the end difference, and both lie inside the window.  The
+// Hamiltonian's linear flow terms and their Lax-Friedrichs dissipation fold
+// into upwind weights: v*g + |v|/2 (hi - lo) = min(v,0) lo + max(v,0) hi.
+// Evader blocks too large for shared memory use the thread-per-cell kernel
+// of world8d_stage.cuh.
+#include <cstdio>
+
 #include "world8d_stage.cuh"
 
 namespace pe {
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kMaxBlockBytes = 96 * 1024;  // per buffer; two buffers per CTA
+
+// e / d as __umulhi(e, m), m = ceil(2^32 / d): exact for e * (m*d - 2^32) <
+// 2^32, which holds for e < 2^24 and d < 256 and, in general, for e < 2^32/d.
+struct Divisor {
+  uint32_t m;
+  int d;
+};
+
+Divisor make_divisor(int d) {
+  return {(uint32_t)((((uint64_t)1 << 32) + (uint64_t)d - 1) / (uint64_t)d), d};
+}
+
+__device__ __forceinline__ int split(int e, Divisor v, int &rem) {
+  const int q = (int)__umulhi((uint32_t)e, v.m);
+  rem = e - q * v.d;
+  return q;
+}
+
+struct FastW8Args {
+  World8Grid g;
+  World8Stage s;
+  Divisor d7, d6, d5;
+  int inner, outer;
+};
+
+enum AxisKind { kExtrapolated = 0, kPeriodic = 1, kInward = 2 };
+
+// a + m |b - a| sign(a): the reference's value beyond an end (a: end node,
+// b: the node next to it, m: nodes beyond the end).
+__device__ __forceinline__ float ghost_value(float a, float b, float m) {
+  const float sgn = a > 0.f ? 1.f : (a < 0.f ? -1.f : 0.f);
+  return fmaf(m * fabsf(b - a), sgn, a);
+}
+
+// Unscaled backward / forward ENO slopes (times the spacing) of a cell at
+// position p of an axis of n nodes, from its clamped (or wrapped) window.
+template <int ORDER>
+__device__ __forceinline__ void axis_slopes(float m2, float m1, float f, float p1,
+                                            float p2, int p, int n, int kind,
+                                            float &dlo, float &dhi) {
+  if (kind == kExtrapolated && (p < 2 || p + 2 >= n)) {
+    if (p == 0) {
+      m1 = ghost_value(f, p1, 1.f);
+      m2 = ghost_value(f, p1, 2.f);
+    } else if (p == 1) {
+      m2 = ghost_value(m1, f, 1.f);
+    }
+    if (p == n - 1) {
+      p1 = ghost_value(f, m1, 1.f);
+      p2 = ghost_value(f, m1, 2.f);
+    } else if (p == n - 2) {
+      p2 = ghost_value(p1, f, 1.f);
+    }
+  }
+  dlo = f - m1;
+  dhi = p1 - f;
+  if (ORDER == 2) {
+    // Second-difference numerators in the reference's form (fp - 2f + fm):
+    // 2f is exact, so they round as the reference's do and the ENO choices
+    // below break exact ties (frequent on the piecewise-linear contact field)
+    // the same way; dividing both sides by h^2 keeps the comparison.
+    const float c = (p1 - 2.f * f) + m1;
+    float l = (f - 2.f * m1) + m2;
+    float r = (p2 - 2.f * p1) + f;
+    if (kind == kInward) {
+      if (p < 2) l = c;
+      if (p + 2 >= n) r = c;
+    }
+    // ties pick the outer difference on the low side and the centred one on
+    // the high side (native_world.cpp:70-71)
+    const float el = fabsf(l) <= fabsf(c) ? l : c;
+    const float er = fabsf(c) <= fabsf(r) ? c : r;
+    dlo = fmaf(0.5f, el, dlo);
+    dhi = fmaf(-0.5f, er, dhi);
+  }
+  if (kind == kInward) {
+    if (p == 0) dlo = dhi = p1 - f;
+    if (p == n - 1) dlo = dhi = f - m1;
+  }
+}
+
+// Window offsets (in cells) of positions p-2, p-1, p+1, p+2 along an axis of
+// stride s: clamped to the ends, or wrapped when periodic.
+__device__ __forceinline__ void window_offsets(int p, int n, int s, bool periodic,
+                                               int &om2, int &om1, int &op1, int &op2) {
+  if (periodic) {
+    om1 = p > 0 ? -s : (n - 1) * s;
+    om2 = p > 1 ? -2 * s : (n - 2) * s;
+    op1 = p < n - 1 ? s : -(n - 1) * s;
+    op2 = p < n - 2 ? 2 * s : -(n - 2) * s;
+  } else {
+    om1 = p > 0 ? -s : 0;
+    om2 = p > 1 ? -2 * s : om1;
+    op1 = p < n - 1 ? s : 0;
+    op2 = p < n - 2 ? 2 * s : op1;
+  }
+}
+
+__device__ __forceinline__ void cp_async4(float *dst, const float *src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(
+                   (uint32_t)__cvta_generic_to_shared(dst)),
+               "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_one() {
+  asm volatile("cp.async.wait_group 1;" ::: "memory");
+}
+
+template <int ORDER>
+__global__ void __launch_bounds__(kThreads)
+    world8_block_kernel(const FastW8Args a) {
+  extern __shared__ __align__(16) float blocks[];  // [2][inner]
+  __shared__ float warp_max[kThreads / 32];
+  const World8Grid &g = a.g;
+  const World8Stage &s = a.s;
+  const int inner = a.inner, tid = threadIdx.x;
+  const int kind_speed = g.linear_speed ? kInward : kExtrapolated;
+  // evader strides inside a block and pursuer strides (whole blocks)
+  const int s7 = 1, s6 = g.shape[7], s5 = g.shape[6] * s6, s4 = g.shape[5] * s5;
+  const float ih[8] = {g.inv_spacing[0], g.inv_spacing[1], g.inv_spacing[2],
+                       g.inv_spacing[3], g.inv_spacing[4], g.inv_spacing[5],
+                       g.inv_spacing[6], g.inv_spacing[7]};
+  float change_max = 0.f;
+  bool bad = false;
+
+  auto stage_block = [&](int o, float *dst) {
+    const float *src = s.src + (int64_t)o * inner;
+    for (int e = tid; e < inner; e += kThreads) cp_async4(dst + e, src + e);
+  };
+
+  int buf = 0;
+  if ((int)blockIdx.x < a.outer) stage_block(blockIdx.x, blocks);
+  cp_async_commit();
+  for (int o = blockIdx.x; o < a.outer; o += gridDim.x, buf ^= 1) {
+    const int next = o + gridDim.x;
+    if (next < a.outer) stage_block(next, blocks + (buf ^ 1) * inner);
+    cp_async_commit();
+    cp_async_wait_one();
+    __syncthreads();
+    const float *blk = blocks + buf * inner;
+
+    // pursuer pose (uniform over the CTA)
+    int qp[4];
+    {
+      int rest = o;
+      qp[3] = rest % g.shape[3];
+      rest /= g.shape[3];
+      qp[2] = rest % g.shape[2];
+      rest /= g.shape[2];
+      qp[1] = rest % g.shape[1];
+      qp[0] = rest / g.shape[1];
+    }
+    const float vp = __ldg(s.pv + qp[3]);
+    const float fpx = vp * __ldg(s.cs + qp[2]), fpy = vp * __ldg(s.sn + qp[2]);
+    const float wp = fabsf(vp) * g.kp;
+    const float palo = qp[3] == 0 ? 0.f : -g.ap;
+    const float pahi = qp[3] == g.np - 1 ? 0.f : g.ap;
+    // upwind weights of the pursuer position axes (unscaled slopes)
+    const float wx_lo = fminf(fpx, 0.f) * ih[0], wx_hi = fmaxf(fpx, 0.f) * ih[0];
+    const float wy_lo = fminf(fpy, 0.f) * ih[1], wy_hi = fmaxf(fpy, 0.f) * ih[1];
+    float avoid = -INFINITY;
+    if (g.avoid_mode == 1) {
+      const float ax = fabsf(__ldg(s.x + qp[0])), ay = fabsf(__ldg(s.x + qp[1]));
+      avoid = (ax < ay ? ay : ax) - g.arena + 1e-6f;
+    }
+    // neighbour offsets along the pursuer axes, in cells
+    int64_t poff[4][4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      int om2, om1, op1, op2;
+      window_offsets(qp[k], g.shape[k], 1, k == 2, om2, om1, op1, op2);
+      const int64_t st = g.stride[k];
+      poff[k][0] = om2 * st;
+      poff[k][1] = om1 * st;
+      poff[k][2] = op1 * st;
+      poff[k][3] = op2 * st;
+    }
+    const int64_t j0 = (int64_t)o * inner;
+    const float *__restrict__ src_o = s.src + j0;
+
+    for (int e = tid; e < inner; e += kThreads) {
+      int q7, q6, q5;
+      int t = split(e, a.d7, q7);
+      t = split(t, a.d6, q6);
+      const int q4 = split(t, a.d5, q5);
+      const float f = blk[e];
+      float dlo[8], dhi[8];
+      // pursuer axes: the same evader cell in the neighbouring blocks
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        const float m2 = __ldg(src_o + poff[k][0] + e);
+        const float m1 = __ldg(src_o + poff[k][1] + e);
+        const float p1 = __ldg(src_o + poff[k][2] + e);
+        const float p2 = __ldg(src_o + poff[k][3] + e);
+        const int kind = k == 2 ? kPeriodic : (k == 3 ? kind_speed : kExtrapolated);
+        axis_slopes<ORDER>(m2, m1, f, p1, p2, qp[k], g.shape[k], kind, dlo[k], dhi[k]);
+      }
+      // evader axes: shared memory
+      const int qe[4] = {q4, q5, q6, q7};
+      const int se[4] = {s4, s5, s6, s7};
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        int om2, om1, op1, op2;
+        window_offsets(qe[k], g.shape[4 + k], se[k], k == 2, om2, om1, op1, op2);
+        const int kind = k == 2 ? kPeriodic : (k == 3 ? kind_speed : kExtrapolated);
+        axis_slopes<ORDER>(blk[e + om2], blk[e + om1], f, blk[e + op1], blk[e + op2],
+                           qe[k], g.shape[4 + k], kind, dlo[4 + k], dhi[4 + k]);
+      }
+      const float ve = __ldg(s.ev + q7);
+      const float fex = ve * __ldg(s.cs + q6), fey = ve * __ldg(s.sn + q6);
+      const float we = fabsf(ve) * g.ke;
+      const float ealo = q7 == 0 ? 0.f : -g.ae;
+      const float eahi = q7 == g.ne - 1 ? 0.f : g.ae;
+      // linear flow axes with their dissipation: upwind weights
+      float total = fmaf(wx_lo, dlo[0], wx_hi * dhi[0]);
+      total = fmaf(wy_lo, dlo[1], fmaf(wy_hi, dhi[1], total));
+      total = fmaf(fminf(fex, 0.f) * ih[4], dlo[4], fmaf(fmaxf(fex, 0.f) * ih[4], dhi[4], total));
+      total = fmaf(fminf(fey, 0.f) * ih[5], dlo[5], fmaf(fmaxf(fey, 0.f) * ih[5], dhi[5], total));
+      // headings: -wp |g_thP| + we |g_thE| and their dissipation
+      const float g2 = 0.5f * ih[2] * (dlo[2] + dhi[2]);
+      const float g6 = 0.5f * ih[6] * (dlo[6] + dhi[6]);
+      total = fmaf(-wp, fabsf(g2), total);
+      total = fmaf(we, fabsf(g6), total);
+      float diss = wp * ih[2] * (dhi[2] - dlo[2]);
+      diss = fmaf(we * ih[6], dhi[6] - dlo[6], diss);
+      // speeds: bounded accelerations
+      const float g3 = 0.5f * ih[3] * (dlo[3] + dhi[3]);
+      const float g7 = 0.5f * ih[7] * (dlo[7] + dhi[7]);
+      total += fminf(palo * g3, pahi * g3) + fmaxf(ealo * g7, eahi * g7);
+      diss = fmaf(g.ap * ih[3], dhi[3] - dlo[3], diss);
+      diss = fmaf(g.ae * ih[7], dhi[7] - dlo[7], diss);
+      total = fmaf(0.5f, diss, total);
+
+      const int64_t j = j0 + e;
+      float value = fmaf(s.dt, total, f);
+      if (s.base) value = 0.5f * (__ldg(s.base + j) + value);
+      if (g.order == 1 || s.base) {
+        const float previous = s.base ? __ldg(s.base + j) : f;
+        const float tube = previous < value ? previous : value;
+        value = tube < avoid ? avoid : tube;
+        if (previous > 0.f && value <= 0.f && isnan(s.arrival[j]))
+          s.arrival[j] = (float)s.tau + s.dt * previous / (previous - value);
+        change_max = fmaxf(change_max, fabsf(value - previous));
+      }
+      bad |= !isfinite(value);
+      s.dst[j] = value;
+    }
+    __syncthreads();  // this buffer is refilled two poses later
+  }
+  asm volatile("cp.async.wait_all;" ::: "memory");
+
+  if (__syncthreads_or(bad) && tid == 0) atomicOr(&s.stats->nonfinite, 1u);
+  for (int off = 16; off > 0; off >>= 1)
+    change_max = fmaxf(change_max, __shfl_xor_sync(0xffffffffu, change_max, off));
+  if ((tid & 31) == 0) warp_max[tid >> 5] = change_max;
+  __syncthreads();
+  if (tid == 0) {
+    float m = 0.f;
+    for (int w = 0; w < kThreads / 32; w++) m = fmaxf(m, warp_max[w]);
+    if (m > 0.f)
+      atomicMax(&s.stats->residual, (unsigned long long)__double_as_longlong((double)m));
+  }
+}
+
+template <int ORDER>
+cudaError_t launch_block(const FastW8Args &a, size_t smem, cudaStream_t stream) {
+  static size_t configured = 0;
+  static int resident = 0;
+  if (configured != smem || resident == 0) {
+    cudaError_t e = cudaFuncSetAttribute(world8_block_kernel<ORDER>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, world8_block_kernel<ORDER>,
+                                                      kThreads, smem);
+    if (e != cudaSuccess) return e;
+    if (resident < 1) return cudaErrorInvalidConfiguration;
+    configured = smem;
+  }
+  int device = 0, sms = 0;
+  cudaGetDevice(&device);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  const int blocks = a.outer < sms * resident ? a.outer : sms * resident;
+  world8_block_kernel<ORDER><<<blocks, kThreads, smem, stream>>>(a);
+  return cudaGetLastError();
+}
+
+}  // namespace
 
 cudaError_t world8_stage_fast(const World8Grid &g, const World8Stage &s,
                               cudaStream_t stream) {
-  return w8::launch_stage<true>(g, s, stream);
+  const int64_t inner = (int64_t)g.shape[4] * g.shape[5] * g.shape[6] * g.shape[7];
+  if (inner * 4 > kMaxBlockBytes) return w8::launch_stage<true>(g, s, stream);
+  FastW8Args a;
+  a.g = g;
+  a.s = s;
+  a.inner = (int)inner;
+  a.outer = (int)(g.cells / inner);
+  a.d7 = make_divisor(g.shape[7]);
+  a.d6 = make_divisor(g.shape[6]);
+  a.d5 = make_divisor(g.shape[5]);
+  const size_t smem = (size_t)2 * inner * sizeof(float);
+  return g.order == 1 ? launch_block<1>(a, smem, stream) : launch_block<2>(a, smem, stream);
 }
 
 }  // namespace pe

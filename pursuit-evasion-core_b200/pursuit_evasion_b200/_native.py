@@ -109,6 +109,31 @@ class SemiLagParams(ctypes.Structure):
     ]
 
 
+class VehicleGridArrays(ctypes.Structure):
+    """pe_vehicle_grid: one car's legal states and held-control stencils."""
+    _fields_ = [
+        ("states", ctypes.c_int32),
+        ("actions", ctypes.c_int32),
+        ("pose", ctypes.c_void_p),
+        ("ids", ctypes.c_void_p),
+        ("weights", ctypes.c_void_p),
+        ("allowed", ctypes.c_void_p),
+    ]
+
+
+class PairDomainArrays(ctypes.Structure):
+    """pe_pair_domain: the pairs within the exit radius."""
+    _fields_ = [
+        ("positions", ctypes.c_int32),
+        ("max_count", ctypes.c_int32),
+        ("p_position", ctypes.c_void_p),
+        ("lookup", ctypes.c_void_p),
+        ("e_indices", ctypes.c_void_p),
+        ("counts", ctypes.c_void_p),
+        ("offsets", ctypes.c_void_p),
+    ]
+
+
 PE_SL_KERNEL_AUTO, PE_SL_KERNEL_GENERIC, PE_SL_KERNEL_TILED = 0, 1, 2
 PE_SL_TUBE = 0
 PE_SL_MINTIME = 1
@@ -172,6 +197,22 @@ SIGNATURES = {
     "pe_table_value": (ctypes.c_int, [_P, _DP, ctypes.c_int64, _DP]),
     "pe_table_field": (ctypes.c_int, [_P, _DP, _DP, ctypes.c_int64, _DP]),
     "pe_table_destroy": (ctypes.c_int, [_P]),
+    "pe_compact_create": (ctypes.c_int, [ctypes.POINTER(VehicleGridArrays),
+                                         ctypes.POINTER(VehicleGridArrays),
+                                         ctypes.POINTER(PairDomainArrays), ctypes.c_double,
+                                         ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p)]),
+    "pe_compact_cells": (ctypes.c_int, [_P, _I64P]),
+    "pe_compact_init": (ctypes.c_int, [_P] + [ctypes.c_double] * 4),
+    "pe_compact_set_field": (ctypes.c_int, [_P, _P, ctypes.c_int64]),
+    "pe_compact_backup": (ctypes.c_int, [_P, ctypes.c_int32]),
+    "pe_compact_copy_field": (ctypes.c_int, [_P, _P, ctypes.c_int64]),
+    "pe_compact_field_device": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_void_p)]),
+    "pe_compact_query": (ctypes.c_int, [_P, ctypes.c_int32, _P, _P, _P, _P, _P]),
+    "pe_compact_set_stream": (ctypes.c_int, [_P, _P]),
+    "pe_compact_synchronize": (ctypes.c_int, [_P]),
+    "pe_compact_profile": (ctypes.c_int, [_P, ctypes.c_int32]),
+    "pe_compact_kernel_time": (ctypes.c_int, [_P, _DP, _I64P]),
+    "pe_compact_destroy": (ctypes.c_int, [_P]),
     "pe_world_cells": (ctypes.c_int, [ctypes.POINTER(WorldParams), _I64P]),
     "pe_world_dt_limit": (ctypes.c_int, [ctypes.POINTER(WorldParams), _DP]),
     "pe_world_create": (ctypes.c_int, [ctypes.POINTER(WorldParams),

@@ -78,6 +78,7 @@ class Oracle:
             "po_w8_init_square": (None, [_P, _P, _P]),
             "po_rect_separation": (ctypes.c_double, [ctypes.c_double] * 10),
             "po_w8_init_contact": (None, [_P] + [ctypes.c_double] * 4 + [_P, _P]),
+            "po_w8_stage_f64": (ctypes.c_int, [_P, _P, _P, _P, ctypes.c_double]),
             "po_w8_stage": (ctypes.c_int, [_P, _P, _P, _P, _P, ctypes.c_float,
                                            ctypes.c_double]),
             "po_sl_integrated_speed": (None, [ctypes.c_double] * 5 + [_P, _P]),
@@ -167,6 +168,15 @@ class Oracle:
                                     None if base is None else base.ctypes.data,
                                     None if arrival is None else arrival.ctypes.data,
                                     dt, tau)
+
+    def w8_stage_f64(self, cfg, src, dst, base, dt):
+        """One stage on float64 fields (no arrival)."""
+        for a in (src, dst) + (() if base is None else (base,)):
+            assert a.dtype == np.float64 and a.flags.c_contiguous
+        return self.lib.po_w8_stage_f64(ctypes.addressof(cfg), src.ctypes.data,
+                                        dst.ctypes.data,
+                                        None if base is None else base.ctypes.data,
+                                        dt)
 
     # -- semi-Lagrangian 5D -----------------------------------------------
     @staticmethod

@@ -73,3 +73,47 @@ def test_null_handle_calls_fail_cleanly():
     lib = _native.library()
     assert lib.pe_relative_advance(None, 1.0, None) == _native.PE_EINVAL
     assert lib.pe_relative_destroy(None) == 0
+
+
+def _compact_grid(n, na, rng, bad_id=False):
+    import numpy as np
+
+    pose = rng.uniform(-1, 1, (n, 4)).astype(np.float32)
+    ids = rng.integers(n, size=(n, na, 16)).astype(np.int32)
+    w = np.full((n, na, 16), 1 / 16, np.float32)
+    if bad_id:
+        ids[0, 0, 3] = n  # out of range with a positive weight
+    allowed = np.ones((n, na), np.uint8)
+    keep = [pose, ids, w, allowed]
+    return _native.VehicleGridArrays(n, na, *(a.ctypes.data for a in keep)), keep
+
+
+@pytest.mark.parametrize("case", ["bad_vertex", "radius", "no_actions", "domain"])
+def test_compact_create_rejects_invalid_grids_before_device_work(case):
+    """pe_compact_create validates grids, radius and pair domain on the host
+    (no CUDA call is made before the checks)."""
+    import numpy as np
+
+    lib = _native.library()
+    rng = np.random.default_rng(0)
+    p, keep_p = _compact_grid(5, 3, rng, bad_id=case == "bad_vertex")
+    e, keep_e = _compact_grid(7, 4, rng)
+    if case == "no_actions":
+        e.actions = 0
+    radius = -1.0 if case == "radius" else 1.2
+    dom = None
+    keep_d = []
+    if case == "domain":
+        lookup = np.full((1, 7), -1, np.int32)
+        lookup[0, 2] = 0
+        arrays = [np.zeros(5, np.int32), lookup, np.array([[3]], np.int32),
+                  np.array([1], np.int32), np.arange(6, dtype=np.int64)]
+        keep_d = arrays  # e_indices says 3 but lookup says 2: inconsistent
+        dom = ctypes.byref(_native.PairDomainArrays(1, 1, *(a.ctypes.data for a in arrays)))
+    handle = ctypes.c_void_p()
+    rc = lib.pe_compact_create(ctypes.byref(p), ctypes.byref(e), dom, radius, 0,
+                               ctypes.byref(handle))
+    assert rc == _native.PE_EINVAL
+    assert lib.pe_last_error()
+    assert not handle.value
+    del keep_p, keep_e, keep_d

@@ -181,30 +181,89 @@ def test_contact_game_full_size_properties(oracle):
     assert v0[5, 5, 0, 0, 5, 5, 0, 0] < 0
 
 
-def _contact_run(grid, steps, fast):
-    with WorldSolver(A3, grid, avoid=False, fast=fast) as s:
-        s.init_contact((0.5, 0.3), (0.5, 0.3))
+def _contact_run(grid, steps, fast, order=2, boundary="linear", avoid=False):
+    with WorldSolver(A3, grid, avoid=avoid, fast=fast, order=order,
+                     speed_boundary=boundary) as s:
+        if avoid:
+            s.init_square()
+        else:
+            s.init_contact((0.5, 0.3), (0.5, 0.3))
         for _ in range(steps):
             s.step(s.dt_limit)
         return s.field().ravel().astype(np.float64), s.arrival().ravel()
 
 
-@pytest.mark.parametrize("grid, steps", [(WorldGrid(7, 6, 4, 3, 3.0), 20),
-                                         (WorldGrid(11, 9, 7, 7, 3.0), 10)])
-def test_fast_world_step_tracks_the_exact_step(grid, steps):
-    """Reciprocal spacings and multiply-add contraction against the
+@pytest.mark.parametrize("grid, steps, order, boundary, avoid", [
+    (WorldGrid(7, 6, 4, 3, 3.0), 20, 2, "linear", False),
+    (WorldGrid(11, 9, 7, 7, 3.0), 10, 2, "linear", False),
+    (WorldGrid(7, 5, 3, 4, 3.0), 20, 2, "legacy_signed", False),
+    (WorldGrid(7, 6, 4, 3, 3.0), 20, 1, "linear", False),
+    (WorldGrid(7, 4, 3, 3, 4.0), 20, 1, "legacy_signed", True),
+    (WorldGrid(9, 6, 5, 4, 4.0), 10, 2, "legacy_signed", True),
+])
+def test_fast_world_step_tracks_the_exact_step(grid, steps, order, boundary, avoid):
+    """The fast stage (evader blocks staged in shared memory, reciprocal
+    spacings, multiply-add contraction, upwind-folded flow terms) against the
     reference-order stage.  The contact field has kinks where the reference's
     `<=` ENO2 comparisons meet exact ties; rounding breaks some of them the
-    other way, and later steps carry that to neighbours.  Stated bounds:
-    99.9 % of the cells within 2e-5 + 2e-6|v|, mean difference below 1e-6
-    (so at most 0.1 % of the cells can be off by 1e-3 or more), none above
-    0.1; capture times agree to 1e-3 s on 99.9 % of the cells captured in
-    both runs."""
-    exact, arr_exact = _contact_run(grid, steps, fast=False)
-    fast, arr_fast = _contact_run(grid, steps, fast=True)
+    other way, and later steps carry that to neighbours (the reference-order
+    float32 stage itself leaves 0.2 % of the cells of a 5-step run beyond
+    2e-5 of the double-precision stage, see test_oracle.py).  Stated bounds:
+    99 % of the cells within 2e-5 + 2e-6|v|, mean difference below 3e-6
+    (the reference-order stage is 1.2e-6 from the double stage after 5 steps),
+    none above 0.1; capture times agree to 1e-3 s on 99.9 % of the cells
+    captured in both runs."""
+    exact, arr_exact = _contact_run(grid, steps, False, order, boundary, avoid)
+    fast, arr_fast = _contact_run(grid, steps, True, order, boundary, avoid)
     diff = np.abs(fast - exact)
     loose = diff > 2e-5 + 2e-6 * np.abs(exact)
-    assert loose.mean() <= 1e-3, loose.mean()
-    assert diff.mean() <= 1e-6 and diff.max() <= 0.1, (diff.mean(), diff.max())
+    assert loose.mean() <= 1e-2, loose.mean()
+    assert diff.mean() <= 3e-6 and diff.max() <= 0.1, (diff.mean(), diff.max())
     both = ~np.isnan(arr_exact) & ~np.isnan(arr_fast)
     assert np.mean(np.abs(arr_exact[both] - arr_fast[both]) <= 1e-3) >= 0.999
+
+
+def _oracle_cfg(grid, order, boundary, avoid):
+    p, e = A3.pursuer, A3.evader
+    return oracle_lib.W8Cfg(grid.positions, grid.headings, grid.p_speeds,
+                            grid.e_speeds, order, int(boundary == "linear"),
+                            int(avoid), grid.extent, A3.arena_half_width,
+                            A3.capture_radius, p.speed_min, p.speed_max,
+                            e.speed_min, e.speed_max, p.acceleration,
+                            e.acceleration, p.max_curvature, e.max_curvature, 0.8)
+
+
+@pytest.mark.parametrize("grid, steps, order, boundary, avoid", [
+    (WorldGrid(7, 6, 4, 3, 3.0), 20, 2, "linear", False),
+    (WorldGrid(7, 5, 3, 4, 3.0), 20, 2, "legacy_signed", False),
+    (WorldGrid(7, 6, 4, 3, 3.0), 20, 1, "linear", False),
+    (WorldGrid(7, 4, 3, 3, 4.0), 20, 1, "legacy_signed", True),
+])
+def test_fast_world_step_is_as_accurate_as_the_exact_step(oracle, grid, steps, order,
+                                                          boundary, avoid):
+    """Both float32 stages against the double-precision stage of the oracle
+    run from the same field with the same dt: the fast stage's error is no
+    larger than the reference-order stage's (within a factor of two on the
+    mean, on the fraction of cells beyond 2e-5 + 2e-6|v| and on the max)."""
+    exact, _ = _contact_run(grid, steps, False, order, boundary, avoid)
+    fast, _ = _contact_run(grid, steps, True, order, boundary, avoid)
+    cfg = _oracle_cfg(grid, order, boundary, avoid)
+    if avoid:
+        a32, _ = oracle.w8_init_square(cfg)
+    else:
+        a32, _ = oracle.w8_init_contact(cfg, (0.5, 0.3), (0.5, 0.3))
+    a = a32.astype(np.float64)
+    b = np.zeros_like(a)
+    with WorldSolver(A3, grid, avoid=avoid, order=order, speed_boundary=boundary) as s:
+        dt = float(np.float32(s.dt_limit))
+    for _ in range(steps):
+        assert oracle.w8_stage_f64(cfg, a, b, None, dt) == 0
+        if order == 1:
+            a, b = b, a
+        else:
+            assert oracle.w8_stage_f64(cfg, b, a, a, dt) == 0
+    err_exact, err_fast = np.abs(exact - a), np.abs(fast - a)
+    tol = 2e-5 + 2e-6 * np.abs(a)
+    assert err_fast.mean() <= 2 * err_exact.mean() + 1e-8, (err_fast.mean(), err_exact.mean())
+    assert np.mean(err_fast > tol) <= 2 * np.mean(err_exact > tol) + 1e-4
+    assert err_fast.max() <= 2 * err_exact.max() + 1e-4, (err_fast.max(), err_exact.max())
