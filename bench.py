@@ -449,6 +449,111 @@ def batch_section(seed=0, count=256):
             "tiles": tiles}
 
 
+def synthetic_vehicle_grid(limits, *, half_width, step, headings, speeds, dt=0.05):
+    """A compact-game vehicle grid with the reference solve's shapes
+    (local_game/reference.py:176-195: 16 headings, 7 speeds) on a synthetic
+    lattice: every lattice state is legal, and the successor of each of the 9
+    held controls (accel in {-A, 0, A} x curvature in {-K, 0, K}) is a plain
+    arc over dt, interpolated with VehicleGrid.stencil.  The reference builds
+    its grids with its native geometry engine (legality, braking backups);
+    only the shapes and the stencil structure matter for throughput."""
+    from pursuit_evasion_b200.local_game.grid_game import VehicleGrid
+
+    n = int(round(2 * half_width / step))
+    x = (np.arange(n + 2) - (n + 1) / 2) * step
+    axes = (x, x, np.arange(headings) * 2 * np.pi / headings - np.pi,
+            np.linspace(limits.speed_min, limits.speed_max, speeds))
+    states = np.stack(np.meshgrid(*axes, indexing="ij"), -1).reshape(-1, 4)
+    controls = np.array([[a, k] for a in (-limits.acceleration, 0, limits.acceleration)
+                         for k in (-limits.max_curvature, 0, limits.max_curvature)])
+    v = states[:, None, 3]
+    v2 = np.clip(v + controls[None, :, 0] * dt, limits.speed_min, limits.speed_max)
+    dist = 0.5 * (v + v2) * dt
+    turn = controls[None, :, 1] * dist
+    mid = states[:, None, 2] + 0.5 * turn
+    nxt = np.stack([states[:, None, 0] + dist * np.cos(mid),
+                    states[:, None, 1] + dist * np.sin(mid),
+                    np.mod(states[:, None, 2] + turn + np.pi, 2 * np.pi) - np.pi, v2], -1)
+    grid = VehicleGrid(axes, states, np.arange(len(states), dtype=np.int32), controls,
+                       None, None, None, None)
+    ids, w, valid, _, mass = grid.stencil(nxt)
+    grid.successors = ids.reshape(len(states), len(controls), 16)
+    grid.weights = w.reshape(len(states), len(controls), 16)
+    grid.allowed = valid.reshape(len(states), len(controls))
+    grid.retained_mass = mass.reshape(len(states), len(controls))
+    return grid
+
+
+def compact_section(backups=5, with_cpu=True):
+    """The compact eight-state contact game (local_game/grid_game.py, the
+    reference's own semi-Lagrangian min-max kernel): pair-packed domain of
+    two synthetic 15 x 15 x 16 x 7 vehicle grids (half width 3.25 m, 0.5 m
+    position step, a3 limits, dt 0.05 s) within a 2 m exit radius, 0.8 x 0.5
+    / 0.4 x 0.25 m footprints; device time of `backups` fused backups."""
+    import torch
+    from pursuit_evasion_b200.local_game.geometry import CircleArena
+    from pursuit_evasion_b200.local_game.grid_game import (
+        PairDomain, backup_packed, initialize_packed, packed_gpu_arrays)
+
+    config = a3_config()
+    p = synthetic_vehicle_grid(config.pursuer, half_width=3.25, step=0.5, headings=16, speeds=7)
+    e = synthetic_vehicle_grid(config.evader, half_width=3.25, step=0.5, headings=16, speeds=7)
+    domain = PairDomain.build(p, e, 2.0)
+    arena = CircleArena([], 3.25)
+    a = packed_gpu_arrays(p, e, domain, max_gb=60)
+    stream = torch.cuda.current_stream()
+    a.set_stream(stream.cuda_stream)
+    initialize_packed(a, p, e, domain, arena)
+    backup_packed(a, p, e, domain)  # warm-up
+    a.profile(True)
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for _ in range(backups):
+        backup_packed(a, p, e, domain)
+    t1.record(stream)
+    a.synchronize()
+    ms = t0.elapsed_time(t1)
+    kms, launches = a.kernel_time()
+    a.profile(False)
+    pairs = domain.states
+    peak, _ = measured_peaks()
+    out = {"workload": "compact8d packed contact game, synthetic 15x15x16x7 vehicle grids "
+                       "(25,200 states each, 9 held controls, 16-vertex stencils), exit "
+                       f"radius 2 m, {backups} backups, float32",
+           "pairs": int(pairs), "value": pairs * backups / (ms / 1e3),
+           "unit": "pair-backups/s", "ms_per_backup": ms / backups,
+           "roofline": {"bound": "L2 gathers / issue; HBM fraction reported",
+                        "achieved": 8 * pairs * launches / (kms / 1e3) / 1e9, "peak": peak,
+                        "unit": "GB/s",
+                        "frac": 8 * pairs * launches / (kms / 1e3) / 1e9 / peak,
+                        "algorithmic_bytes_per_launch": 8 * pairs}}
+    if with_cpu:
+        import importlib.util
+
+        spec = importlib.util.spec_from_file_location(
+            "compact_game_oracle", REPO / "oracle" / "compact_game.py")
+        cg = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(cg)
+        flat = a["current"].get().astype(np.float64)
+        pd = {k: np.asarray(getattr(p, k)) for k in ("states", "successors", "weights", "allowed")}
+        ed = {k: np.asarray(getattr(e, k)) for k in ("states", "successors", "weights", "allowed")}
+        dd = {k: getattr(domain, k) for k in ("p_position", "lookup", "e_indices", "counts",
+                                              "offsets")}
+        dd["exit_radius"] = domain.exit_radius
+        ips = np.random.default_rng(0).choice(len(p.states), size=16, replace=False)
+        t = time.perf_counter()
+        cg.backup_packed(flat, pd, ed, dd, ips=ips)
+        seconds = time.perf_counter() - t
+        sample = int(sum(domain.offsets[i + 1] - domain.offsets[i] for i in ips))
+        out["cpu_baseline"] = {
+            "value": sample / seconds, "unit": "pair-backups/s", "cores": 1, "kind": "port",
+            "sample": f"oracle/compact_game.py (NumPy FP64; the reference runs this game "
+                      f"only on the GPU): the pairs of 16 random pursuer states "
+                      f"({sample} pairs), {seconds:.2f} s"}
+    a.close()
+    return out
+
+
 def run_case(name, repeats):
     """A short, fixed launch sequence of one kernel for profilers (ncu):
     no timing, no JSON line.  One warm-up launch then `repeats` launches of
@@ -638,7 +743,9 @@ def run_ours(args, world, rank, local):
         if not args.no_sections and world == 1:
             for key, fn in (("world8d", world8d_section),
                             ("semilag5d", lambda: semilag_section(not args.no_cpu_baseline)),
-                            ("batch", batch_section)):
+                            ("batch", batch_section),
+                            ("compact8d", lambda: compact_section(
+                                with_cpu=not args.no_cpu_baseline))):
                 try:
                     line[key] = fn()
                 except Exception as exc:  # report, keep the headline line

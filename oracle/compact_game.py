@@ -118,8 +118,9 @@ def e_reach(e):
     return float(np.where(w > 0, dist, 0).max()) + 1e-4
 
 
-def backup_packed(flat, p, e, domain):
-    """One backup of the packed pair vector (grid_game.py:384-421)."""
+def backup_packed(flat, p, e, domain, ips=None):
+    """One backup of the packed pair vector (grid_game.py:384-421); with
+    `ips`, only the pairs of those pursuer states are updated."""
     radius = float(domain["exit_radius"])
     n_p, n_e = len(p["states"]), len(e["states"])
     reach = radius + e_reach(e)
@@ -127,7 +128,7 @@ def backup_packed(flat, p, e, domain):
     lookup, offsets, ppos = domain["lookup"], domain["offsets"], domain["p_position"]
     ew = e["weights"].astype(np.float64)
     eid = e["successors"]
-    for ip in range(n_p):
+    for ip in range(n_p) if ips is None else ips:
         pos = ppos[ip]
         cells_e = domain["e_indices"][pos, : domain["counts"][pos]]
         if not len(cells_e):

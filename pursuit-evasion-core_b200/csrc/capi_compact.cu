@@ -19,6 +19,8 @@
 // reference's.  Rows longer than the shared-memory budget go to a
 // per-CTA scratch row in global memory (L2-resident).
 #include <cmath>
+#include <map>
+#include <utility>
 #include <vector>
 
 #include "pe_internal.h"
@@ -32,6 +34,12 @@ constexpr int kMaxRowBytes = 192 * 1024;
 
 struct CompactDev {
   int np, ne, npa, nea;
+  // reach lists: for each pursuer position class, the evader states within
+  // the exit radius plus the evader stencil reach (the only entries of an
+  // interpolated row that a reduction reads)
+  const int *p_class;        // [np] position class of each pursuer state
+  const int *reach_index;    // concatenated evader ids
+  const long long *reach_start;  // [classes + 1]
   const float4 *p_pose, *e_pose;
   const int *p_ids, *e_ids;
   const float *p_w, *e_w;
@@ -101,11 +109,11 @@ __global__ void __launch_bounds__(kThreads)
     backup_kernel(const CompactDev d, const float *__restrict__ cur, float *__restrict__ out,
                   float *__restrict__ scratch) {
   extern __shared__ float row_smem[];
-  __shared__ int s_ids[kStencil];
+  __shared__ long long s_row[kStencil], s_off[kStencil];
   __shared__ float s_w[kStencil];
   float *g = SMEM ? row_smem : scratch + (size_t)blockIdx.x * d.ne;
   const int tid = threadIdx.x;
-  const float r2 = d.exit_value * d.exit_value, reach2 = d.reach * d.reach;
+  const float r2 = d.exit_value * d.exit_value;
 
   for (int ip = blockIdx.x; ip < d.np; ip += gridDim.x) {
     int count, pos = 0;
@@ -120,6 +128,8 @@ __global__ void __launch_bounds__(kThreads)
     }
     const int *cell_e = PACKED ? d.e_indices + (long long)pos * d.max_count : nullptr;
     const float4 pp = d.p_pose[ip];
+    const int cls = d.p_class[ip];
+    const long long r_begin = d.reach_start[cls], r_end = d.reach_start[cls + 1];
     // the running minimum starts at the current value; every cell is owned
     // by the same thread for the whole pose
     for (int k = tid; k < count; k += kThreads) out[base + k] = cur[base + k];
@@ -129,27 +139,36 @@ __global__ void __launch_bounds__(kThreads)
       __syncthreads();  // the previous row's readers are done
       if (tid < kStencil) {
         const long long s = ((long long)ip * d.npa + u) * kStencil + tid;
-        s_ids[tid] = d.p_ids[s];
-        s_w[tid] = d.p_w[s];
+        const int nxt = d.p_ids[s];
+        const float w = d.p_w[s];
+        s_w[tid] = w;
+        // row bases of the vertex: its lookup row and field row (packed), its
+        // field row (dense); unused vertices get 0
+        if (PACKED) {
+          s_row[tid] = w > 0.f ? (long long)d.p_position[nxt] * d.ne : 0;
+          s_off[tid] = w > 0.f ? d.offsets[nxt] : 0;
+        } else {
+          s_off[tid] = w > 0.f ? (long long)nxt * d.ne : 0;
+        }
       }
       __syncthreads();
-      // interpolated pursuer successor against every evader state
-      for (int ie = tid; ie < d.ne; ie += kThreads) {
+      // interpolated pursuer successor against the evader states within
+      // reach (entries beyond it are never read: every evader stencil vertex
+      // of a cell in the exit radius lies within the reach)
+      for (long long t = r_begin + tid; t < r_end; t += kThreads) {
+        const int ie = __ldg(d.reach_index + t);
         float v = 0.f;
         if (PACKED) {
-          const float4 ep = d.e_pose[ie];
-          const float dx = pp.x - ep.x, dy = pp.y - ep.y;
-          if (dx * dx + dy * dy > reach2) {
-            v = d.exit_value;
-          } else {
 #pragma unroll
-            for (int k = 0; k < kStencil; k++)
-              if (s_w[k] > 0.f) v = fmaf(s_w[k], packed_at(d, cur, s_ids[k], ie), v);
-          }
+          for (int k = 0; k < kStencil; k++)
+            if (s_w[k] > 0.f) {
+              const int rank = __ldg(d.lookup + s_row[k] + ie);
+              v = fmaf(s_w[k], rank < 0 ? d.exit_value : __ldg(cur + s_off[k] + rank), v);
+            }
         } else {
 #pragma unroll
           for (int k = 0; k < kStencil; k++)
-            if (s_w[k] > 0.f) v = fmaf(s_w[k], __ldg(cur + (long long)s_ids[k] * d.ne + ie), v);
+            if (s_w[k] > 0.f) v = fmaf(s_w[k], __ldg(cur + s_off[k] + ie), v);
         }
         g[ie] = v;
       }
@@ -165,25 +184,51 @@ __global__ void __launch_bounds__(kThreads)
         const float best = out[base + k];
         float worst = -1e30f;
         bool dropped = false;
-        for (int a = 0; a < d.nea; a++) {
-          if (!d.e_allowed[(long long)ie * d.nea + a]) continue;
+        // the next allowed reply's stencil is loaded while this one reduces
+        const uint8_t *allowed = d.e_allowed + (long long)ie * d.nea;
+        int a = 0;
+        while (a < d.nea && !__ldg(allowed + a)) a++;
+        int4 ci[kStencil / 4];
+        float4 cw[kStencil / 4];
+        if (a < d.nea) {
           const long long s = ((long long)ie * d.nea + a) * kStencil;
-          const int4 *ids4 = reinterpret_cast<const int4 *>(d.e_ids + s);
-          const float4 *w4 = reinterpret_cast<const float4 *>(d.e_w + s);
+#pragma unroll
+          for (int q = 0; q < kStencil / 4; q++) {
+            ci[q] = __ldg(reinterpret_cast<const int4 *>(d.e_ids + s) + q);
+            cw[q] = __ldg(reinterpret_cast<const float4 *>(d.e_w + s) + q);
+          }
+        }
+        while (a < d.nea) {
+          int next = a + 1;
+          while (next < d.nea && !__ldg(allowed + next)) next++;
+          int4 ni[kStencil / 4];
+          float4 nw[kStencil / 4];
+          if (next < d.nea) {
+            const long long s = ((long long)ie * d.nea + next) * kStencil;
+#pragma unroll
+            for (int q = 0; q < kStencil / 4; q++) {
+              ni[q] = __ldg(reinterpret_cast<const int4 *>(d.e_ids + s) + q);
+              nw[q] = __ldg(reinterpret_cast<const float4 *>(d.e_w + s) + q);
+            }
+          }
           float value = 0.f;
 #pragma unroll
           for (int q = 0; q < kStencil / 4; q++) {
-            const int4 i = __ldg(ids4 + q);
-            const float4 w = __ldg(w4 + q);
-            if (w.x > 0.f) value = fmaf(w.x, g[i.x], value);
-            if (w.y > 0.f) value = fmaf(w.y, g[i.y], value);
-            if (w.z > 0.f) value = fmaf(w.z, g[i.z], value);
-            if (w.w > 0.f) value = fmaf(w.w, g[i.w], value);
+            if (cw[q].x > 0.f) value = fmaf(cw[q].x, g[ci[q].x], value);
+            if (cw[q].y > 0.f) value = fmaf(cw[q].y, g[ci[q].y], value);
+            if (cw[q].z > 0.f) value = fmaf(cw[q].z, g[ci[q].z], value);
+            if (cw[q].w > 0.f) value = fmaf(cw[q].w, g[ci[q].w], value);
           }
           worst = fmaxf(worst, value);
           if (worst >= best) {
             dropped = true;
             break;
+          }
+          a = next;
+#pragma unroll
+          for (int q = 0; q < kStencil / 4; q++) {
+            ci[q] = ni[q];
+            cw[q] = nw[q];
           }
         }
         if (!dropped) out[base + k] = fminf(best, worst);
@@ -297,6 +342,38 @@ int check_domain(const pe_pair_domain *dm, int np, int ne) {
   return PE_OK;
 }
 
+// Position classes of the pursuer states (equal (x, y)) and, per class, the
+// evader states within `reach` of it, in increasing order.
+void reach_lists(const pe_vehicle_grid *p, const pe_vehicle_grid *e, double reach,
+                 std::vector<int> *p_class, std::vector<int> *index,
+                 std::vector<long long> *start) {
+  std::map<std::pair<float, float>, int> classes;
+  std::vector<std::pair<float, float>> centre;
+  p_class->resize(p->states);
+  for (int i = 0; i < p->states; i++) {
+    const std::pair<float, float> xy(p->pose[4 * i], p->pose[4 * i + 1]);
+    auto it = classes.find(xy);
+    if (it == classes.end()) {
+      it = classes.emplace(xy, (int)centre.size()).first;
+      centre.push_back(xy);
+    }
+    (*p_class)[i] = it->second;
+  }
+  start->assign(1, 0);
+  index->clear();
+  // a little beyond the float32 reach test of the reference kernels, so that
+  // every entry they could read is present
+  const double r2 = (reach + 1e-5) * (reach + 1e-5);
+  for (const auto &c : centre) {
+    for (int j = 0; j < e->states; j++) {
+      const double dx = (double)c.first - e->pose[4 * j];
+      const double dy = (double)c.second - e->pose[4 * j + 1];
+      if (dx * dx + dy * dy <= r2) index->push_back(j);
+    }
+    start->push_back((long long)index->size());
+  }
+}
+
 // Largest centre displacement of an evader interpolation vertex with a
 // positive weight, plus 1e-4 (grid_game.py:456-466).
 double evader_reach(const pe_vehicle_grid *e) {
@@ -404,6 +481,14 @@ int pe_compact_create(const pe_vehicle_grid *p, const pe_vehicle_grid *e,
   d.reach = (float)(exit_radius + evader_reach(e));
   rc = upload_grid(h, p, &d.p_pose, &d.p_ids, &d.p_w, &d.p_allowed);
   if (!rc) rc = upload_grid(h, e, &d.e_pose, &d.e_ids, &d.e_w, &d.e_allowed);
+  if (!rc) {
+    std::vector<int> p_class, index;
+    std::vector<long long> start;
+    reach_lists(p, e, d.reach, &p_class, &index, &start);
+    rc = own(h, p_class.data(), p_class.size(), &d.p_class);
+    if (!rc) rc = own(h, index.data(), index.size(), &d.reach_index);
+    if (!rc) rc = own(h, start.data(), start.size(), &d.reach_start);
+  }
   if (!rc && domain) {
     d.positions = domain->positions;
     d.max_count = domain->max_count;

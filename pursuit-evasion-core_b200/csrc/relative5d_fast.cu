@@ -385,7 +385,6 @@ __global__ void __launch_bounds__(TARGET_THREADS, 2)
     const float dt = a.dt;
     const int ctr = (r + 2) * XP + x0;  // this chunk in an own slot
     const int nbo = r * XP + x0;        // this chunk in a neighbour slot
-    const bool x_edge = x0 == 0 || x0 + 5 >= g.nx;  // chunk touches an x end
     const bool tail = x0 + 4 > g.nx;                // chunk holds row padding
     float2 finite_acc = f2(0.f);
     unsigned og = 0, ng = 0;
@@ -426,18 +425,21 @@ __global__ void __launch_bounds__(TARGET_THREADS, 2)
         win[d] = *reinterpret_cast<const float4 *>(own + slot * L.own_floats + ctr);
       }
 
+      // ring positions, advanced by one per step: the refill plane k+2 (slot
+      // and phase parity), the centre plane k, the neighbour set
+      int rslot = (int)((base + 5) % OWN_SLOTS);  // plane 3, read at k = 1
+      uint32_t rpar = (uint32_t)(((base + 5) / OWN_SLOTS) & 1);
+      int cslot = (int)((base + 2) % OWN_SLOTS);
+      int ns = (int)(ng % NB_SLOTS);
+      uint32_t npar = (uint32_t)((ng / NB_SLOTS) & 1);
       for (int k = 0; k < it.steps; k++) {
         if (k > 0) {
-          const unsigned q = base + k + 4;  // plane k+2
-          const int slot = (int)(q % OWN_SLOTS);
-          if (alive) alive &= wait_phase(&own_full[slot], (uint32_t)((q / OWN_SLOTS) & 1), timeout);
+          if (alive) alive &= wait_phase(&own_full[rslot], rpar, timeout);
 #pragma unroll
           for (int d = 0; d < 4; d++) win[d] = win[d + 1];
-          win[4] = *reinterpret_cast<const float4 *>(own + slot * L.own_floats + ctr);
+          win[4] = *reinterpret_cast<const float4 *>(own + rslot * L.own_floats + ctr);
         }
-        const int ns = (int)(ng % NB_SLOTS);
-        if (alive) alive &= wait_phase(&nb_full[ns], (uint32_t)((ng / NB_SLOTS) & 1), timeout);
-        const int cslot = (int)((base + k + 2) % OWN_SLOTS);  // plane k
+        if (alive) alive &= wait_phase(&nb_full[ns], npar, timeout);
 
         if (active && alive) {
           const float *o0 = own + cslot * L.own_floats + ctr;
@@ -450,10 +452,9 @@ __global__ void __launch_bounds__(TARGET_THREADS, 2)
           const float2 xr = *reinterpret_cast<const float2 *>(o0 + 4);
           const float w[8] = {xl.x, xl.y, C.x, C.y, C.z, C.w, xr.x, xr.y};
           float xlo[4], xhi[4];
-          if (x_edge)
-            slopes_x<ORDER, true>(w, x0, g.nx, xlo, xhi);
-          else
-            slopes_x<ORDER, false>(w, x0, g.nx, xlo, xhi);
+          // every warp holds chunks at both x ends: the end rules as selects
+          // cost less than running both variants of a divergent branch
+          slopes_x<ORDER, true>(w, x0, g.nx, xlo, xhi);
           const float2 lx_a = make_float2(xlo[0], xlo[1]), lx_b = make_float2(xlo[2], xlo[3]);
           const float2 hx_a = make_float2(xhi[0], xhi[1]), hx_b = make_float2(xhi[2], xhi[3]);
 
@@ -614,6 +615,15 @@ __global__ void __launch_bounds__(TARGET_THREADS, 2)
         ng++;
         gdst += PP;
         garr += PP;
+        if (k > 0 && ++rslot == OWN_SLOTS) {
+          rslot = 0;
+          rpar ^= 1u;
+        }
+        if (++cslot == OWN_SLOTS) cslot = 0;
+        if (++ns == NB_SLOTS) {
+          ns = 0;
+          npar ^= 1u;
+        }
       }
       og = base + it.steps + 4;
     }
