@@ -6,17 +6,20 @@
 // interpolation of every successor only mixes the three vP and three vE
 // slabs around the item, with weights that depend on the acceleration
 // alone, so the item stages, for each of the 9 (pursuer accel, evader
-// accel) combinations, the speed-blended (y, x) plane of three consecutive
-// headings in a shared-memory ring (27 planes, rows + 4 by 72 floats, with
-// two halo cells on every side holding the linear extension of the field
-// beyond the position box).  Every (pursuer, evader) action pair is then a
-// bilinear gather of 4 corners in each of two ring planes plus a heading
-// lerp: 8 shared-memory loads instead of 32 global ones.
+// accel) combinations, the speed-blended (y, x) planes of three consecutive
+// headings in shared memory (rows + 4 by 72 positions, with two halo cells
+// on every side holding the linear extension of the field beyond the
+// position box).  They are kept as two "heading-pair" planes of float2:
+// (psi-1, psi) and (psi, psi+1), the lower and upper heading of a successor
+// side by side.  Every (pursuer, evader) action pair is then a bilinear
+// gather of 4 float2 corners (both heading planes at once) plus a heading
+// lerp: 4 shared-memory loads instead of 32 global ones, with the position
+// lerps in packed FP32.
 //
-// The heading ring advances one plane per psi step: the raw slab rows of
-// the plane after next are fetched with cp.async while the current plane
-// is computed, extended into the halo, blended and stored over the plane
-// that is no longer needed.
+// The ring advances one heading per psi step: the raw slab rows of the
+// plane after next are fetched with cp.async while the current heading is
+// computed, extended into the halo, blended, and written with the plane
+// before it as the new heading pair over the pair that is no longer needed.
 //
 // Value-only backups prune with the optimal (pursuer, evader) pair of the
 // previous backup at each cell (a hint byte) as the guide: a pursuer action
@@ -43,21 +46,21 @@ constexpr int kCombos = 9;
 constexpr float kMagic = 12582912.0f;  // 1.5 * 2^23: x + kMagic rounds x to an integer
 constexpr unsigned kMagicBits = 0x4B400000u;
 constexpr int kCPT = 2;  // cells per thread
+// Tiles have at most kRowsMax rows, so every staged plane has the fixed
+// stride kPlane and all ring and raw offsets are compile-time multiples.
+constexpr int kRowsMax = 13;
+constexpr int kRR = kRowsMax + 2 * kHalo;  // staged rows of a plane
+constexpr int kPlane = kRR * kPitch;       // positions per staged plane
 
 struct __align__(16) SLPair {  // one (pursuer, evader) action pair at the current heading
-  float ox, oy;     // successor offset in local ring coordinates
-  float c, s;       // the pursuer's turn: successor = R(c, s) (X, Y) + (ox, oy)
-  float wp;         // heading weight of the upper plane
-  unsigned lo, hi;  // ring offsets of the lower / upper heading plane, minus
-                    // the magic bits of the packed (row, col) index
-  float pad;
+  float2 o;        // successor offset in local ring coordinates
+  float2 cc;       // (c, c), (s, s): the pursuer's turn, successor =
+  float2 ss;       //   c (X, Y) + s (Y, -X) + o
+  float wp;        // heading weight of the upper plane
+  unsigned base;   // float2 offset of its heading-pair plane, minus the
+                   // magic bits of the packed (row, col) index
 };
 static_assert(sizeof(SLPair) == 32, "pair table entry is 32 bytes");
-
-__device__ __forceinline__ int mod3(int q) {
-  const int r = q % 3;
-  return r < 0 ? r + 3 : r;
-}
 
 __device__ __forceinline__ int wrap_psi(int q, int nh) {
   const int r = q % nh;
@@ -86,27 +89,28 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) {  // a - b
+  return __ffma2_rn(b, make_float2(-1.f, -1.f), a);
+}
+
 // Interpolated value of one action pair at a cell with centred index
 // coordinates P = (X, Y) and Q = (Y, -X).  Both position axes, and the two
-// heading planes, are carried side by side in packed FP32 pairs.
-__device__ __forceinline__ float pair_value(const float *ring, const SLPair &p, float2 P,
+// heading planes (the .x and .y of every ring element), are carried side by
+// side in packed FP32 pairs.
+__device__ __forceinline__ float pair_value(const float2 *ring, const SLPair &p, float2 P,
                                             float2 Q) {
-  const float2 F = __ffma2_rn(make_float2(p.c, p.c), P,
-                              __ffma2_rn(make_float2(p.s, p.s), Q, make_float2(p.ox, p.oy)));
+  const float2 F = __ffma2_rn(p.cc, P, __ffma2_rn(p.ss, Q, p.o));
+  // round(F - 0.5) + magic: the floor of F in the low mantissa bits
   const float2 T = __fadd2_rn(__fadd2_rn(F, make_float2(-0.5f, -0.5f)),
-                              make_float2(kMagic, kMagic));  // round(F - 0.5) + magic
-  const float2 W = __fadd2_rn(F, __fadd2_rn(make_float2(kMagic, kMagic), make_float2(-T.x, -T.y)));
-  const unsigned idx = __float_as_uint(T.y) * (unsigned)kPitch + __float_as_uint(T.x);
-  const float *a = ring + (int)(idx + p.lo);
-  const float *b = ring + (int)(idx + p.hi);
-  // (lower plane, upper plane) pairs of the four corners
-  const float2 v00 = make_float2(a[0], b[0]), v01 = make_float2(a[1], b[1]);
-  const float2 v10 = make_float2(a[kPitch], b[kPitch]);
-  const float2 v11 = make_float2(a[kPitch + 1], b[kPitch + 1]);
+                              make_float2(kMagic, kMagic));
+  const float2 W = sub2(F, __fadd2_rn(T, make_float2(-kMagic, -kMagic)));
+  const unsigned idx = __float_as_uint(T.y) * (unsigned)kPitch + __float_as_uint(T.x) + p.base;
+  const float2 *a = ring + idx;
+  const float2 v00 = a[0], v01 = a[1], v10 = a[kPitch], v11 = a[kPitch + 1];
   const float2 wx = make_float2(W.x, W.x), wy = make_float2(W.y, W.y);
-  const float2 r0 = __ffma2_rn(wx, __fadd2_rn(v01, make_float2(-v00.x, -v00.y)), v00);
-  const float2 r1 = __ffma2_rn(wx, __fadd2_rn(v11, make_float2(-v10.x, -v10.y)), v10);
-  const float2 r = __ffma2_rn(wy, __fadd2_rn(r1, make_float2(-r0.x, -r0.y)), r0);
+  const float2 r0 = __ffma2_rn(wx, sub2(v01, v00), v00);
+  const float2 r1 = __ffma2_rn(wx, sub2(v11, v10), v10);
+  const float2 r = __ffma2_rn(wy, sub2(r1, r0), r0);
   return fmaf(p.wp, r.y - r.x, r.x);
 }
 
@@ -144,7 +148,7 @@ __device__ __forceinline__ float extended(const float *raw_plane, int gx, int gy
 //      (hu if it remains, else the lowest probe) in full;
 //  C2. the remaining actions one reply at a time (he first), each abandoned
 //      once its reply maximum reaches `best`.
-__device__ __forceinline__ void minmax_cell(const float *ring, const SLPair *pairs, float2 P,
+__device__ __forceinline__ void minmax_cell(const float2 *ring, const SLPair *pairs, float2 P,
                                             float2 Q, int hu, int he, bool live, float &best,
                                             int &bu, int &be) {
   bu = hu;
@@ -222,11 +226,13 @@ __global__ void __launch_bounds__(SL_TILED_MAX_THREADS, 1)
     sl_tiled_kernel(const SLGrid g, const SLBackup b, const SLTiled t,
                     const SLTiledPlan plan) {
   extern __shared__ __align__(16) float smem[];
-  const int rr = plan.rows + 2 * kHalo;  // staged rows
-  const int pl = rr * kPitch;            // floats per staged plane
-  float *ring = smem;                    // [combo][slot][rr][kPitch]
-  float *raw = ring + 3 * kCombos * pl;  // [slab][rr][kPitch]
+  constexpr int pl = kPlane;
+  // heading-pair planes [combo][q & 1][rr][kPitch] of float2: the pair
+  // (q, q+1) (plane q in .x, q+1 in .y) lives in slot q & 1
+  float2 *ring = reinterpret_cast<float2 *>(smem);
+  float *raw = smem + 2 * 2 * kCombos * pl;  // [slab][rr][kPitch]
   SLPair *pairs = reinterpret_cast<SLPair *>(raw + kCombos * pl);
+  __shared__ int64_t slab_off[kCombos];
 
   const int nx = g.nx, nh = g.nh;
   const int tid = threadIdx.x, nthreads = blockDim.x;
@@ -248,18 +254,35 @@ __global__ void __launch_bounds__(SL_TILED_MAX_THREADS, 1)
     const int p0 = chunk * plan.psi_chunk, p1 = min(nh, p0 + plan.psi_chunk);
     const SLSpeedStep ps = t.pstep[iv], es = t.estep[ie];
     const int gy_lo = max(0, ty0 - kHalo), gy_hi = min(nx, ty0 + trows + kHalo);
-    const int in_rows = gy_hi - gy_lo;
+    // this thread's cells of every heading plane of the item: row << 16 |
+    // column, or -1 past the tile
+    int cpos[CPT];
+#pragma unroll
+    for (int k = 0; k < CPT; k++) {
+      const int c = tid + k * nthreads;
+      const int row = c / nx;
+      cpos[k] = c < trows * nx ? (row << 16) | (c - row * nx) : -1;
+    }
+    const int64_t item_base = (((int64_t)iv * g.nve + ie) * nh) * nx * nx + (int64_t)ty0 * nx;
+    // offsets of the 9 staged (vP, vE) slabs at heading 0
+    if (tid < kCombos) {
+      const int va = ps.base + tid / 3, vb = es.base + tid % 3;
+      slab_off[tid] = ((int64_t)va * g.nve + vb) * nh * nx * nx;
+    }
+    __syncthreads();
 
     // raw slab rows of heading plane q (unwrapped) -> raw, asynchronously;
     // one warp per (slab, row), lanes along x
     auto load_raw = [&](int q) {
-      const int w = wrap_psi(q, nh);
-      for (int rw = warp; rw < kCombos * in_rows; rw += nwarps) {
-        const int s = rw / in_rows, gy = gy_lo + (rw - s * in_rows);
-        const int va = ps.base + s / 3, vb = es.base + s % 3;
-        const float *src = b.src + ((((int64_t)va * g.nve + vb) * nh + w) * nx + gy) * nx;
-        float *dst = raw + s * pl + (gy - ty0 + kHalo) * kPitch + kHalo;
-        for (int gx = lane; gx < nx; gx += 32) cp_async4(dst + gx, src + gx);
+      const float *plane_src = b.src + (int64_t)wrap_psi(q, nh) * nx * nx;
+      for (int rw = warp; rw < kCombos * kRR; rw += nwarps) {
+        const int s = rw / kRR, gy = ty0 - kHalo + (rw - s * kRR);
+        if (gy < gy_lo || gy >= gy_hi) continue;
+        const float *src = plane_src + slab_off[s] + gy * nx + lane;
+        float *dst = raw + s * pl + (gy - ty0 + kHalo) * kPitch + kHalo + lane;
+#pragma unroll
+        for (int i = 0; i < (kPitch - 2 * kHalo + 31) / 32; i++)  // nx <= kPitch - 4
+          if (lane + 32 * i < nx) cp_async4(dst + 32 * i, src + 32 * i);
       }
     };
     // halo of the raw plane (needs the in-box rows in place): the two
@@ -267,27 +290,35 @@ __global__ void __launch_bounds__(SL_TILED_MAX_THREADS, 1)
     // column), whole rows beyond the box (lanes along x)
     auto fill_halo = [&]() {
       const int srows = trows + 2 * kHalo;
-      const int side = kCombos * in_rows * 2 * kHalo;
+      constexpr int side = kCombos * kRR * 2 * kHalo;
       for (int k = tid; k < side; k += nthreads) {
-        const int s = k / (in_rows * 2 * kHalo), r = k - s * (in_rows * 2 * kHalo);
-        const int gy = gy_lo + r / (2 * kHalo), q = r % (2 * kHalo);
+        const int s = k / (kRR * 2 * kHalo), r = k - s * (kRR * 2 * kHalo);
+        const int gy = ty0 - kHalo + r / (2 * kHalo), q = r % (2 * kHalo);
+        if (gy < gy_lo || gy >= gy_hi) continue;
         const int gx = q < kHalo ? q - kHalo : nx + q - kHalo;
         float *plane = raw + s * pl;
         plane[(gy - ty0 + kHalo) * kPitch + gx + kHalo] = extended(plane, gx, gy, nx, ty0);
       }
-      for (int rw = warp; rw < kCombos * srows; rw += nwarps) {
-        const int s = rw / srows, lr = rw - s * srows;
+      if (ty0 >= kHalo && ty0 + trows + kHalo <= nx) return;  // no row beyond the box
+      for (int rw = warp; rw < kCombos * kRR; rw += nwarps) {
+        const int s = rw / kRR, lr = rw - s * kRR;
         const int gy = ty0 - kHalo + lr;
-        if (gy >= 0 && gy < nx) continue;
+        if (lr >= srows || (gy >= 0 && gy < nx)) continue;
         float *plane = raw + s * pl;
         for (int lc = lane; lc < nx + 2 * kHalo; lc += 32)
           plane[lr * kPitch + lc] = extended(plane, lc - kHalo, gy, nx, ty0);
       }
     };
-    // speed blends of the raw plane into ring slot `slot` (whole rows of the
-    // pitch: the pad columns past nx + 4 hold unused values, never read)
-    auto blend = [&](int slot) {
+    // speed blends of the raw plane of heading q (whole rows of the pitch:
+    // the pad columns past nx + 4 hold unused values, never read).  MODE
+    // 0 (warm-up): write the plane as .x of pair (q, q+1) if `as_lower` and
+    // as .y of pair (q-1, q) if `as_upper`; MODE 1 (advance): write pair
+    // (q-1, q) whole, its .x copied from the .y of pair (q-2, q-1).
+    auto blend = [&](int q, bool as_lower, bool as_upper, bool advance) {
       const int count = (trows + 2 * kHalo) * kPitch;
+      float2 *lower = ring + (q & 1) * pl;        // pair (q, q+1), combo 0
+      float2 *upper = ring + ((q - 1) & 1) * pl;  // pair (q-1, q), combo 0
+      const float2 *prev = ring + ((q - 2) & 1) * pl;  // pair (q-2, q-1)
       for (int off = tid; off < count; off += nthreads) {
         float v[9];
 #pragma unroll
@@ -312,7 +343,14 @@ __global__ void __launch_bounds__(SL_TILED_MAX_THREADS, 1)
             const float w = es.w[e], w0 = 1.f - w;
             const float x0 = lo == 0 ? pv[a][0] : pv[a][1];
             const float x1 = lo == 0 ? pv[a][1] : pv[a][2];
-            ring[((a * 3 + e) * 3 + slot) * pl + off] = fmaf(w, x1, w0 * x0);
+            const float nv = fmaf(w, x1, w0 * x0);
+            const int c = (a * 3 + e) * 2 * pl + off;
+            if (advance) {
+              upper[c] = make_float2(prev[c].y, nv);
+            } else {
+              if (as_lower) reinterpret_cast<float *>(lower + c)[0] = nv;
+              if (as_upper) reinterpret_cast<float *>(upper + c)[1] = nv;
+            }
           }
       }
     };
@@ -325,24 +363,22 @@ __global__ void __launch_bounds__(SL_TILED_MAX_THREADS, 1)
         const SLEvaderMove em = b.emove[((int64_t)wrap_psi(ip, nh) * g.nve + ie) * 9 + ue];
         const float dxp = em.ex - pa.px, dyp = em.ey - pa.py;
         SLPair p;
-        p.ox = fmaf(pa.c, dxp, pa.s * dyp) * g.ihx + center + (float)kHalo;
-        p.oy = fmaf(pa.c, dyp, -pa.s * dxp) * g.ihx + center + (float)(kHalo - ty0);
-        p.c = pa.c;
-        p.s = pa.s;
+        p.o = make_float2(fmaf(pa.c, dxp, pa.s * dyp) * g.ihx + center + (float)kHalo,
+                          fmaf(pa.c, dyp, -pa.s * dxp) * g.ihx + center + (float)(kHalo - ty0));
+        p.cc = make_float2(pa.c, pa.c);
+        p.ss = make_float2(pa.s, pa.s);
         const float delta = ea.turn_idx - pa.turn_idx;
         const float fl = floorf(delta);
         p.wp = delta - fl;
         const int combo = (up / 3) * 3 + ue / 3;
-        const int q = ip + (int)fl;
+        const int q = ip + (int)fl;  // lower heading of the successor
         const unsigned bias = kMagicBits * (unsigned)(kPitch + 1);
-        p.lo = (unsigned)((combo * 3 + mod3(q)) * pl) - bias;
-        p.hi = (unsigned)((combo * 3 + mod3(q + 1)) * pl) - bias;
-        p.pad = 0.f;
+        p.base = (unsigned)((combo * 2 + (q & 1)) * pl) - bias;
         pairs[k] = p;
       }
     };
 
-    // warm-up: planes p0-1, p0, p0+1 into the ring
+    // warm-up: planes p0-1, p0, p0+1 into the pairs (p0-1, p0), (p0, p0+1)
     for (int q = p0 - 1; q <= p0 + 1; q++) {
       load_raw(q);
       cp_async_commit_wait();
@@ -350,7 +386,7 @@ __global__ void __launch_bounds__(SL_TILED_MAX_THREADS, 1)
       fill_halo();
       if (q == p0 + 1) pair_table(p0);
       __syncthreads();
-      blend(mod3(q));
+      blend(q, q <= p0, q >= p0, false);
       __syncthreads();
     }
     if (p0 + 2 <= p1) load_raw(p0 + 2);
@@ -358,13 +394,13 @@ __global__ void __launch_bounds__(SL_TILED_MAX_THREADS, 1)
 
     for (int ip = p0; ip < p1; ip++) {
       // ---- compute the cells of heading ip (one cell of each thread at a time)
+      const int64_t plane_base = item_base + (int64_t)ip * nx * nx;
 #pragma unroll 1
       for (int k = 0; k < CPT; k++) {
-        const int c = tid + k * nthreads;
-        const bool valid = c < trows * nx;
-        const int row = valid ? c / nx : 0, col = valid ? c - row * nx : 0;
+        const bool valid = cpos[k] >= 0;
+        const int row = valid ? cpos[k] >> 16 : 0, col = valid ? cpos[k] & 0xffff : 0;
         const int iy = ty0 + row;
-        const int64_t cell = ((((int64_t)iv * g.nve + ie) * nh + ip) * nx + iy) * nx + col;
+        const int64_t cell = plane_base + (int64_t)row * nx + col;
         const float cur = valid ? b.src[cell] : 0.f;
         const int h = valid ? (int)t.hint[cell] : 0x44;
         const float x = fmaf((float)col, g.dx, -g.extent);
@@ -391,13 +427,13 @@ __global__ void __launch_bounds__(SL_TILED_MAX_THREADS, 1)
         }
       }
       if (ip + 1 < p1) {
-        // ---- advance the ring: plane ip+2 replaces plane ip-1
+        // ---- advance the ring: pair (ip+1, ip+2) replaces pair (ip-1, ip)
         cp_async_wait();
         __syncthreads();
         fill_halo();
         pair_table(ip + 1);
         __syncthreads();
-        blend(mod3(ip + 2));
+        blend(ip + 2, false, false, true);
         __syncthreads();
         if (ip + 3 <= p1) load_raw(ip + 3);
         cp_async_commit();
@@ -449,14 +485,15 @@ cudaError_t launch(const SLGrid &g, const SLBackup &b, const SLTiled &t,
 bool sl_tiled_plan(const SLGrid &g, int max_smem, int want_rows, SLTiledPlan *plan) {
   const int nx = g.nx;
   if (nx + 2 * kHalo > kPitch || g.nvp < 3 || g.nve < 3) return false;
-  // rows per tile: about 864 cells (432 threads), at most 16 rows, equal tiles
+  // rows per tile: about 864 cells (432 threads), at most kRowsMax rows,
+  // equal tiles
   int rows = want_rows > 0 ? want_rows : 864 / nx;
-  rows = rows < 1 ? 1 : (rows > 16 ? 16 : rows);
+  rows = rows < 1 ? 1 : (rows > kRowsMax ? kRowsMax : rows);
   const int tiles = (nx + rows - 1) / rows;
   rows = (nx + tiles - 1) / tiles;
-  const int rr = rows + 2 * kHalo;
-  const size_t smem = sizeof(float) * (size_t)(4 * kCombos) * rr * kPitch +
-                      sizeof(SLPair) * 81;
+  // two float2 heading-pair planes and one raw plane per combination, at
+  // the fixed plane stride
+  const size_t smem = sizeof(float) * (size_t)(5 * kCombos) * kPlane + sizeof(SLPair) * 81;
   if ((int)smem > max_smem) return false;
   const int cells = rows * nx;
   int threads = ((cells + kCPT - 1) / kCPT + 31) / 32 * 32;
