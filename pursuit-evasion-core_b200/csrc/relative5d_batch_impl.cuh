@@ -84,35 +84,67 @@ __device__ __forceinline__ int find_solve(const Rel5BatchArgs &A, int64_t item) 
   return lo;
 }
 
+// One stage of every active item.  A CTA's items (blockIdx.x, +gridDim.x,
+// ...) mostly fall in the same solve as the one before, so the solve's
+// descriptor is looked up (binary search) and staged in shared memory only
+// when the item leaves the cached solve's range, and the residual
+// reductions (block maxima, atomics) run once per solve and CTA rather
+// than once per item.
 template <int BLEND, class Cell>
 __device__ void stage_items(const Rel5BatchArgs &A, int step, int64_t n_items,
-                            double *scratch) {
+                            double *scratch, Rel5Grid *sg) {
+  int64_t lo = 0, hi = 0;  // item range of the cached solve
+  const Rel5BatchSolve *S = nullptr;
+  Rel5Stage s{};
+  int rows = 1, blocks = 1;
+  double change_abs = 0, change_up = 0;
+  bool bad = false;
+  auto flush = [&]() {
+    if (!S) return;
+    if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(&S->stats->nonfinite, 1u);
+    if (BLEND) {
+      const double m_abs = block_max(change_abs, scratch);
+      const double m_up = block_max(change_up, scratch);
+      if (threadIdx.x == 0) {
+        atomic_max_nonneg(&S->stats->residual, m_abs);
+        atomic_max_nonneg(&S->stats->increase, m_up);
+      }
+    }
+    change_abs = change_up = 0;
+    bad = false;
+  };
   for (int64_t item = blockIdx.x; item < n_items; item += gridDim.x) {
-    const Rel5BatchSolve &S = A.solves[find_solve(A, item)];
-    const Rel5Grid &g = S.g;
-    int64_t local = item - S.item_base;
-    const int blocks = (g.nx + S.rows - 1) / S.rows;
+    if (item < lo || item >= hi) {  // the same for every thread of the CTA
+      flush();
+      S = &A.solves[find_solve(A, item)];
+      lo = S->item_base;
+      hi = lo + S->items;
+      __syncthreads();  // the previous solve's grid copy is no longer read
+      if (threadIdx.x == 0) *sg = S->g;
+      const double2 td = S->steps[step];
+      s.src = BLEND ? S->b : S->a;
+      s.dst = BLEND ? S->a : S->b;
+      s.arrival = S->arrival;
+      s.sn = S->sn;
+      s.cs = S->cs;
+      s.t = td.x;
+      s.dt = td.y;
+      s.stats = S->stats;
+      rows = S->rows;
+      __syncthreads();
+      blocks = (sg->nx + rows - 1) / rows;
+    }
+    const Rel5Grid &g = *sg;
+    int64_t local = item - lo;
     const int rb = (int)(local % blocks);
     local /= blocks;
     const int ip = (int)(local % g.nh);
     local /= g.nh;
     const int ie = (int)(local % g.nve);
     const int iv = (int)(local / g.nve);
-    const double2 td = S.steps[step];
-    Rel5Stage s{};
-    s.src = BLEND ? S.b : S.a;
-    s.dst = BLEND ? S.a : S.b;
-    s.arrival = S.arrival;
-    s.sn = S.sn;
-    s.cs = S.cs;
-    s.t = td.x;
-    s.dt = td.y;
-    s.stats = S.stats;
-    const int y0 = rb * S.rows, y1 = min(g.nx, y0 + S.rows);
+    const int y0 = rb * rows, y1 = min(g.nx, y0 + rows);
     const int cells = (y1 - y0) * g.nx;
     const int64_t plane = (((int64_t)iv * g.nve + ie) * g.nh + ip) * g.sp;
-    double change_abs = 0, change_up = 0;
-    bool bad = false;
     for (int c = threadIdx.x; c < cells; c += blockDim.x) {
       const int iy = y0 + c / g.nx, ix = c % g.nx;
       double ca = 0, cu = 0;
@@ -121,22 +153,15 @@ __device__ void stage_items(const Rel5BatchArgs &A, int step, int64_t n_items,
       change_abs = fmax(change_abs, ca);
       change_up = fmax(change_up, cu);
     }
-    if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(&S.stats->nonfinite, 1u);
-    if (BLEND) {
-      const double m_abs = block_max(change_abs, scratch);
-      const double m_up = block_max(change_up, scratch);
-      if (threadIdx.x == 0) {
-        atomic_max_nonneg(&S.stats->residual, m_abs);
-        atomic_max_nonneg(&S.stats->increase, m_up);
-      }
-    }
   }
+  flush();
 }
 
 template <class Cell>
 __global__ void __launch_bounds__(kRel5BatchThreads)
     rel5_batch_kernel(const Rel5BatchArgs A) {
   __shared__ double scratch[kRel5BatchThreads / 32];
+  __shared__ Rel5Grid sg;  // grid of the solve whose items the CTA is on
   unsigned round = 0;
   for (int step = 0; step < A.max_steps; step++) {
     const int64_t n_items = A.active_items[step];
@@ -145,9 +170,9 @@ __global__ void __launch_bounds__(kRel5BatchThreads)
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < A.count;
          k += gridDim.x * blockDim.x)
       if (step < A.solves[k].nsteps) A.solves[k].stats->residual = 0ull;
-    stage_items<0, Cell>(A, step, n_items, scratch);
+    stage_items<0, Cell>(A, step, n_items, scratch, &sg);
     if (!grid_barrier(A.sync, ++round)) break;
-    stage_items<1, Cell>(A, step, n_items, scratch);
+    stage_items<1, Cell>(A, step, n_items, scratch, &sg);
     if (!grid_barrier(A.sync, ++round)) break;
   }
 }
