@@ -112,6 +112,21 @@ int pe_relative_synchronize(pe_relative *h);
 int pe_relative_copy_field(pe_relative *h, float *host_field);
 int pe_relative_copy_arrival(pe_relative *h, float *host_arrival);
 
+/* Asynchronous history output (the reference writes each output frame of
+ * fields.f32 between advances with the solver stopped meanwhile,
+ * native_relative.cpp:111-120).  pe_relative_snapshot packs
+ * the current field into snapshot buffer `slot` (0 or 1; dense, storage
+ * order) on the handle's stream and returns at once; the next advance can
+ * be issued right after.  pe_relative_copy_snapshot copies that snapshot
+ * to host memory on a separate copy stream once it is complete and waits
+ * for the copy; it may run on another host thread while the handle
+ * advances.  A slot is refilled only after its previous copy finished. */
+int pe_relative_snapshot(pe_relative *h, int32_t slot);
+int pe_relative_copy_snapshot(pe_relative *h, int32_t slot, float *host_field);
+/* Page-locked host memory for full-speed copies (cudaHostAlloc). */
+int pe_host_alloc(size_t bytes, void **out);
+int pe_host_free(void *ptr);
+
 /* Device address of the current field: storage order [vP, vE, psi, y, x]
  * with every x row padded to pe_relative_row_pitch() floats (pad = 0);
  * valid until the next step or destroy. */

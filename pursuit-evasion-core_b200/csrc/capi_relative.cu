@@ -27,6 +27,11 @@ struct pe_relative {
   int64_t steps = 0;
   bool initialized = false;
   pe::LaunchTimer timer;  // per-stage launch times (pe_relative_profile)
+  // asynchronous history output: two dense snapshot buffers, filled on the
+  // compute stream and copied out on their own stream
+  float *snap[2] = {nullptr, nullptr};
+  cudaEvent_t snap_ready[2] = {nullptr, nullptr}, snap_free[2] = {nullptr, nullptr};
+  cudaStream_t copy_stream = nullptr;
 };
 
 namespace {
@@ -48,6 +53,13 @@ void release(pe_relative *h) {
   cudaFree(h->csf);
   cudaFree(h->stats);
   if (h->host_stats) cudaFreeHost(h->host_stats);
+  if (h->copy_stream) cudaStreamSynchronize(h->copy_stream);
+  for (int i = 0; i < 2; i++) {
+    cudaFree(h->snap[i]);
+    if (h->snap_ready[i]) cudaEventDestroy(h->snap_ready[i]);
+    if (h->snap_free[i]) cudaEventDestroy(h->snap_free[i]);
+  }
+  if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
   if (h->own) cudaStreamDestroy(h->own);
 }
 
@@ -280,6 +292,53 @@ int pe_relative_synchronize(pe_relative *h) {
   int rc = enter(h);
   if (rc) return rc;
   return read_stats(h);
+}
+
+int pe_relative_snapshot(pe_relative *h, int32_t slot) {
+  int rc = enter(h);
+  if (rc) return rc;
+  if (slot < 0 || slot > 1) return fail(PE_EINVAL, "snapshot slot must be 0 or 1");
+  if (!h->initialized) return fail(PE_ESTATE, "snapshot before init");
+  if (!h->copy_stream) {
+    PE_CUDA_TRY(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
+    for (int i = 0; i < 2; i++) {
+      PE_CUDA_TRY(cudaMalloc(&h->snap[i], sizeof(float) * (size_t)h->g.n));
+      PE_CUDA_TRY(cudaEventCreateWithFlags(&h->snap_ready[i], cudaEventDisableTiming));
+      PE_CUDA_TRY(cudaEventCreateWithFlags(&h->snap_free[i], cudaEventDisableTiming));
+      PE_CUDA_TRY(cudaEventRecord(h->snap_free[i], h->copy_stream));
+    }
+  }
+  // the previous copy out of this slot must be done before it is refilled
+  PE_CUDA_TRY(cudaStreamWaitEvent(h->stream, h->snap_free[slot], 0));
+  PE_CUDA_TRY(pe::rel5_pack(h->g, h->a, h->snap[slot], h->stream));
+  pe::count_launches(1);
+  PE_CUDA_TRY(cudaEventRecord(h->snap_ready[slot], h->stream));
+  return PE_OK;
+}
+
+int pe_relative_copy_snapshot(pe_relative *h, int32_t slot, float *host_field) {
+  int rc = enter(h);
+  if (rc) return rc;
+  if (slot < 0 || slot > 1 || !host_field) return fail(PE_EINVAL, "bad slot or NULL buffer");
+  if (!h->copy_stream) return fail(PE_ESTATE, "no snapshot taken");
+  PE_CUDA_TRY(cudaStreamWaitEvent(h->copy_stream, h->snap_ready[slot], 0));
+  PE_CUDA_TRY(cudaMemcpyAsync(host_field, h->snap[slot], sizeof(float) * (size_t)h->g.n,
+                              cudaMemcpyDeviceToHost, h->copy_stream));
+  PE_CUDA_TRY(cudaEventRecord(h->snap_free[slot], h->copy_stream));
+  PE_CUDA_TRY(cudaStreamSynchronize(h->copy_stream));
+  return PE_OK;
+}
+
+int pe_host_alloc(size_t bytes, void **out) {
+  if (!out) return fail(PE_EINVAL, "out is NULL");
+  *out = nullptr;
+  PE_CUDA_TRY(cudaHostAlloc(out, bytes, cudaHostAllocDefault));
+  return PE_OK;
+}
+
+int pe_host_free(void *ptr) {
+  if (ptr) PE_CUDA_TRY(cudaFreeHost(ptr));
+  return PE_OK;
 }
 
 int pe_relative_copy_field(pe_relative *h, float *host_field) {

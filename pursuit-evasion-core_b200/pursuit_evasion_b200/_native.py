@@ -197,6 +197,10 @@ SIGNATURES = {
     "pe_table_value": (ctypes.c_int, [_P, _DP, ctypes.c_int64, _DP]),
     "pe_table_field": (ctypes.c_int, [_P, _DP, _DP, ctypes.c_int64, _DP]),
     "pe_table_destroy": (ctypes.c_int, [_P]),
+    "pe_relative_snapshot": (ctypes.c_int, [_P, ctypes.c_int32]),
+    "pe_relative_copy_snapshot": (ctypes.c_int, [_P, ctypes.c_int32, _P]),
+    "pe_host_alloc": (ctypes.c_int, [ctypes.c_size_t, ctypes.POINTER(ctypes.c_void_p)]),
+    "pe_host_free": (ctypes.c_int, [_P]),
     "pe_compact_create": (ctypes.c_int, [ctypes.POINTER(VehicleGridArrays),
                                          ctypes.POINTER(VehicleGridArrays),
                                          ctypes.POINTER(PairDomainArrays), ctypes.c_double,

@@ -31,13 +31,15 @@ import json
 import math
 import os
 from pathlib import Path
+import queue
 import shutil
+import threading
 import time
 
 import numpy as np
 
 from .model import config_dict
-from .relative_solver import RelativeSolver
+from .relative_solver import PinnedBuffer, RelativeSolver
 
 SCHEMA = "reversible_relative5d_v1"
 SOURCE_DIR = Path(__file__).resolve().parents[2] / "csrc"
@@ -259,6 +261,61 @@ def solve(
     return meta
 
 
+class _HistoryWriter:
+    """Writes the output frames of fields.f32 while the solver runs on: each
+    frame is snapshotted on the device (two slots), copied to page-locked
+    host memory on a separate stream and written by this thread, in order.
+    The reference stops its solver for every history write
+    (native_relative.cpp:111-120)."""
+
+    def __init__(self, solver, file, count):
+        self.solver, self.file = solver, file
+        self.buffers = [PinnedBuffer(count), PinnedBuffer(count)]
+        self.free = threading.Semaphore(2)
+        self.queue = queue.Queue()
+        self.next_slot = 0
+        self.transfer_seconds = self.write_seconds = 0.0
+        self.error = None
+        self.thread = threading.Thread(target=self._loop, name="history-writer", daemon=True)
+        self.thread.start()
+
+    def submit(self):
+        """Queue the solver's current field as the next frame."""
+        self.free.acquire()  # a slot whose previous frame has been written
+        if self.error is not None:
+            self.free.release()
+            raise self.error
+        slot, self.next_slot = self.next_slot, self.next_slot ^ 1
+        self.solver.snapshot(slot)
+        self.queue.put(slot)
+
+    def _loop(self):
+        while True:
+            slot = self.queue.get()
+            if slot is None:
+                return
+            try:
+                if self.error is None:
+                    t0 = time.perf_counter()
+                    self.solver.copy_snapshot(slot, self.buffers[slot].ptr)
+                    t1 = time.perf_counter()
+                    self.buffers[slot].array.tofile(self.file)
+                    self.transfer_seconds += t1 - t0
+                    self.write_seconds += time.perf_counter() - t1
+            except BaseException as exc:  # reported by submit / close
+                self.error = exc
+            finally:
+                self.free.release()
+
+    def close(self):
+        self.queue.put(None)
+        self.thread.join()
+        for b in self.buffers:
+            b.close()
+        if self.error is not None:
+            raise self.error
+
+
 def _run(solver, output, times, *, history, tol, save_final):
     """Frame loop: advance to each output time, save the frame, log progress."""
     N = solver.cells
@@ -268,17 +325,14 @@ def _run(solver, output, times, *, history, tol, save_final):
     converged_time = None
     kept_times = [float(times[0])]
     history_file = (output / "fields.f32").open("wb") if history else None
+    writer = None
     log = (output / "solver.log").open("w")
     progress = (output / "progress.jsonl").open("w")
     started = time.perf_counter()
     try:
         if history_file:
-            t0 = time.perf_counter()
-            solver.field(host)
-            transfer_seconds += time.perf_counter() - t0
-            t0 = time.perf_counter()
-            host.tofile(history_file)
-            write_seconds += time.perf_counter() - t0
+            writer = _HistoryWriter(solver, history_file, N)
+            writer.submit()  # frame 0: the initial field
         for index, goal in enumerate(times[1:], start=1):
             t0 = time.perf_counter()
             if tol is None:
@@ -289,13 +343,8 @@ def _run(solver, output, times, *, history, tol, save_final):
             update_seconds += time.perf_counter() - t0
             frames += 1
             kept_times.append(float(solver.time if converged_time else goal))
-            if history_file:
-                t0 = time.perf_counter()
-                solver.field(host)
-                transfer_seconds += time.perf_counter() - t0
-                t0 = time.perf_counter()
-                host.tofile(history_file)
-                write_seconds += time.perf_counter() - t0
+            if writer:
+                writer.submit()
             if index % 5 == 0 or index == len(times) - 1 or converged_time:
                 resolved = int(np.isfinite(solver.arrival()).sum())
                 row = dict(time=kept_times[-1], steps=solver.steps,
@@ -309,10 +358,15 @@ def _run(solver, output, times, *, history, tol, save_final):
             if converged_time is not None:
                 break
     finally:
-        if history_file:
-            history_file.close()
-        log.close()
-        progress.close()
+        try:
+            if writer:
+                writer.close()
+                transfer_seconds, write_seconds = writer.transfer_seconds, writer.write_seconds
+        finally:
+            if history_file:
+                history_file.close()
+            log.close()
+            progress.close()
     final_write = 0.0
     if save_final:
         t0 = time.perf_counter()

@@ -157,6 +157,17 @@ class RelativeSolver:
         _native.check(self._lib.pe_relative_copy_arrival(self._h, out.ctypes.data))
         return out.reshape(self.shape)
 
+    def snapshot(self, slot):
+        """Enqueue a copy of the current field into snapshot buffer `slot`
+        (0 or 1) on the solver's stream; returns at once."""
+        _native.check(self._lib.pe_relative_snapshot(self._h, int(slot)))
+
+    def copy_snapshot(self, slot, host_ptr):
+        """Copy snapshot `slot` to host memory once it is complete (on a
+        separate copy stream; callable from another thread while the solver
+        advances)."""
+        _native.check(self._lib.pe_relative_copy_snapshot(self._h, int(slot), host_ptr))
+
     def device_field_ptr(self):
         ptr = ctypes.c_void_p()
         _native.check(self._lib.pe_relative_device_field(self._h, ctypes.byref(ptr)))
@@ -198,3 +209,26 @@ class RelativeSolver:
                                                         ctypes.byref(ms),
                                                         ctypes.byref(n)))
         return ms.value, n.value
+
+
+class PinnedBuffer:
+    """Page-locked host float32 buffer (pe_host_alloc) with a NumPy view."""
+
+    def __init__(self, count):
+        self._lib = _native.library()
+        ptr = ctypes.c_void_p()
+        _native.check(self._lib.pe_host_alloc(ctypes.c_size_t(4 * int(count)), ctypes.byref(ptr)))
+        self.ptr = ptr.value
+        self.array = np.ctypeslib.as_array((ctypes.c_float * int(count)).from_address(self.ptr))
+
+    def close(self):
+        if self.ptr:
+            self.array = None
+            _native.check(self._lib.pe_host_free(ctypes.c_void_p(self.ptr)))
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -191,3 +191,21 @@ def test_full_size_grid_properties():
     change = np.abs(v_fast.astype(np.float64) - before_last).max()
     assert residual == pytest.approx(change, rel=1e-6)
     assert np.all(arrival[v0 <= 0] == 0)
+
+
+def test_history_written_while_solving_equals_synchronous_frames(tmp_path):
+    """fields.f32 from the asynchronous history writer (device snapshots, two
+    slots, a writer thread) holds, in order, exactly the frames a stopped
+    solver copies out synchronously, also when frames queue up."""
+    grid = RelativeGrid(9, 8, 7, 7, 1.0)
+    times = np.round(np.arange(0, 21) * 0.025, 10)
+    meta = solve(A3, grid, tmp_path / "h", horizon=float(times[-1]), output_dt=0.025)
+    assert meta["frames"] == len(times)
+    written = np.fromfile(tmp_path / "h" / "fields.f32", np.float32).reshape(len(times), -1)
+    with RelativeSolver(A3, grid, local_precision="float64") as s:  # solve's default
+        s.initialize()
+        expected = [s.field().ravel().copy()]
+        for goal in times[1:]:
+            s.advance(float(goal))
+            expected.append(s.field().ravel().copy())
+    np.testing.assert_array_equal(written.view(np.uint32), np.array(expected).view(np.uint32))
