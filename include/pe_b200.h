@@ -485,6 +485,48 @@ int pe_table_field(pe_table *h, const double *host_states, const double *host_bu
 int pe_table_destroy(pe_table *h);
 
 /* ------------------------------------------------------------------------
+ * Legacy six-dimensional square game [xP, yP, thP, xE, yE, thE] with
+ * constant speeds and bounded turn rates.
+ *
+ * Replaces the executable src/pursuit_evasion/dp/native_square.cpp (argv
+ * in, fields.f32 out), run by dp/native.py:14-106.  The options are its
+ * argv (native_square.cpp:65-80); init is its target/avoid surfaces
+ * (:110-128), advance its frame loop (:185-198) and the stage its ENO1/ENO2
+ * LF RK1/RK2 update (:145-183), in float32 in the reference's operation
+ * order: fields equal the executable's bit for bit.
+ * ------------------------------------------------------------------------ */
+typedef struct pe_square_params {
+  int32_t positions, headings;     /* --positions, --headings */
+  double extent, arena;            /* --extent (> arena), --arena */
+  double capture_radius;           /* --radius */
+  double p_speed, e_speed;         /* --vp, --ve */
+  double p_turn_rate, e_turn_rate; /* --wp, --we */
+  double cfl;                      /* --cfl, in (0, 1] */
+  int32_t order;                   /* --order, 1 or 2 */
+  int32_t device;                  /* CUDA device ordinal */
+} pe_square_params;
+
+typedef struct pe_square pe_square;
+
+int pe_square_cells(const pe_square_params *params, int64_t *cells);
+/* max_internal_dt of native_square.cpp:94-95 (host only). */
+int pe_square_dt_limit(const pe_square_params *params, double *dt);
+int pe_square_create(const pe_square_params *params, pe_square **out);
+/* max(target, avoid) and arrival (0 where <= 0, else NaN); time 0. */
+int pe_square_init(pe_square *h);
+/* Internal steps of min(dt_limit, goal - t) until t >= goal - 1e-10. */
+int pe_square_advance(pe_square *h, double goal, int64_t *steps_taken);
+int pe_square_time(const pe_square *h, double *t, int64_t *steps);
+int pe_square_synchronize(pe_square *h);
+int pe_square_copy_field(pe_square *h, float *host_field);
+int pe_square_copy_arrival(pe_square *h, float *host_arrival);
+/* Sup-norm change of the last step (synchronises). */
+int pe_square_residual(pe_square *h, double *residual);
+int pe_square_profile(pe_square *h, int32_t enable);
+int pe_square_kernel_time(pe_square *h, double *total_ms, int64_t *launches);
+int pe_square_destroy(pe_square *h);
+
+/* ------------------------------------------------------------------------
  * Compact eight-state semi-Lagrangian contact game (local pair game).
  *
  * Replaces the CuPy RawKernels and host loops of

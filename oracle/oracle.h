@@ -33,6 +33,22 @@ int po_rel_solve_f32(const po_rel_cfg *c, double horizon, double output_dt,
 int po_rel_solve_f64(const po_rel_cfg *c, double horizon, double output_dt,
                      double *final, long *steps_out);
 
+/* Legacy 6D square game: storage [xP, yP, thP, xE, yE, thE], thE fastest;
+ * constant speeds vp, ve and turn-rate bounds wp, we. */
+typedef struct {
+  int n, nh, order;
+  float extent, arena, radius, vp, ve, wp, we;
+  double cfl;
+} po_s6_cfg;
+
+size_t po_s6_cells(const po_s6_cfg *c);
+double po_s6_dt_limit(const po_s6_cfg *c);
+/* max(target, avoid) and arrival = 0 where <= 0, NaN elsewhere. */
+void po_s6_init(const po_s6_cfg *c, float *a, float *arrival);
+/* One stage; base != NULL: the RK2 average, tube minimum and avoid floor. */
+int po_s6_stage(const po_s6_cfg *c, const float *src, float *dst, const float *base,
+                float *arrival, float dt, double tau);
+
 /* Dense 8D game: storage [xP, yP, thP, vP, xE, yE, thE, vE], vE fastest. */
 typedef struct {
   int n, nh, np, ne, order;

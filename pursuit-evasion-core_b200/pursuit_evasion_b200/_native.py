@@ -134,6 +134,24 @@ class PairDomainArrays(ctypes.Structure):
     ]
 
 
+class SquareParams(ctypes.Structure):
+    """pe_square_params: the options of native_square.cpp."""
+    _fields_ = [
+        ("positions", ctypes.c_int32),
+        ("headings", ctypes.c_int32),
+        ("extent", ctypes.c_double),
+        ("arena", ctypes.c_double),
+        ("capture_radius", ctypes.c_double),
+        ("p_speed", ctypes.c_double),
+        ("e_speed", ctypes.c_double),
+        ("p_turn_rate", ctypes.c_double),
+        ("e_turn_rate", ctypes.c_double),
+        ("cfl", ctypes.c_double),
+        ("order", ctypes.c_int32),
+        ("device", ctypes.c_int32),
+    ]
+
+
 PE_SL_KERNEL_AUTO, PE_SL_KERNEL_GENERIC, PE_SL_KERNEL_TILED = 0, 1, 2
 PE_SL_TUBE = 0
 PE_SL_MINTIME = 1
@@ -201,6 +219,20 @@ SIGNATURES = {
     "pe_relative_copy_snapshot": (ctypes.c_int, [_P, ctypes.c_int32, _P]),
     "pe_host_alloc": (ctypes.c_int, [ctypes.c_size_t, ctypes.POINTER(ctypes.c_void_p)]),
     "pe_host_free": (ctypes.c_int, [_P]),
+    "pe_square_cells": (ctypes.c_int, [ctypes.POINTER(SquareParams), _I64P]),
+    "pe_square_dt_limit": (ctypes.c_int, [ctypes.POINTER(SquareParams), _DP]),
+    "pe_square_create": (ctypes.c_int, [ctypes.POINTER(SquareParams),
+                                        ctypes.POINTER(ctypes.c_void_p)]),
+    "pe_square_init": (ctypes.c_int, [_P]),
+    "pe_square_advance": (ctypes.c_int, [_P, ctypes.c_double, _I64P]),
+    "pe_square_time": (ctypes.c_int, [_P, _DP, _I64P]),
+    "pe_square_synchronize": (ctypes.c_int, [_P]),
+    "pe_square_copy_field": (ctypes.c_int, [_P, _P]),
+    "pe_square_copy_arrival": (ctypes.c_int, [_P, _P]),
+    "pe_square_residual": (ctypes.c_int, [_P, _DP]),
+    "pe_square_profile": (ctypes.c_int, [_P, ctypes.c_int32]),
+    "pe_square_kernel_time": (ctypes.c_int, [_P, _DP, _I64P]),
+    "pe_square_destroy": (ctypes.c_int, [_P]),
     "pe_compact_create": (ctypes.c_int, [ctypes.POINTER(VehicleGridArrays),
                                          ctypes.POINTER(VehicleGridArrays),
                                          ctypes.POINTER(PairDomainArrays), ctypes.c_double,

@@ -56,3 +56,9 @@ def world_goldens():
 
 def bits(a):
     return np.ascontiguousarray(a, dtype=np.float32).view(np.uint32)
+
+
+def square_goldens():
+    """Golden vectors of the legacy 6D square game (tests/golden/square6d_*.npz,
+    made by the reference executable native_square.cpp)."""
+    return {p.stem[len("square6d_"):]: p for p in sorted(GOLDEN.glob("square6d_*.npz"))}

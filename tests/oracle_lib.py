@@ -40,6 +40,12 @@ class W8Cfg(ctypes.Structure):
     ] + [("cfl", ctypes.c_double)]
 
 
+class S6Cfg(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int) for n in ("n", "nh", "order")] + [
+        (n, ctypes.c_float) for n in ("extent", "arena", "radius", "vp", "ve", "wp", "we")
+    ] + [("cfl", ctypes.c_double)]
+
+
 class SLCfg(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int) for n in ("nx", "nh", "nvp", "nve", "mode")] + [
         (n, ctypes.c_double)
@@ -79,6 +85,11 @@ class Oracle:
             "po_rect_separation": (ctypes.c_double, [ctypes.c_double] * 10),
             "po_w8_init_contact": (None, [_P] + [ctypes.c_double] * 4 + [_P, _P]),
             "po_w8_stage_f64": (ctypes.c_int, [_P, _P, _P, _P, ctypes.c_double]),
+            "po_s6_cells": (ctypes.c_size_t, [_P]),
+            "po_s6_dt_limit": (ctypes.c_double, [_P]),
+            "po_s6_init": (None, [_P, _P, _P]),
+            "po_s6_stage": (ctypes.c_int, [_P, _P, _P, _P, _P, ctypes.c_float,
+                                           ctypes.c_double]),
             "po_w8_stage": (ctypes.c_int, [_P, _P, _P, _P, _P, ctypes.c_float,
                                            ctypes.c_double]),
             "po_sl_integrated_speed": (None, [ctypes.c_double] * 5 + [_P, _P]),
@@ -177,6 +188,46 @@ class Oracle:
                                         dst.ctypes.data,
                                         None if base is None else base.ctypes.data,
                                         dt)
+
+    # -- legacy 6D square game ---------------------------------------------
+    @staticmethod
+    def s6_cfg(options):
+        """S6Cfg from the reference executable's options (its defaults for the
+        missing ones, native_square.cpp:65-80)."""
+        o = dict(extent=3.5, arena=3.0, radius=0.3, vp=1.0, ve=0.3, wp=1.0, we=2.0,
+                 order=2, cfl=0.8)
+        o.update(options)
+        return S6Cfg(int(o["positions"]), int(o["headings"]), int(o["order"]),
+                     o["extent"], o["arena"], o["radius"], o["vp"], o["ve"], o["wp"],
+                     o["we"], o["cfl"])
+
+    def s6_solve(self, cfg, horizon, output_dt):
+        """The executable's frame loop (native_square.cpp:185-202): frames,
+        final arrival and the number of internal steps."""
+        n = self.lib.po_s6_cells(ctypes.addressof(cfg))
+        a, b = np.zeros(n, np.float32), np.zeros(n, np.float32)
+        arrival = np.zeros(n, np.float32)
+        self.lib.po_s6_init(ctypes.addressof(cfg), a.ctypes.data, arrival.ctypes.data)
+        frames = [a.copy()]
+        maxdt = self.lib.po_s6_dt_limit(ctypes.addressof(cfg))
+        tau, steps = 0.0, 0
+        for frame in range(1, int(np.ceil(horizon / output_dt - 1e-10)) + 1):
+            goal = min(horizon, frame * output_dt)
+            while tau < goal - 1e-10:
+                dt = np.float32(min(maxdt, goal - tau))
+                if cfg.order == 1:
+                    self.lib.po_s6_stage(ctypes.addressof(cfg), a.ctypes.data, b.ctypes.data,
+                                         None, arrival.ctypes.data, dt, tau)
+                    a, b = b, a
+                else:
+                    self.lib.po_s6_stage(ctypes.addressof(cfg), a.ctypes.data, b.ctypes.data,
+                                         None, arrival.ctypes.data, dt, tau)
+                    self.lib.po_s6_stage(ctypes.addressof(cfg), b.ctypes.data, a.ctypes.data,
+                                         a.ctypes.data, arrival.ctypes.data, dt, tau)
+                tau += min(maxdt, goal - tau)
+                steps += 1
+            frames.append(a.copy())
+        return np.array(frames), arrival, steps
 
     # -- semi-Lagrangian 5D -----------------------------------------------
     @staticmethod

@@ -153,3 +153,26 @@ def test_world_fp64_stage_tracks_the_float_stage(oracle):
     assert 0 < err.mean() < 5e-6
     assert np.mean(err > 2e-5 + 2e-6 * np.abs(f64)) < 1e-2
     assert err.max() < 1e-2
+
+
+SQUARE = __import__("tests.helpers", fromlist=["square_goldens"]).square_goldens()
+
+
+@pytest.mark.parametrize("name", sorted(SQUARE))
+def test_square_oracle_reproduces_reference_golden_bitwise(oracle, name):
+    """The 6D square-game restatement (oracle/square6d.c) equals the
+    reference executable native_square.cpp bit for bit: every frame, the
+    arrival times and the step count."""
+    import json
+
+    z = np.load(SQUARE[name])
+    options = json.loads(str(z["options"]))
+    cfg = oracle.s6_cfg(options)
+    # native_timing.json prints the bound with 12 significant digits
+    assert oracle.lib.po_s6_dt_limit(ctypes.addressof(cfg)) == pytest.approx(
+        float(z["max_internal_dt"]), rel=1e-11)
+    frames, arrival, steps = oracle.s6_solve(cfg, options["horizon"], options["output-dt"])
+    assert steps == int(z["internal_steps"])
+    np.testing.assert_array_equal(bits(frames.reshape(z["fields"].shape)), bits(z["fields"]))
+    np.testing.assert_array_equal(bits(arrival), bits(z["arrival"]))
+    np.testing.assert_array_equal(bits(frames[-1]), bits(z["final"]))
