@@ -554,6 +554,59 @@ def compact_section(backups=5, with_cpu=True):
     return out
 
 
+def square6d_section(horizon=2.0, with_cpu=True):
+    """The legacy 6D square game on the reference's default grid (17
+    positions, 16 headings: 21,381,376 cells), default GameConfig, order 2,
+    CFL 0.8, `horizon` seconds: device time of the reference-order stage
+    (bit-identical to native_square.cpp), with the reference executable
+    itself (oracle/_ref/square6d, all host threads, 0.2 s) beside it."""
+    import subprocess
+    import tempfile
+    from pursuit_evasion_b200.dp.grid import GridSpec
+    from pursuit_evasion_b200.dp.native import SquareSolver
+    from pursuit_evasion_b200.model import GameConfig
+
+    grid = GridSpec(17, 16, 3.5)
+    with SquareSolver(GameConfig(), grid) as s:
+        s.initialize()
+        s.advance(0.1)  # warm-up
+        s.synchronize()
+        s.initialize()
+        s.profile(True)
+        t0 = time.perf_counter()
+        s.advance(horizon)
+        s.synchronize()
+        wall = time.perf_counter() - t0
+        kms, launches = s.kernel_time()
+        steps = s.steps
+        s.profile(False)
+    cells = grid.states
+    peak, _ = measured_peaks()
+    algorithmic = (8 + 12) * cells * steps
+    out = {"workload": f"square6d GridSpec(17,16,3.5) default GameConfig, order 2, CFL 0.8, "
+                       f"{horizon} s = {steps} RK2 steps, float32 reference order",
+           "cells": cells, "value": cells * launches / (kms / 1e3), "unit": METRIC,
+           "ms_per_rk2_step": kms / steps, "wall_seconds": wall,
+           "roofline": {"bound": "hbm", "achieved": algorithmic / (kms / 1e3) / 1e9,
+                        "peak": peak, "unit": "GB/s",
+                        "frac": algorithmic / (kms / 1e3) / 1e9 / peak}}
+    exe = REPO / "oracle" / "_ref" / "square6d"
+    if with_cpu and exe.exists():
+        threads = os.cpu_count() or 1
+        with tempfile.TemporaryDirectory() as tmp:
+            subprocess.run([str(exe), "--horizon", "0.2", "--output-dt", "0.1", "--threads",
+                            str(threads), "--history", "0", "--output", tmp + "/o"],
+                           check=True, capture_output=True)
+            timing = json.loads(Path(tmp + "/o/native_timing.json").read_text())
+        value = cells * timing["internal_steps"] * 2 / timing["update_seconds"]
+        out["cpu_baseline"] = {
+            "value": value, "unit": METRIC, "cores": threads, "kind": "reference",
+            "sample": f"native_square.cpp built from the reference sources, same grid, 0.2 s = "
+                      f"{timing['internal_steps']} RK2 steps, update loop "
+                      f"{timing['update_seconds']:.2f} s on {threads} threads"}
+    return out
+
+
 def run_case(name, repeats):
     """A short, fixed launch sequence of one kernel for profilers (ncu):
     no timing, no JSON line.  One warm-up launch then `repeats` launches of
@@ -587,6 +640,32 @@ def run_case(name, repeats):
             s.init_contact((0.5, 0.3), (0.5, 0.3))
             for _ in range(1 + repeats):
                 s.step(s.dt_limit)
+            s.synchronize()
+    elif name == "compact8d":
+        from pursuit_evasion_b200.local_game.geometry import CircleArena
+        from pursuit_evasion_b200.local_game.grid_game import (
+            PairDomain, backup_packed, initialize_packed, packed_gpu_arrays)
+
+        p = synthetic_vehicle_grid(config.pursuer, half_width=3.25, step=0.5, headings=16,
+                                   speeds=7)
+        e = synthetic_vehicle_grid(config.evader, half_width=3.25, step=0.5, headings=16,
+                                   speeds=7)
+        domain = PairDomain.build(p, e, 2.0)
+        a = packed_gpu_arrays(p, e, domain, max_gb=60)
+        initialize_packed(a, p, e, domain, CircleArena([], 3.25))
+        for _ in range(1 + repeats):
+            backup_packed(a, p, e, domain)
+        a.synchronize()
+        a.close()
+    elif name == "square6d":
+        from pursuit_evasion_b200.dp.grid import GridSpec
+        from pursuit_evasion_b200.dp.native import SquareSolver
+        from pursuit_evasion_b200.model import GameConfig
+
+        with SquareSolver(GameConfig(), GridSpec(17, 16, 3.5)) as s:
+            s.initialize()
+            for _ in range(1 + repeats):
+                s.advance(s.time + s.dt_limit)
             s.synchronize()
     elif name == "mlp":
         from pursuit_evasion_b200.learned.mlp import ValueMLP
@@ -745,6 +824,8 @@ def run_ours(args, world, rank, local):
                             ("semilag5d", lambda: semilag_section(not args.no_cpu_baseline)),
                             ("batch", batch_section),
                             ("compact8d", lambda: compact_section(
+                                with_cpu=not args.no_cpu_baseline)),
+                            ("square6d", lambda: square6d_section(
                                 with_cpu=not args.no_cpu_baseline))):
                 try:
                     line[key] = fn()
@@ -779,7 +860,8 @@ def main():
     parser.add_argument("--samples", type=int, default=1 << 22)
     parser.add_argument("--epochs", type=int, default=20)
     parser.add_argument("--case", choices=["relative5d", "semilag5d", "semilag5d-generic",
-                                           "world8d", "world8d-fast", "mlp"],
+                                           "world8d", "world8d-fast", "mlp", "compact8d",
+                                           "square6d"],
                         help="run a short launch sequence of one kernel for a profiler")
     parser.add_argument("--repeats", type=int, default=2)
     args = parser.parse_args()

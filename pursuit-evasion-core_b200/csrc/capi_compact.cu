@@ -18,6 +18,7 @@
 // value so far drops the action) is kept, so the values equal the
 // reference's.  Rows longer than the shared-memory budget go to a
 // per-CTA scratch row in global memory (L2-resident).
+#include <algorithm>
 #include <cmath>
 #include <map>
 #include <utility>
@@ -238,6 +239,157 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
+// Backup with every pursuer action at once (up to kMaxActions actions,
+// evader state ids below 2^16): for a pursuer state the CTA builds the
+// interpolated rows of all its allowed actions over the evader states within
+// reach, G[u][t] for reach entry t, plus a map from evader state to t; each
+// thread then walks the replies of its cells once, loading every evader
+// stencil a single time and applying it to all actions still alive.  An
+// action drops out once its running reply maximum reaches the cell's
+// current value (it cannot lower the minimum), so the value equals the
+// reference's action-by-action loop with its early exit.
+constexpr int kMaxActions = 9;
+
+template <bool PACKED>
+__global__ void __launch_bounds__(kThreads)
+    backup_all_kernel(const CompactDev d, const float *__restrict__ cur,
+                      float *__restrict__ out, int rcap, int group) {
+  extern __shared__ __align__(16) float smem[];
+  float *G = smem;                                                      // [group][rcap]
+  unsigned short *lmap = reinterpret_cast<unsigned short *>(G + group * rcap);  // [ne]
+  __shared__ long long s_row[kMaxActions][kStencil], s_off[kMaxActions][kStencil];
+  __shared__ float s_w[kMaxActions][kStencil];
+  __shared__ unsigned s_allowed;
+  const int tid = threadIdx.x;
+  const float r2 = d.exit_value * d.exit_value;
+
+  for (int ip = blockIdx.x; ip < d.np; ip += gridDim.x) {
+    int count, pos = 0;
+    long long base;
+    if (PACKED) {
+      pos = d.p_position[ip];
+      count = d.counts[pos];
+      base = d.offsets[ip];
+    } else {
+      count = d.ne;
+      base = (long long)ip * d.ne;
+    }
+    const int *cell_e = PACKED ? d.e_indices + (long long)pos * d.max_count : nullptr;
+    const float4 pp = d.p_pose[ip];
+    const int cls = d.p_class[ip];
+    const long long r_begin = d.reach_start[cls];
+    const int r_n = (int)(d.reach_start[cls + 1] - r_begin);
+    if (tid < d.npa * kStencil) {
+      const int u = tid / kStencil, k = tid % kStencil;
+      const long long s = ((long long)ip * d.npa + u) * kStencil + k;
+      const bool allowed = d.p_allowed[(long long)ip * d.npa + u] != 0;
+      const int nxt = d.p_ids[s];
+      const float w = allowed ? d.p_w[s] : 0.f;
+      s_w[u][k] = w;
+      if (PACKED) {
+        s_row[u][k] = w > 0.f ? (long long)d.p_position[nxt] * d.ne : 0;
+        s_off[u][k] = w > 0.f ? d.offsets[nxt] : 0;
+      } else {
+        s_off[u][k] = w > 0.f ? (long long)nxt * d.ne : 0;
+      }
+    }
+    if (tid == 0) {
+      unsigned m = 0;
+      for (int u = 0; u < d.npa; u++) m |= d.p_allowed[(long long)ip * d.npa + u] ? 1u << u : 0u;
+      s_allowed = m;
+    }
+    __syncthreads();
+    const unsigned allowed_u = s_allowed;
+    for (int t = tid; t < r_n; t += kThreads)
+      lmap[__ldg(d.reach_index + r_begin + t)] = (unsigned short)t;
+    bool first = true;  // no group has written this pursuer state's cells yet
+    for (int u0 = 0; u0 < d.npa; u0 += group) {
+      const unsigned in_group = allowed_u & (((1u << group) - 1u) << u0);
+      if (!in_group) continue;  // the same for the whole CTA
+      // rows of the group's allowed actions over the reach list
+      for (int t = tid; t < r_n; t += kThreads) {
+        const int ie = __ldg(d.reach_index + r_begin + t);
+        for (int u = u0; u < u0 + group && u < d.npa; u++) {
+          if (!((in_group >> u) & 1u)) continue;
+          float v = 0.f;
+#pragma unroll
+          for (int k = 0; k < kStencil; k++)
+            if (s_w[u][k] > 0.f) {
+              float x;
+              if (PACKED) {
+                const int rank = __ldg(d.lookup + s_row[u][k] + ie);
+                x = rank < 0 ? d.exit_value : __ldg(cur + s_off[u][k] + rank);
+              } else {
+                x = __ldg(cur + s_off[u][k] + ie);
+              }
+              v = fmaf(s_w[u][k], x, v);
+            }
+          G[(u - u0) * rcap + t] = v;
+        }
+      }
+      __syncthreads();
+      for (int k = tid; k < count; k += kThreads) {
+        const int ie = PACKED ? cell_e[k] : k;
+        // the running minimum: the current value before the first group
+        const float best = first ? cur[base + k] : out[base + k];
+        if (!PACKED) {
+          const float4 ep = d.e_pose[ie];
+          const float dx = pp.x - ep.x, dy = pp.y - ep.y;
+          if (dx * dx + dy * dy > r2) {  // outside the local game
+            out[base + k] = best;
+            continue;
+          }
+        }
+        float worst[kMaxActions];
+#pragma unroll
+        for (int u = 0; u < kMaxActions; u++) worst[u] = -1e30f;
+        unsigned alive = in_group >> u0;  // bit g: action u0 + g
+        const uint8_t *allowed_e = d.e_allowed + (long long)ie * d.nea;
+        for (int a = 0; a < d.nea && alive; a++) {
+          if (!__ldg(allowed_e + a)) continue;
+          const long long s = ((long long)ie * d.nea + a) * kStencil;
+          int t[kStencil];
+          float w[kStencil];
+#pragma unroll
+          for (int q = 0; q < kStencil / 4; q++) {
+            const int4 i4 = __ldg(reinterpret_cast<const int4 *>(d.e_ids + s) + q);
+            const float4 w4 = __ldg(reinterpret_cast<const float4 *>(d.e_w + s) + q);
+            w[4 * q] = w4.x;
+            w[4 * q + 1] = w4.y;
+            w[4 * q + 2] = w4.z;
+            w[4 * q + 3] = w4.w;
+            t[4 * q] = w4.x > 0.f ? lmap[i4.x] : 0;
+            t[4 * q + 1] = w4.y > 0.f ? lmap[i4.y] : 0;
+            t[4 * q + 2] = w4.z > 0.f ? lmap[i4.z] : 0;
+            t[4 * q + 3] = w4.w > 0.f ? lmap[i4.w] : 0;
+          }
+#pragma unroll
+          for (int g = 0; g < kMaxActions; g++) {
+            if (!((alive >> g) & 1u)) continue;
+            const float *row = G + g * rcap;
+            float value = 0.f;
+#pragma unroll
+            for (int q = 0; q < kStencil; q++)
+              if (w[q] > 0.f) value = fmaf(w[q], row[t[q]], value);
+            worst[g] = fmaxf(worst[g], value);
+            if (worst[g] >= best) alive &= ~(1u << g);
+          }
+        }
+        float result = best;
+#pragma unroll
+        for (int g = 0; g < kMaxActions; g++)
+          if ((alive >> g) & 1u) result = fminf(result, worst[g]);
+        out[base + k] = result;
+      }
+      __syncthreads();  // the rows are rebuilt for the next group
+      first = false;
+    }
+    if (!allowed_u)  // no allowed action: every cell keeps its value
+      for (int k = tid; k < count; k += kThreads) out[base + k] = cur[base + k];
+    __syncthreads();  // the map is rebuilt for the next pursuer state
+  }
+}
+
 template <bool PACKED>
 __global__ void query_kernel(CompactDev d, const float *__restrict__ f, int n,
                              const int *__restrict__ pi, const float *__restrict__ pw,
@@ -285,6 +437,9 @@ struct pe_compact {
   int grid = 0;
   size_t smem = 0;
   bool smem_row = true;
+  bool all_actions = false;  // backup_all_kernel applies
+  int rcap = 0;              // longest reach list
+  int group = 0;             // pursuer actions per pass of backup_all_kernel
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   bool initialized = false;
@@ -423,9 +578,38 @@ int upload_grid(pe_compact *h, const pe_vehicle_grid *g, const float4 **pose,
   return own(h, g->allowed, rows, allowed);
 }
 
-int configure_launch(pe_compact *h) {
+int configure_launch(pe_compact *h, int rcap) {
   int sms = 0;
   PE_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
+  int max_smem = 0;
+  PE_CUDA_TRY(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin,
+                                     h->device));
+  // groups of actions at once: rows of `group` actions over the longest
+  // reach list and a 16-bit map of the evader states
+  const size_t map_bytes = sizeof(unsigned short) * (size_t)h->d.ne + 16;
+  const int64_t fit = rcap > 0 ? ((int64_t)max_smem - 4096 - (int64_t)map_bytes) /
+                                     ((int64_t)sizeof(float) * rcap)
+                               : 0;
+  const int group = (int)std::min<int64_t>(std::min(h->d.npa, pe::kMaxActions), fit);
+  const size_t all_smem = sizeof(float) * (size_t)std::max(group, 1) * rcap + map_bytes;
+  if (h->d.npa <= pe::kMaxActions && h->d.ne <= 65536 && group >= 2) {
+    const void *kernel = h->packed ? (const void *)pe::backup_all_kernel<true>
+                                   : (const void *)pe::backup_all_kernel<false>;
+    PE_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)all_smem));
+    int resident = 0;
+    PE_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, kernel, pe::kThreads,
+                                                              all_smem));
+    if (resident >= 1) {
+      h->all_actions = true;
+      h->rcap = rcap;
+      h->group = group;
+      h->smem = all_smem;
+      const int64_t slots = (int64_t)sms * resident;
+      h->grid = (int)(h->d.np < slots ? h->d.np : slots);
+      return PE_OK;
+    }
+  }
   const size_t row = (size_t)h->d.ne * sizeof(float);
   h->smem_row = row <= (size_t)pe::kMaxRowBytes;
   h->smem = h->smem_row ? row : 0;
@@ -473,6 +657,7 @@ int pe_compact_create(const pe_vehicle_grid *p, const pe_vehicle_grid *e,
   h->device = device;
   h->packed = domain != nullptr;
   pe::CompactDev &d = h->d;
+  int rcap = 0;
   d.np = p->states;
   d.ne = e->states;
   d.npa = p->actions;
@@ -485,6 +670,8 @@ int pe_compact_create(const pe_vehicle_grid *p, const pe_vehicle_grid *e,
     std::vector<int> p_class, index;
     std::vector<long long> start;
     reach_lists(p, e, d.reach, &p_class, &index, &start);
+    for (size_t c = 0; c + 1 < start.size(); c++)
+      rcap = std::max(rcap, (int)(start[c + 1] - start[c]));
     rc = own(h, p_class.data(), p_class.size(), &d.p_class);
     if (!rc) rc = own(h, index.data(), index.size(), &d.reach_index);
     if (!rc) rc = own(h, start.data(), start.size(), &d.reach_start);
@@ -509,7 +696,7 @@ int pe_compact_create(const pe_vehicle_grid *p, const pe_vehicle_grid *e,
         err1 == cudaSuccess ? cudaMalloc(&h->next, (size_t)h->cells * sizeof(float)) : err1;
     if (err2 != cudaSuccess) rc = pe::cuda_fail(err2, "compact field");
   }
-  if (!rc) rc = configure_launch(h);
+  if (!rc) rc = configure_launch(h, rcap);
   if (!rc) {
     const cudaError_t err = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
     if (err != cudaSuccess) rc = pe::cuda_fail(err, "cudaStreamCreate");
@@ -572,7 +759,14 @@ int pe_compact_backup(pe_compact *h, int32_t count) {
   PE_CUDA_TRY(cudaSetDevice(h->device));
   for (int32_t i = 0; i < count && h->cells > 0; i++) {
     cudaEvent_t t0 = h->timer.begin(h->stream);
-    if (h->packed) {
+    if (h->all_actions) {
+      if (h->packed)
+        pe::backup_all_kernel<true><<<h->grid, pe::kThreads, h->smem, h->stream>>>(
+            h->d, h->field, h->next, h->rcap, h->group);
+      else
+        pe::backup_all_kernel<false><<<h->grid, pe::kThreads, h->smem, h->stream>>>(
+            h->d, h->field, h->next, h->rcap, h->group);
+    } else if (h->packed) {
       if (h->smem_row)
         pe::backup_kernel<true, true><<<h->grid, pe::kThreads, h->smem, h->stream>>>(
             h->d, h->field, h->next, h->scratch);

@@ -173,3 +173,27 @@ def test_memory_guard_raises_before_allocating():
     p, e, _ = grids(z)
     with pytest.raises(MemoryError):
         gpu_arrays(vehicle(p), vehicle(e), max_gb=1e-9)
+
+
+def test_grouped_actions_carry_the_running_minimum():
+    """A reach list of 20,000 evader states leaves shared memory for only a
+    few pursuer actions per pass; with the first actions disallowed for some
+    states, later passes start from the minimum of earlier ones (or from the
+    current value when no earlier pass ran)."""
+    cg = load_oracle()
+    rng = np.random.default_rng(21)
+    p = random_grid(5, 9, rng, spread=0.3, local=2)
+    e = random_grid(20_000, 4, rng, spread=0.3, local=300)
+    p["allowed"][:3, :4] = False
+    p["allowed"][:3, 8] = True
+    radius = 1.0
+    P, E = vehicle(p), vehicle(e)
+    a = gpu_arrays(P, E)
+    initialize_gpu(a, P, E, ARENA, exit_radius=radius)
+    field = a["current"].get().reshape(5, 20_000).astype(np.float64)
+    for _ in range(2):
+        expected = cg.backup_dense(field, p, e, radius)
+        backup_gpu(a, P, E)
+        field = a["current"].get().reshape(5, 20_000).astype(np.float64)
+        np.testing.assert_allclose(field, expected, atol=1e-6)
+    a.close()
