@@ -35,6 +35,9 @@ namespace {
 constexpr int OWN_SLOTS = 6;
 constexpr int NB_SLOTS = 2;
 constexpr int NEIGHBOURS = 8;  // vE-2, vE-1, vE+1, vE+2, vP-2, vP-1, vP+1, vP+2
+// a neighbour set also holds, on RK2 stage 2, the item's rows of the
+// stage's old value V (the blend partner), prefetched with the neighbours
+constexpr int NB_PLANES = NEIGHBOURS + 1;
 constexpr int MAX_THREADS = 512;
 constexpr int TARGET_THREADS = 256;  // launch bound: two CTAs of 256 per SM
 constexpr unsigned WAIT_LIMIT = 1u << 22;
@@ -226,7 +229,7 @@ __host__ __device__ inline SmemLayout smem_layout(int rows, int xp, int headings
   L.nb_floats = rows * xp;
   L.own_off = 0;
   L.nb_off = OWN_SLOTS * L.own_floats;
-  L.bar_off = 4 * (L.nb_off + NB_SLOTS * NEIGHBOURS * L.nb_floats);
+  L.bar_off = 4 * (L.nb_off + NB_SLOTS * NB_PLANES * L.nb_floats);
   L.red_off = L.bar_off + 8 * 2 * (OWN_SLOTS + NB_SLOTS);
   L.trig_off = L.red_off + 4 * (MAX_THREADS / 32);
   L.bytes = L.trig_off + 4 * 2 * headings;
@@ -349,13 +352,20 @@ __global__ void __launch_bounds__(TARGET_THREADS, 2)
           if (use > 0) alive &= wait_phase(&nb_empty[slot], (uint32_t)((use - 1) & 1), timeout);
           if (!alive) return;
           fence_async_shared();
-          mbar_expect_tx(&nb_full[slot], nb_bytes * nb_count);
+          mbar_expect_tx(&nb_full[slot], nb_bytes * (nb_count + (BLEND ? 1 : 0)));
           for (int q = 0; q < NEIGHBOURS; q++)
             if (nb_e[q] >= 0)
-              bulk_load(nbr + (slot * NEIGHBOURS + q) * L.nb_floats,
+              bulk_load(nbr + (slot * NB_PLANES + q) * L.nb_floats,
                         a.s.src + plane_index(nb_v[q], nb_e[q], it.p0 + k) * PP +
                             (int64_t)it.y0 * XP,
                         nb_bytes, &nb_full[slot]);
+          // the blend partner V of this step's rows: read here before any
+          // consumer writes them (they wait for this set first)
+          if (BLEND)
+            bulk_load(nbr + (slot * NB_PLANES + NEIGHBOURS) * L.nb_floats,
+                      a.s.dst + plane_index(it.iv, it.ie, it.p0 + k) * PP +
+                          (int64_t)it.y0 * XP,
+                      nb_bytes, &nb_full[slot]);
           ng++;
         };
         for (int d = -2; d <= 1 && alive; d++) issue_own(d);
@@ -443,7 +453,7 @@ __global__ void __launch_bounds__(TARGET_THREADS, 2)
 
         if (active && alive) {
           const float *o0 = own + cslot * L.own_floats + ctr;
-          const float *nb = nbr + ns * NEIGHBOURS * L.nb_floats + nbo;
+          const float *nb = nbr + ns * NB_PLANES * L.nb_floats + nbo;
           const float4 C = win[2];
           const float2 v_a = lo2(C), v_b = hi2(C);
 
@@ -513,7 +523,8 @@ __global__ void __launch_bounds__(TARGET_THREADS, 2)
           const float2 bx2 = f2(bx), by2 = f2(by);
           const float ax_coef = fmaf(fabsf(bx), a.ihx, wy);  // alpha_x / h
           const float aby = fabsf(by) * a.ihx;
-          const float4 prev4 = BLEND ? *reinterpret_cast<const float4 *>(gdst) : C;
+          const float4 prev4 =
+              BLEND ? *reinterpret_cast<const float4 *>(nb + NEIGHBOURS * L.nb_floats) : C;
 
           float2 out[2];
 #pragma unroll
