@@ -48,6 +48,7 @@ struct pe_batch {
   cudaGraphExec_t graph = nullptr;
   cudaStream_t graph_stream = nullptr;
   int grid = 0;
+  size_t tiled_smem = 0;  // dynamic shared memory of the tiled float32 kernel
   bool initialized = false;
   pe::LaunchTimer timer;
 };
@@ -87,6 +88,7 @@ int check_solve(const pe_batch *h, int32_t solve) {
 int upload_descriptors(pe_batch *h) {
   std::vector<pe::Rel5BatchSolve> d(h->count);
   int64_t base = 0;
+  size_t smem = 0;
   for (int pos = 0; pos < h->count; pos++) {
     const int i = h->order[pos];
     const pe::Rel5Grid &g = h->grids[i];
@@ -100,10 +102,29 @@ int upload_descriptors(pe_batch *h) {
     s.steps = h->step_table + h->step_off[i];
     s.stats = h->stats + i;
     s.nsteps = (int)h->steps[i].size();
-    s.rows = h->rows[i];
-    s.items = (int64_t)g.nvp * g.nve * g.nh * ((g.nx + s.rows - 1) / s.rows);
+    if (h->exact) {
+      // item: `rows` y rows of one (vP, vE, psi) plane
+      s.rows = h->rows[i];
+      s.items = (int64_t)g.nvp * g.nve * g.nh * ((g.nx + s.rows - 1) / s.rows);
+    } else {
+      // item: `rows` y rows of one (vP, vE) plane stack, all headings
+      s.rows = pe::rel5_batch_tiled_rows(g.nx, g.xp, h->rows[i]);
+      s.items = (int64_t)g.nvp * g.nve * ((g.nx + s.rows - 1) / s.rows);
+      smem = std::max(smem, pe::rel5_batch_tiled_smem(s.rows, g.xp));
+    }
     s.item_base = base;
     base += s.items;
+  }
+  if (!h->exact && smem != h->tiled_smem) {
+    // a different launch shape: size the cooperative grid again and record
+    // a new graph at the next run
+    h->tiled_smem = smem;
+    h->grid = pe::rel5_batch_grid_tiled(smem);
+    if (h->grid <= 0) return fail(PE_EINVAL, "batch tiles do not fit the tiled kernel");
+    if (h->graph) {
+      cudaGraphExecDestroy(h->graph);
+      h->graph = nullptr;
+    }
   }
   std::vector<int64_t> active(std::max(h->max_steps, 1), 0);
   for (int k = 0; k < h->max_steps; k++) {
@@ -138,7 +159,7 @@ int capture(pe_batch *h) {
   cudaError_t err = cudaMemsetAsync(h->sync, 0, 4 * sizeof(unsigned), h->stream);
   if (err == cudaSuccess)
     err = h->exact ? pe::rel5_batch_run_exact(args, h->grid, h->stream)
-                   : pe::rel5_batch_run_fast(args, h->grid, h->stream);
+                   : pe::rel5_batch_run_tiled(args, h->grid, h->tiled_smem, h->stream);
   cudaError_t end = cudaStreamEndCapture(h->stream, &g);
   if (err == cudaSuccess) err = end;
   if (err == cudaSuccess) err = cudaGraphInstantiate(&h->graph, g, 0);
@@ -207,7 +228,10 @@ int pe_batch_create(const pe_relative_params *params, const double *horizons, in
     }
     h->max_steps = std::max(h->max_steps, (int)st.size());
     h->steps.push_back(std::move(st));
-    h->rows.push_back(std::max(1, std::min(g.nx, (256 + g.nx - 1) / g.nx)));
+    // default tile: about one cell per thread (exact), the widest item the
+    // CTA holds (tiled float32)
+    h->rows.push_back(h->exact ? std::max(1, std::min(g.nx, (256 + g.nx - 1) / g.nx))
+                               : pe::rel5_batch_tiled_rows(g.nx, g.xp, 0));
     h->field_off.push_back(fields);
     fields += 3 * (size_t)g.n_padded;
     h->table_off.push_back(tables);
@@ -260,8 +284,10 @@ int pe_batch_create(const pe_relative_params *params, const double *horizons, in
     take(cudaMemset(h->sync, 0, 4 * sizeof(unsigned)));
   }
   if (err == cudaSuccess) {
-    h->grid = h->exact ? pe::rel5_batch_grid_exact() : pe::rel5_batch_grid_fast();
-    if (h->grid <= 0) err = cudaErrorInvalidConfiguration;
+    if (h->exact) {  // the tiled kernel's grid is sized with its tiles
+      h->grid = pe::rel5_batch_grid_exact();
+      if (h->grid <= 0) err = cudaErrorInvalidConfiguration;
+    }
   }
   int rc = PE_OK;
   if (err != cudaSuccess) {

@@ -36,15 +36,22 @@ constexpr int kRel5BatchThreads = 256;
 
 // CTAs of one cooperative launch on the current device (all co-resident).
 int rel5_batch_grid_exact();
-int rel5_batch_grid_fast();
 
 // Every step of every solve (RK2) in one cooperative launch; stages are
 // separated by a grid-wide barrier whose waits are bounded (timeout flag
 // sync[2]).  `sync` must be zeroed before the launch.  Exact: the
-// single-grid exact path's arithmetic (each solve equals it bit for bit);
-// fast: float32 local arithmetic (within float rounding and ENO selection
-// ties of the exact path, like the single-grid float32 kernel).
+// single-grid exact path's arithmetic (each solve equals it bit for bit).
 cudaError_t rel5_batch_run_exact(const Rel5BatchArgs &args, int grid, cudaStream_t stream);
-cudaError_t rel5_batch_run_fast(const Rel5BatchArgs &args, int grid, cudaStream_t stream);
+
+// Float32 update, tiled (relative5d_batch_tiled.cu): a work item is `rows` y
+// rows of one (vP, vE) plane stack, all headings, one thread per 4-cell x
+// chunk.  rows: the tile clamped to the CTA (want < 1: the largest that
+// fits); smem: dynamic shared memory of a CTA for that tile; grid: CTAs of
+// one cooperative launch with that shared memory.
+int rel5_batch_tiled_rows(int nx, int xp, int want);
+size_t rel5_batch_tiled_smem(int rows, int xp);
+int rel5_batch_grid_tiled(size_t smem);
+cudaError_t rel5_batch_run_tiled(const Rel5BatchArgs &args, int grid, size_t smem,
+                                 cudaStream_t stream);
 
 }  // namespace pe

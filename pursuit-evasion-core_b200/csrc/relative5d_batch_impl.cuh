@@ -1,5 +1,5 @@
 // Persistent batched stage loop shared by the exact and the float32 batched
-// kernels (relative5d_batch_exact.cu, relative5d_batch_fast.cu).
+// kernels (relative5d_batch_exact.cu, relative5d_batch_tiled.cu).
 //
 // The CTAs walk, for every RK2 step k and each of its two stages, the work
 // items of the solves that still have a step k (solves are sorted by step

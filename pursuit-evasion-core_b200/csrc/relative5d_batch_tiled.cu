@@ -1,0 +1,409 @@
+// Batched relative 5D solves with the float32 cell update, tiled: the
+// formulas of the exact update (native_relative.cpp:38-67 slopes, :124-172
+// stage) in float32 with reciprocal spacings and multiply-add contraction,
+// the arithmetic of the single-grid float32 kernel (relative5d_fast.cu).
+//
+// A work item is `rows` y rows of one (vP, vE) plane stack of one solve, all
+// headings.  A thread owns a 4-cell x chunk of one row and walks the
+// headings with a 5-heading register window (the psi stencil).  For each
+// heading the CTA stages, with 16-byte cp.async copies double-buffered
+// against the previous heading's arithmetic, the item's own plane rows with
+// a 2-row y halo and the rows of the 8 speed-neighbour planes (vE +-1, +-2,
+// vP +-1, +-2); the x, y and speed stencils then read shared memory.  The
+// persistent loop over steps, the active-item prefix and the bounded grid
+// barrier are those of relative5d_batch_impl.cuh.
+#include "relative5d_batch_impl.cuh"
+#include "relative5d_eno_f32.cuh"
+
+namespace pe {
+namespace {
+
+using namespace eno32;
+
+constexpr int kThreads = kRel5BatchThreads;
+constexpr int kNb = 8;  // vE-2, vE-1, vE+1, vE+2, vP-2, vP-1, vP+1, vP+2
+
+__device__ __forceinline__ void cp_async16(float *dst, const float *src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
+                   (unsigned)__cvta_generic_to_shared(dst)),
+               "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+}
+
+// Shared memory of one heading: own rows [R + 4][xp] then [kNb][R][xp].
+__host__ __device__ inline int buffer_floats(int rows, int xp) {
+  return (rows + 4) * xp + kNb * rows * xp;
+}
+
+struct ItemGeom {
+  int iv, ie, y0, r_eff, R, xc;
+};
+
+// Stage heading `psi` of an item into buffer `buf`.
+__device__ __forceinline__ void stage_heading(const Rel5Grid &g, const float *__restrict__ src,
+                                              const ItemGeom &it, int psi, float *buf) {
+  const int xp = g.xp, xc = it.xc;
+  const int64_t PP = (int64_t)g.nx * xp;
+  // own plane rows y0-2 .. y0+r_eff+1 (inside the box)
+  const int lo = max(0, it.y0 - 2), hi = min(g.nx, it.y0 + it.r_eff + 2);
+  const float *own_src = src + (((int64_t)it.iv * g.nve + it.ie) * g.nh + psi) * PP;
+  const int own_chunks = (hi - lo) * xc;
+  for (int k = threadIdx.x; k < own_chunks; k += kThreads) {
+    const int row = lo + k / xc, col = 4 * (k % xc);
+    cp_async16(buf + (row - it.y0 + 2) * xp + col, own_src + (int64_t)row * xp + col);
+  }
+  // neighbour planes, rows y0 .. y0+r_eff-1
+  float *nbr = buf + (it.R + 4) * xp;
+  const int nb_chunks = it.r_eff * xc;
+#pragma unroll 1
+  for (int q = 0; q < kNb; q++) {
+    const int d = (q & 3) < 2 ? (q & 3) - 2 : (q & 3) - 1;  // -2, -1, +1, +2
+    const int nv = it.iv + (q < 4 ? 0 : d), ne = it.ie + (q < 4 ? d : 0);
+    if (nv < 0 || nv >= g.nvp || ne < 0 || ne >= g.nve) continue;
+    const float *nsrc = src + (((int64_t)nv * g.nve + ne) * g.nh + psi) * PP +
+                        (int64_t)it.y0 * xp;
+    float *ndst = nbr + q * it.R * xp;
+    for (int k = threadIdx.x; k < nb_chunks; k += kThreads) {
+      const int row = k / xc, col = 4 * (k % xc);
+      cp_async16(ndst + row * xp + col, nsrc + (int64_t)row * xp + col);
+    }
+  }
+}
+
+// One stage of one item (all headings).  Returns the largest |change| of
+// this thread's cells (stage 2) and flags non-finite values.
+template <int ORDER, int BLEND>
+__device__ void item_stage(const Rel5Grid &g, const Rel5Stage &s, const ItemGeom &it,
+                           float *smem, float &change_max, float &change_up,
+                           float2 &finite_acc) {
+  const int xp = g.xp, xc = it.xc;
+  const int64_t PP = (int64_t)g.nx * xp;
+  const int tid = threadIdx.x;
+  const int r = tid / xc, c = tid - (tid / xc) * xc;
+  const bool active = tid < it.R * xc && r < it.r_eff;
+  const int x0 = 4 * c, iy = it.y0 + r;
+  const int bufsz = buffer_floats(it.R, xp);
+
+  const float ext = (float)g.extent, dxf = (float)g.dx;
+  const float ihx = (float)(1.0 / g.dx), ihp = (float)(1.0 / g.dphi);
+  const float ihv = (float)(1.0 / g.dvp), ihe = (float)(1.0 / g.dve);
+  const float ap = (float)g.acc_p, ae = (float)g.acc_e;
+  const float vp = (float)(g.vp_lo + it.iv * g.dvp), ve = (float)(g.ve_lo + it.ie * g.dve);
+  const float wp = fabsf(vp) * (float)g.curv_p, we = fabsf(ve) * (float)g.curv_e;
+  const float plo = it.iv == 0 ? 0.f : -ap, phi = it.iv == g.nvp - 1 ? 0.f : ap;
+  const float elo = it.ie == 0 ? 0.f : -ae, ehi = it.ie == g.nve - 1 ? 0.f : ae;
+  const bool p_inner = it.iv > 0 && it.iv < g.nvp - 1;
+  const bool e_inner = it.ie > 0 && it.ie < g.nve - 1;
+  const bool v_slope_inner = it.iv >= 2 && it.iv + 2 < g.nvp;
+  const bool e_slope_inner = it.ie >= 2 && it.ie + 2 < g.nve;
+  const bool y_edge = iy < 2 || iy + 2 >= g.nx;
+  const bool tail = x0 + 4 > g.nx;
+  float xs[4];
+#pragma unroll
+  for (int i = 0; i < 4; i++) xs[i] = fmaf((float)(x0 + i), dxf, -ext);
+  const float2 negx_a = make_float2(-xs[0], -xs[1]), negx_b = make_float2(-xs[2], -xs[3]);
+  const float2 absx_a = make_float2(fabsf(xs[0]), fabsf(xs[1]));
+  const float2 absx_b = make_float2(fabsf(xs[2]), fabsf(xs[3]));
+  const float hx = 0.5f * ihx, hp = 0.5f * ihp, hv = 0.5f * ihv, he = 0.5f * ihe;
+  const float dt = (float)s.dt;
+  const float y = fmaf((float)iy, dxf, -ext);
+  const float ap_coef = (wp + we) * ihp, av_coef = ap * ihv, ae_coef = ae * ihe;
+  const float2 ay_a = __fmul2_rn(__fmul2_rn(f2(wp), absx_a), f2(ihx));
+  const float2 ay_b = __fmul2_rn(__fmul2_rn(f2(wp), absx_b), f2(ihx));
+  const float wy = wp * fabsf(y) * ihx;
+  const int64_t stack = ((int64_t)it.iv * g.nve + it.ie) * g.nh * PP;
+  const int64_t cell0 = stack + (int64_t)iy * xp + x0;  // heading 0
+  const int nh = g.nh;
+  auto wrap = [nh](int q) { return q < 0 ? q + nh : (q >= nh ? q - nh : q); };
+  auto load_window = [&](int q) {
+    return active ? *reinterpret_cast<const float4 *>(s.src + cell0 + (int64_t)wrap(q) * PP)
+                  : make_float4(0.f, 0.f, 0.f, 0.f);
+  };
+
+  float4 win[5];
+#pragma unroll
+  for (int d = 0; d < 5; d++) win[d] = load_window(d - 2);
+
+  stage_heading(g, s.src, it, 0, smem);
+  cp_async_commit();
+  for (int k = 0; k < nh; k++) {
+    cp_async_wait_all();
+    __syncthreads();  // heading k staged; heading k-1's buffer no longer read
+    if (k + 1 < nh) stage_heading(g, s.src, it, k + 1, smem + ((k + 1) & 1) * bufsz);
+    cp_async_commit();
+    const float4 next = k + 1 < nh ? load_window(k + 3) : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float *own = smem + (k & 1) * bufsz;
+    if (active) {
+      const float *o0 = own + (r + 2) * xp + x0;
+      const float *nb = own + (it.R + 4) * xp + r * xp + x0;
+      const float4 C = win[2];
+      const float2 v_a = lo2(C), v_b = hi2(C);
+      const float2 xl = *reinterpret_cast<const float2 *>(o0 - 2);
+      const float2 xr = *reinterpret_cast<const float2 *>(o0 + 4);
+      // rows are padded: x0 - 2 < 0 and x0 + 5 >= xp only read the row's
+      // neighbours in the buffer, which the end rules of slopes_x ignore
+      const float w[8] = {xl.x, xl.y, C.x, C.y, C.z, C.w, xr.x, xr.y};
+      float xlo[4], xhi[4];
+      slopes_x<ORDER, true>(w, x0, g.nx, xlo, xhi);
+      const float2 lx_a = make_float2(xlo[0], xlo[1]), lx_b = make_float2(xlo[2], xlo[3]);
+      const float2 hx_a = make_float2(xhi[0], xhi[1]), hx_b = make_float2(xhi[2], xhi[3]);
+      float2 ly_a, ly_b, hy_a, hy_b;
+      {
+        const float4 m2 = *reinterpret_cast<const float4 *>(o0 - 2 * xp);
+        const float4 m1 = *reinterpret_cast<const float4 *>(o0 - xp);
+        const float4 p1 = *reinterpret_cast<const float4 *>(o0 + xp);
+        const float4 p2 = *reinterpret_cast<const float4 *>(o0 + 2 * xp);
+        if (y_edge) {
+          slope_pair<ORDER, true>(lo2(m2), lo2(m1), v_a, lo2(p1), lo2(p2), iy, g.nx, ly_a, hy_a);
+          slope_pair<ORDER, true>(hi2(m2), hi2(m1), v_b, hi2(p1), hi2(p2), iy, g.nx, ly_b, hy_b);
+        } else {
+          slope_pair<ORDER, false>(lo2(m2), lo2(m1), v_a, lo2(p1), lo2(p2), iy, g.nx, ly_a, hy_a);
+          slope_pair<ORDER, false>(hi2(m2), hi2(m1), v_b, hi2(p1), hi2(p2), iy, g.nx, ly_b, hy_b);
+        }
+      }
+      float2 lp_a, lp_b, hp_a, hp_b;
+      slope_pair<ORDER, false>(lo2(win[0]), lo2(win[1]), v_a, lo2(win[3]), lo2(win[4]), 2, 5,
+                               lp_a, hp_a);
+      slope_pair<ORDER, false>(hi2(win[0]), hi2(win[1]), v_b, hi2(win[3]), hi2(win[4]), 2, 5,
+                               lp_b, hp_b);
+      const int nbf = it.R * xp;
+      float2 le_a, le_b, he_a, he_b, lv_a, lv_b, hv_a, hv_b;
+      {
+        const float4 m2 = *reinterpret_cast<const float4 *>(nb + 0 * nbf);
+        const float4 m1 = *reinterpret_cast<const float4 *>(nb + 1 * nbf);
+        const float4 p1 = *reinterpret_cast<const float4 *>(nb + 2 * nbf);
+        const float4 p2 = *reinterpret_cast<const float4 *>(nb + 3 * nbf);
+        if (e_slope_inner) {
+          slope_pair<ORDER, false>(lo2(m2), lo2(m1), v_a, lo2(p1), lo2(p2), it.ie, g.nve, le_a, he_a);
+          slope_pair<ORDER, false>(hi2(m2), hi2(m1), v_b, hi2(p1), hi2(p2), it.ie, g.nve, le_b, he_b);
+        } else {
+          slope_pair<ORDER, true>(lo2(m2), lo2(m1), v_a, lo2(p1), lo2(p2), it.ie, g.nve, le_a, he_a);
+          slope_pair<ORDER, true>(hi2(m2), hi2(m1), v_b, hi2(p1), hi2(p2), it.ie, g.nve, le_b, he_b);
+        }
+      }
+      {
+        const float4 m2 = *reinterpret_cast<const float4 *>(nb + 4 * nbf);
+        const float4 m1 = *reinterpret_cast<const float4 *>(nb + 5 * nbf);
+        const float4 p1 = *reinterpret_cast<const float4 *>(nb + 6 * nbf);
+        const float4 p2 = *reinterpret_cast<const float4 *>(nb + 7 * nbf);
+        if (v_slope_inner) {
+          slope_pair<ORDER, false>(lo2(m2), lo2(m1), v_a, lo2(p1), lo2(p2), it.iv, g.nvp, lv_a, hv_a);
+          slope_pair<ORDER, false>(hi2(m2), hi2(m1), v_b, hi2(p1), hi2(p2), it.iv, g.nvp, lv_b, hv_b);
+        } else {
+          slope_pair<ORDER, true>(lo2(m2), lo2(m1), v_a, lo2(p1), lo2(p2), it.iv, g.nvp, lv_a, hv_a);
+          slope_pair<ORDER, true>(hi2(m2), hi2(m1), v_b, hi2(p1), hi2(p2), it.iv, g.nvp, lv_b, hv_b);
+        }
+      }
+      // Hamiltonian + dissipation (native_relative.cpp:144-157)
+      const float bx = fmaf(ve, (float)s.cs[k], -vp);
+      const float by = ve * (float)s.sn[k];
+      const float2 bx2 = f2(bx), by2 = f2(by);
+      const float ax_coef = fmaf(fabsf(bx), ihx, wy);
+      const float aby = fabsf(by) * ihx;
+      const int64_t cell = cell0 + (int64_t)k * PP;
+      const float4 prev4 = BLEND ? *reinterpret_cast<const float4 *>(s.dst + cell) : C;
+      float2 out[2];
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const float2 lx = h ? lx_b : lx_a, hxv = h ? hx_b : hx_a;
+        const float2 ly = h ? ly_b : ly_a, hy = h ? hy_b : hy_a;
+        const float2 lp = h ? lp_b : lp_a, hpv = h ? hp_b : hp_a;
+        const float2 lv = h ? lv_b : lv_a, hvv = h ? hv_b : hv_a;
+        const float2 le = h ? le_b : le_a, hev = h ? he_b : he_a;
+        const float2 v = h ? v_b : v_a;
+        const float2 negx = h ? negx_b : negx_a;
+        const float2 ay = __fadd2_rn(h ? ay_b : ay_a, f2(aby));
+        const float2 gx = __fmul2_rn(__fadd2_rn(lx, hxv), f2(hx));
+        const float2 gy = __fmul2_rn(__fadd2_rn(ly, hy), f2(hx));
+        const float2 gpn = __fmul2_rn(__fadd2_rn(lp, hpv), f2(-hp));  // -gp
+        const float2 gv = __fmul2_rn(__fadd2_rn(lv, hvv), f2(hv));
+        const float2 ge = __fmul2_rn(__fadd2_rn(le, hev), f2(he));
+        float2 H = __ffma2_rn(by2, gy, __fmul2_rn(bx2, gx));
+        float2 t = __ffma2_rn(f2(y), gx, gpn);
+        t = __ffma2_rn(negx, gy, t);
+        float hs[2] = {H.x, H.y};
+        const float ts[2] = {t.x, t.y}, gps[2] = {gpn.x, gpn.y};
+        const float gvs[2] = {gv.x, gv.y}, ges[2] = {ge.x, ge.y};
+#pragma unroll
+        for (int l = 0; l < 2; l++) {
+          hs[l] = fmaf(-wp, fabsf(ts[l]), hs[l]);
+          hs[l] = fmaf(we, fabsf(gps[l]), hs[l]);
+          hs[l] = p_inner ? fmaf(-ap, fabsf(gvs[l]), hs[l])
+                          : hs[l] + fminf(plo * gvs[l], phi * gvs[l]);
+          hs[l] = e_inner ? fmaf(ae, fabsf(ges[l]), hs[l])
+                          : hs[l] + fmaxf(elo * ges[l], ehi * ges[l]);
+        }
+        H = make_float2(hs[0], hs[1]);
+        float2 diss = __fmul2_rn(f2(ax_coef), sub2(hxv, lx));
+        diss = __ffma2_rn(ay, sub2(hy, ly), diss);
+        diss = __ffma2_rn(f2(ap_coef), sub2(hpv, lp), diss);
+        diss = __ffma2_rn(f2(av_coef), sub2(hvv, lv), diss);
+        diss = __ffma2_rn(f2(ae_coef), sub2(hev, le), diss);
+        H = __ffma2_rn(f2(0.5f), diss, H);
+        float2 value = __ffma2_rn(f2(dt), make_float2(fminf(H.x, 0.f), fminf(H.y, 0.f)), v);
+        const float2 prev = BLEND ? (h ? hi2(prev4) : lo2(prev4)) : v;
+        if (BLEND) value = __fmul2_rn(f2(0.5f), __fadd2_rn(prev, value));
+        if (tail && x0 + 2 * h + 1 >= g.nx) {  // row padding stays 0
+          if (x0 + 2 * h >= g.nx) value.x = 0.f;
+          value.y = 0.f;
+        }
+        finite_acc = __ffma2_rn(value, f2(0.f), finite_acc);
+        out[h] = value;
+        if (BLEND) {
+          const float2 change = sub2(value, prev);
+          change_max = fmaxf(change_max, fmaxf(fabsf(change.x), fabsf(change.y)));
+          change_up = fmaxf(change_up, fmaxf(change.x, change.y));
+          const float2 sgn = __fmul2_rn(prev, value);
+          if (sgn.x <= 0.f || sgn.y <= 0.f) {
+            const float pv[2] = {prev.x, prev.y}, nv[2] = {value.x, value.y};
+#pragma unroll
+            for (int l = 0; l < 2; l++) {
+              float *slot = s.arrival + cell + 2 * h + l;
+              if (pv[l] > 0.f && nv[l] <= 0.f && x0 + 2 * h + l < g.nx && isnan(*slot))
+                *slot = (float)(s.t + s.dt * (double)pv[l] /
+                                            ((double)pv[l] - (double)nv[l]));
+            }
+          }
+        }
+      }
+      *reinterpret_cast<float4 *>(s.dst + cell) =
+          make_float4(out[0].x, out[0].y, out[1].x, out[1].y);
+    }
+#pragma unroll
+    for (int d = 0; d < 4; d++) win[d] = win[d + 1];
+    win[4] = next;
+  }
+  cp_async_wait_all();
+  __syncthreads();  // the buffers are restaged by the next item
+}
+
+template <int BLEND>
+__device__ void tiled_stage(const Rel5BatchArgs &A, int step, int64_t n_items, double *scratch,
+                            Rel5Grid *sg, float *smem) {
+  int64_t lo = 0, hi = 0;
+  const Rel5BatchSolve *S = nullptr;
+  Rel5Stage s{};
+  int rows = 1, slabs = 1, xc = 1;
+  float change_max = 0.f, change_up = 0.f;
+  float2 finite_acc = make_float2(0.f, 0.f);
+  auto flush = [&]() {
+    if (!S) return;
+    const bool bad = !(isfinite(finite_acc.x) && isfinite(finite_acc.y));
+    if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(&S->stats->nonfinite, 1u);
+    if (BLEND) {
+      const double m_abs = batch_impl::block_max((double)change_max, scratch);
+      const double m_up = batch_impl::block_max((double)change_up, scratch);
+      if (threadIdx.x == 0) {
+        batch_impl::atomic_max_nonneg(&S->stats->residual, m_abs);
+        batch_impl::atomic_max_nonneg(&S->stats->increase, m_up);
+      }
+    }
+    change_max = change_up = 0.f;
+    finite_acc = make_float2(0.f, 0.f);
+  };
+  for (int64_t item = blockIdx.x; item < n_items; item += gridDim.x) {
+    if (item < lo || item >= hi) {  // the same for every thread of the CTA
+      flush();
+      S = &A.solves[batch_impl::find_solve(A, item)];
+      lo = S->item_base;
+      hi = lo + S->items;
+      __syncthreads();  // the previous solve's grid copy is no longer read
+      if (threadIdx.x == 0) *sg = S->g;
+      const double2 td = S->steps[step];
+      s.src = BLEND ? S->b : S->a;
+      s.dst = BLEND ? S->a : S->b;
+      s.arrival = S->arrival;
+      s.sn = S->sn;
+      s.cs = S->cs;
+      s.t = td.x;
+      s.dt = td.y;
+      s.stats = S->stats;
+      rows = S->rows;
+      __syncthreads();
+      slabs = (sg->nx + rows - 1) / rows;
+      xc = sg->xp / 4;
+    }
+    const Rel5Grid &g = *sg;
+    int64_t local = item - lo;
+    ItemGeom it;
+    const int slab = (int)(local % slabs);
+    local /= slabs;
+    it.ie = (int)(local % g.nve);
+    it.iv = (int)(local / g.nve);
+    it.R = rows;
+    it.xc = xc;
+    it.y0 = slab * rows;
+    it.r_eff = min(rows, g.nx - it.y0);
+    item_stage<2, BLEND>(g, s, it, smem, change_max, change_up, finite_acc);
+  }
+  flush();
+}
+
+__global__ void __launch_bounds__(kThreads, 2)
+    rel5_batch_tiled_kernel(const Rel5BatchArgs A) {
+  extern __shared__ __align__(16) float smem[];
+  __shared__ double scratch[kThreads / 32];
+  __shared__ Rel5Grid sg;
+  unsigned round = 0;
+  for (int step = 0; step < A.max_steps; step++) {
+    const int64_t n_items = A.active_items[step];
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < A.count;
+         k += gridDim.x * blockDim.x)
+      if (step < A.solves[k].nsteps) A.solves[k].stats->residual = 0ull;
+    tiled_stage<0>(A, step, n_items, scratch, &sg, smem);
+    if (!batch_impl::grid_barrier(A.sync, ++round)) break;
+    tiled_stage<1>(A, step, n_items, scratch, &sg, smem);
+    if (!batch_impl::grid_barrier(A.sync, ++round)) break;
+  }
+}
+
+}  // namespace
+
+int rel5_batch_tiled_rows(int nx, int xp, int want) {
+  const int cap = kThreads / (xp / 4);
+  int rows = want < 1 ? cap : want;
+  rows = rows > cap ? cap : rows;
+  rows = rows > nx ? nx : rows;
+  return rows < 1 ? 1 : rows;
+}
+
+size_t rel5_batch_tiled_smem(int rows, int xp) {
+  return 2 * sizeof(float) * (size_t)buffer_floats(rows, xp);
+}
+
+int rel5_batch_grid_tiled(size_t smem) {
+  int device = 0, sms = 0, per_sm = 0;
+  if (cudaGetDevice(&device) != cudaSuccess) return 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
+    return 0;
+  if (cudaFuncSetAttribute(rel5_batch_tiled_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem) != cudaSuccess)
+    return 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rel5_batch_tiled_kernel, kThreads,
+                                                    smem) != cudaSuccess)
+    return 0;
+  return sms * per_sm;
+}
+
+cudaError_t rel5_batch_run_tiled(const Rel5BatchArgs &args, int grid, size_t smem,
+                                 cudaStream_t stream) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3(kThreads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, rel5_batch_tiled_kernel, args);
+}
+
+}  // namespace pe

@@ -1,9 +1,11 @@
 """Tile autotuner of the batched solver.
 
-The batched kernel's work item is `rows` y rows of one (vP, vE, psi) plane
-of one solve.  Fewer rows give more, smaller items (better balance, less
-reuse of neighbour rows in L1); more rows the reverse, and the best choice
-depends on the grid width.  `tune` times every candidate row count on a few
+A work item of the exact batched kernel is `rows` y rows of one (vP, vE,
+psi) plane of one solve; one of the tiled float32 kernel is `rows` y rows of
+one (vP, vE) plane stack over all headings, a thread per 4-cell x chunk (at
+most 256 / ceil(positions / 4) rows).  Fewer rows give more, smaller items
+(better balance across the CTAs); more rows the reverse (less y halo per
+cell), and the best choice depends on the grid width.  `tune` times every candidate row count on a few
 solves of each width bucket (each solve cut to a short horizon, so a trial
 is a few RK2 steps) and keeps the fastest; the winners are cached in a JSON
 file keyed by device name and arithmetic, and `apply` sets them on a
@@ -42,8 +44,13 @@ def _device_name(device):
     return torch.cuda.get_device_name(device)
 
 
-def candidates(narrowest):
-    """Row counts that give every thread of a 256-thread CTA a cell."""
+def candidates(narrowest, local_precision="float64"):
+    """Row counts to try for a bucket whose narrowest grid has `narrowest`
+    positions: exact kernel, those that give every thread of a 256-thread
+    CTA a cell; tiled float32 kernel, those up to the CTA's capacity."""
+    if local_precision == "float32":
+        cap = min(narrowest, 256 // ((narrowest + 3) // 4))
+        return sorted({min(r, cap) for r in CANDIDATE_ROWS if r <= narrowest} | {cap})
     rows = [r for r in CANDIDATE_ROWS if r <= narrowest and r * narrowest >= 256]
     return rows or [narrowest]
 
@@ -54,7 +61,8 @@ def tune(solves, *, device=0, local_precision="float32", per_bucket=6, trial_ste
     import torch
 
     cache = Path(cache) if cache else default_cache()
-    key = f"{_device_name(device)} {local_precision}"
+    key = f"{_device_name(device)} {local_precision}" + (" tiled" if local_precision == "float32"
+                                                         else "")
     try:
         table = json.loads(cache.read_text())
     except (OSError, ValueError):
@@ -74,7 +82,7 @@ def tune(solves, *, device=0, local_precision="float32", per_bucket=6, trial_ste
             limits = [probe.info(i)["dt_limit"] for i in range(len(sample))]
         trial = [replace(s, horizon=trial_steps * lim) for s, lim in zip(sample, limits)]
         with BatchSolver(trial, local_precision=local_precision, device=device) as b:
-            for rows in candidates(min(s.grid.positions for s in trial)):
+            for rows in candidates(min(s.grid.positions for s in trial), local_precision):
                 for i in range(len(trial)):
                     b.set_tile(i, rows)
                 best = None

@@ -37,7 +37,11 @@ def test_buckets_and_candidates():
     assert autotune.bucket_of(65) == "other"
     for n in (17, 24, 33, 49):
         assert all(r * n >= 256 and r <= n for r in autotune.candidates(n))
+        # tiled float32 kernel: at most one 4-cell chunk per thread of 256
+        tiled = autotune.candidates(n, "float32")
+        assert tiled and all(1 <= r <= n and r * ((n + 3) // 4) <= 256 for r in tiled)
     assert autotune.candidates(17) == [16]
+    assert autotune.candidates(49, "float32")[-1] == 19
 
 
 @pytest.mark.parametrize("field, value", [("order", 1), ("precision", _native.PE_LOCAL_F32),
