@@ -112,6 +112,25 @@ int pe_relative_synchronize(pe_relative *h);
 int pe_relative_copy_field(pe_relative *h, float *host_field);
 int pe_relative_copy_arrival(pe_relative *h, float *host_arrival);
 
+/* Initialise from a plane broadcast over the outer axes, as the reference
+ * GPU path's `initialize` kernel does (gpu_relative.py:42-45, field[j] =
+ * plane[j % plane_size] over the dense storage order): plane_size is
+ * positions^2 (one (y, x) plane) or headings * positions^2 (a (psi, y, x)
+ * block, e.g. the rectangle-contact capture field).  Arrival = start_time
+ * where the value is <= 0, else NaN. */
+int pe_relative_init_plane(pe_relative *h, const float *plane, int64_t plane_size,
+                           double start_time);
+/* Local exit (gpu_relative.py:96-101): cells with x^2 + y^2 > radius_squared
+ * take the value `radius` in every stage and never arrive.  The reference
+ * compiles both numbers into its kernel as literals (9 significant digits);
+ * the caller passes them as it rounds them.  0, 0 disables the exit. */
+int pe_relative_set_exit(pe_relative *h, double radius, double radius_squared);
+/* Values of the current field at n states (gpu_relative.py:189-214,
+ * :299-306): 32-corner multilinear stencils, dense storage-order cell
+ * indices [n][32] and weights [n][32] (host), summed in double. */
+int pe_relative_probe(pe_relative *h, int64_t n, const int64_t *indices, const double *weights,
+                      double *host_out);
+
 /* Asynchronous history output (the reference writes each output frame of
  * fields.f32 between advances with the solver stopped meanwhile,
  * native_relative.cpp:111-120).  pe_relative_snapshot packs

@@ -27,6 +27,8 @@ struct pe_relative {
   int64_t steps = 0;
   bool initialized = false;
   pe::LaunchTimer timer;  // per-stage launch times (pe_relative_profile)
+  double exit_r = 0, exit_r2 = 0;  // local exit (0: none)
+  int2 *exit_keep = nullptr;        // its kept x range per y row (float32 kernels)
   // asynchronous history output: two dense snapshot buffers, filled on the
   // compute stream and copied out on their own stream
   float *snap[2] = {nullptr, nullptr};
@@ -52,6 +54,7 @@ void release(pe_relative *h) {
   cudaFree(h->snf);
   cudaFree(h->csf);
   cudaFree(h->stats);
+  cudaFree(h->exit_keep);
   if (h->host_stats) cudaFreeHost(h->host_stats);
   if (h->copy_stream) cudaStreamSynchronize(h->copy_stream);
   for (int i = 0; i < 2; i++) {
@@ -76,6 +79,9 @@ int launch_stage(pe_relative *h, int stage, const float *src, float *dst,
   s.dt = dt;
   s.t = h->t;
   s.stats = h->stats;
+  s.exit_r = h->exit_r;
+  s.exit_r2 = h->exit_r2;
+  s.exit_keep = h->exit_r2 > 0 ? h->exit_keep : nullptr;
   cudaEvent_t e0 = h->timer.begin(h->stream);
   const cudaError_t err =
       h->p.precision == PE_LOCAL_F64
@@ -292,6 +298,89 @@ int pe_relative_synchronize(pe_relative *h) {
   int rc = enter(h);
   if (rc) return rc;
   return read_stats(h);
+}
+
+int pe_relative_init_plane(pe_relative *h, const float *plane, int64_t plane_size,
+                           double start_time) {
+  int rc = enter(h);
+  if (rc) return rc;
+  const int64_t nx2 = (int64_t)h->g.nx * h->g.nx;
+  if (!plane || (plane_size != nx2 && plane_size != nx2 * h->g.nh))
+    return fail(PE_EINVAL, "plane must hold positions^2 or headings * positions^2 values");
+  if (!std::isfinite(start_time) || start_time < 0)
+    return fail(PE_EINVAL, "start_time must be finite and >= 0");
+  for (int64_t i = 0; i < plane_size; i++)
+    if (!std::isfinite(plane[i])) return fail(PE_EINVAL, "non-finite plane value");
+  float *dplane = nullptr;
+  PE_CUDA_TRY(cudaMalloc(&dplane, sizeof(float) * (size_t)plane_size));
+  cudaError_t err = cudaMemcpyAsync(dplane, plane, sizeof(float) * (size_t)plane_size,
+                                    cudaMemcpyHostToDevice, h->stream);
+  if (err == cudaSuccess) err = cudaMemsetAsync(h->stats, 0, sizeof(pe::Rel5Stats), h->stream);
+  if (err == cudaSuccess)
+    err = pe::rel5_init(h->g, dplane, h->a, h->arrival, (float)start_time, h->stream,
+                        plane_size);
+  if (err == cudaSuccess) err = cudaStreamSynchronize(h->stream);
+  cudaFree(dplane);
+  if (err != cudaSuccess) return pe::cuda_fail(err, "pe_relative_init_plane");
+  pe::count_launches(1);
+  h->t = start_time;
+  h->steps = 0;
+  h->initialized = true;
+  return PE_OK;
+}
+
+int pe_relative_set_exit(pe_relative *h, double radius, double radius_squared) {
+  int rc = enter(h);
+  if (rc) return rc;
+  if (!std::isfinite(radius) || !std::isfinite(radius_squared) || radius < 0 ||
+      radius_squared < 0 || (radius > 0) != (radius_squared > 0))
+    return fail(PE_EINVAL, "exit radius must be finite and >= 0");
+  if (radius > 0 && !(radius < h->g.extent))
+    return fail(PE_EINVAL, "Local exit radius must lie inside the numerical grid");
+  if (radius > 0) {
+    if (!h->exit_keep) PE_CUDA_TRY(cudaMalloc(&h->exit_keep, sizeof(int2) * h->g.nx));
+    cudaError_t err = pe::rel5_exit_rows(h->g, (float)radius_squared, h->exit_keep, h->stream);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(h->stream);
+    if (err != cudaSuccess) return pe::cuda_fail(err, "pe_relative_set_exit");
+    pe::count_launches(1);
+  }
+  h->exit_r = radius;
+  h->exit_r2 = radius_squared;
+  return PE_OK;
+}
+
+int pe_relative_probe(pe_relative *h, int64_t n, const int64_t *indices, const double *weights,
+                      double *host_out) {
+  int rc = enter(h);
+  if (rc) return rc;
+  if (n < 0 || (n > 0 && (!indices || !weights || !host_out)))
+    return fail(PE_EINVAL, "bad probe arrays");
+  if (n == 0) return PE_OK;
+  for (int64_t i = 0; i < 32 * n; i++)
+    if (indices[i] < 0 || indices[i] >= h->g.n || !std::isfinite(weights[i]))
+      return fail(PE_EINVAL, "probe stencil out of range");
+  int64_t *didx = nullptr;
+  double *dw = nullptr, *dout = nullptr;
+  cudaError_t err = cudaMalloc(&didx, sizeof(int64_t) * 32 * (size_t)n);
+  if (err == cudaSuccess) err = cudaMalloc(&dw, sizeof(double) * 32 * (size_t)n);
+  if (err == cudaSuccess) err = cudaMalloc(&dout, sizeof(double) * (size_t)n);
+  if (err == cudaSuccess)
+    err = cudaMemcpyAsync(didx, indices, sizeof(int64_t) * 32 * (size_t)n,
+                          cudaMemcpyHostToDevice, h->stream);
+  if (err == cudaSuccess)
+    err = cudaMemcpyAsync(dw, weights, sizeof(double) * 32 * (size_t)n, cudaMemcpyHostToDevice,
+                          h->stream);
+  if (err == cudaSuccess) err = pe::rel5_probe(h->g, h->a, n, didx, dw, dout, h->stream);
+  if (err == cudaSuccess)
+    err = cudaMemcpyAsync(host_out, dout, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost,
+                          h->stream);
+  if (err == cudaSuccess) err = cudaStreamSynchronize(h->stream);
+  cudaFree(didx);
+  cudaFree(dw);
+  cudaFree(dout);
+  if (err != cudaSuccess) return pe::cuda_fail(err, "pe_relative_probe");
+  pe::count_launches(1);
+  return PE_OK;
 }
 
 int pe_relative_snapshot(pe_relative *h, int32_t slot) {

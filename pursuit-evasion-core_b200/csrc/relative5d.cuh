@@ -41,6 +41,12 @@ struct Rel5Stage {
   const float *snf, *csf;  // the same, rounded to float
   double dt, t;            // step size and the step's start time
   Rel5Stats *stats;
+  // local exit (gpu_relative.py:96-101): cells with x^2 + y^2 > exit_r2 are
+  // set to exit_r and never arrive; exit_r2 = 0 disables it
+  double exit_r, exit_r2;
+  // the same exit as kept x ranges per y row, [lo, hi] (float32 kernels;
+  // nullptr when there is no exit)
+  const int2 *exit_keep;
 };
 
 // Tiling of the fast stage kernel: a CTA owns `rows` y-rows of one (vP, vE)
@@ -77,7 +83,18 @@ cudaError_t rel5_stage_f64(const Rel5Grid &g, const Rel5Stage &s, int blend,
 // value is <= 0, NaN elsewhere.  With plane == nullptr the field is taken as
 // already filled and only arrival (and the padding) is set.
 cudaError_t rel5_init(const Rel5Grid &g, const float *plane, float *field,
-                      float *arrival, float start_time, cudaStream_t stream);
+                      float *arrival, float start_time, cudaStream_t stream,
+                      int64_t plane_size = 0);
+
+// Kept x range per y row for the float32 kernels: ix in [lo, hi] has
+// x*x + y*y <= r2 in float32 arithmetic without contraction (x = -W + ix*dx,
+// dx = 2W/(nx-1)), as the reference's float32 kernel evaluates its exit.
+cudaError_t rel5_exit_rows(const Rel5Grid &g, float r2, int2 *keep, cudaStream_t stream);
+
+// Probe values: out[i] = sum_k w[i][k] * field[idx[i][k]] in double, idx
+// dense storage-order cell indices [n][32] (device arrays).
+cudaError_t rel5_probe(const Rel5Grid &g, const float *field, int64_t n, const int64_t *idx,
+                       const double *w, double *out, cudaStream_t stream);
 
 // Convert one field between the padded device layout and the dense table
 // layout (device to device).

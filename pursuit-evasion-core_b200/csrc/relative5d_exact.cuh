@@ -89,6 +89,11 @@ __device__ __forceinline__ void cell_update(const Rel5Grid &g, const Rel5Stage &
 
   const double x = -g.extent + ix * g.dx;
   const double y = -g.extent + iy * g.dx;
+  if (s.exit_r2 > 0 && x * x + y * y > s.exit_r2) {  // held at the exit value
+    s.dst[j] = (float)s.exit_r;
+    change_abs = change_up = 0;
+    return;
+  }
   const double vp = g.vp_lo + iv * g.dvp, ve = g.ve_lo + ie * g.dve;
   const double wp = fabs(vp) * g.curv_p, we = fabs(ve) * g.curv_e;
   const double bx = ve * s.cs[ip] - vp, by = ve * s.sn[ip];

@@ -299,6 +299,8 @@ __global__ void __launch_bounds__(TARGET_THREADS, 2)
     const float2 absx_b = make_float2(fabsf(xs[2]), fabsf(xs[3]));
     const float hx = 0.5f * a.ihx, hp = 0.5f * a.ihp, hv = 0.5f * a.ihv, he = 0.5f * a.ihe;
     const float dt = a.dt;
+    const bool has_exit = a.s.exit_keep != nullptr;
+    const float exit_r = (float)a.s.exit_r;
     const int ctr = (r + 2) * XP + x0;  // this chunk in an own slot
     const int nbo = r * XP + x0;        // this chunk in a neighbour slot
     const bool tail = x0 + 4 > g.nx;                // chunk holds row padding
@@ -310,6 +312,7 @@ __global__ void __launch_bounds__(TARGET_THREADS, 2)
       const bool active = r < it.r_eff;
       const int iy = it.y0 + r;
       const bool y_edge = iy < 2 || iy + 2 >= g.nx;
+      const int2 keep = has_exit ? a.s.exit_keep[iy] : make_int2(0, 0);
       const float vp = (float)(g.vp_lo + it.iv * g.dvp);
       const float ve = (float)(g.ve_lo + it.ie * g.dve);
       const float wp = fabsf(vp) * (float)g.curv_p;
@@ -486,6 +489,11 @@ __global__ void __launch_bounds__(TARGET_THREADS, 2)
                 __ffma2_rn(f2(dt), make_float2(fminf(H.x, 0.f), fminf(H.y, 0.f)), v);
             const float2 prev = BLEND ? (h ? hi2(prev4) : lo2(prev4)) : v;
             if (BLEND) value = __fmul2_rn(f2(0.5f), __fadd2_rn(prev, value));
+            if (has_exit) {  // cells beyond the local exit hold the exit value
+              const int ix = x0 + 2 * h;
+              if (ix < keep.x || ix > keep.y) value.x = exit_r;
+              if (ix + 1 < keep.x || ix + 1 > keep.y) value.y = exit_r;
+            }
             if (tail && x0 + 2 * h + 1 >= g.nx) {  // row padding stays 0
               if (x0 + 2 * h >= g.nx) value.x = 0.f;
               value.y = 0.f;
@@ -594,7 +602,7 @@ cudaError_t launch(const FastArgs &args, size_t smem, int threads,
   return cudaGetLastError();
 }
 
-__global__ void rel5_init_kernel(const float *__restrict__ plane,
+__global__ void rel5_init_kernel(const float *__restrict__ plane, int64_t plane_size,
                                  float *__restrict__ field,
                                  float *__restrict__ arrival, int64_t n_padded,
                                  int nx, int xp, float start_time) {
@@ -609,7 +617,9 @@ __global__ void rel5_init_kernel(const float *__restrict__ plane,
       arrival[j] = 0.f;
       continue;
     }
-    const float v = plane ? plane[iy * nx + ix] : field[j];
+    // dense index modulo the plane: one (y, x) plane or a (psi, y, x) block
+    const int64_t dense = (j / pp) * nx * nx + (int64_t)iy * nx + ix;
+    const float v = plane ? plane[dense % plane_size] : field[j];
     if (plane) field[j] = v;
     arrival[j] = v <= 0.f ? start_time : __int_as_float(0x7fc00000);
   }
@@ -709,13 +719,60 @@ cudaError_t rel5_stage_f32(const Rel5Grid &g, const Rel5Tile &t,
   return launch<2, 0>(args, smem, threads, stream);
 }
 
+__global__ void rel5_probe_kernel(const float *__restrict__ field, int nx, int xp,
+                                  int64_t n, const int64_t *__restrict__ idx,
+                                  const double *__restrict__ w, double *__restrict__ out) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double total = 0;
+  for (int k = 0; k < 32; k++) {
+    const int64_t d = idx[32 * i + k];  // dense index -> padded row layout
+    total += w[32 * i + k] * (double)field[(d / nx) * xp + d % nx];
+  }
+  out[i] = total;
+}
+
+__global__ void rel5_exit_rows_kernel(int nx, float extent, float r2, int2 *keep) {
+  const int iy = blockIdx.x * blockDim.x + threadIdx.x;
+  if (iy >= nx) return;
+  // explicit round-to-nearest operations: nothing is contracted
+  const float dx = __fdiv_rn(__fmul_rn(2.f, extent), (float)(nx - 1));
+  const float y = __fadd_rn(-extent, __fmul_rn((float)iy, dx));
+  const float yy = __fmul_rn(y, y);
+  int lo = nx, hi = -1;
+  for (int ix = 0; ix < nx; ix++) {
+    const float x = __fadd_rn(-extent, __fmul_rn((float)ix, dx));
+    if (!(__fadd_rn(__fmul_rn(x, x), yy) > r2)) {
+      lo = min(lo, ix);
+      hi = ix;
+    }
+  }
+  keep[iy] = make_int2(lo, hi);  // x^2 is unimodal in ix: the kept set is one range
+}
+
+cudaError_t rel5_exit_rows(const Rel5Grid &g, float r2, int2 *keep, cudaStream_t stream) {
+  rel5_exit_rows_kernel<<<(g.nx + 127) / 128, 128, 0, stream>>>(g.nx, (float)g.extent, r2,
+                                                                keep);
+  return cudaGetLastError();
+}
+
+cudaError_t rel5_probe(const Rel5Grid &g, const float *field, int64_t n, const int64_t *idx,
+                       const double *w, double *out, cudaStream_t stream) {
+  if (n <= 0) return cudaSuccess;
+  rel5_probe_kernel<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(field, g.nx, g.xp, n, idx,
+                                                                     w, out);
+  return cudaGetLastError();
+}
+
 cudaError_t rel5_init(const Rel5Grid &g, const float *plane, float *field,
-                      float *arrival, float start_time, cudaStream_t stream) {
+                      float *arrival, float start_time, cudaStream_t stream,
+                      int64_t plane_size) {
   const int threads = 256;
   int64_t blocks = (g.n_padded + threads - 1) / threads;
   if (blocks > 148 * 64) blocks = 148 * 64;
   rel5_init_kernel<<<(unsigned)blocks, threads, 0, stream>>>(
-      plane, field, arrival, g.n_padded, g.nx, g.xp, start_time);
+      plane, plane_size > 0 ? plane_size : (int64_t)g.nx * g.nx, field, arrival, g.n_padded,
+      g.nx, g.xp, start_time);
   return cudaGetLastError();
 }
 

@@ -215,6 +215,9 @@ SIGNATURES = {
     "pe_table_value": (ctypes.c_int, [_P, _DP, ctypes.c_int64, _DP]),
     "pe_table_field": (ctypes.c_int, [_P, _DP, _DP, ctypes.c_int64, _DP]),
     "pe_table_destroy": (ctypes.c_int, [_P]),
+    "pe_relative_init_plane": (ctypes.c_int, [_P, _P, ctypes.c_int64, ctypes.c_double]),
+    "pe_relative_set_exit": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_double]),
+    "pe_relative_probe": (ctypes.c_int, [_P, ctypes.c_int64, _P, _P, _P]),
     "pe_relative_snapshot": (ctypes.c_int, [_P, ctypes.c_int32]),
     "pe_relative_copy_snapshot": (ctypes.c_int, [_P, ctypes.c_int32, _P]),
     "pe_host_alloc": (ctypes.c_int, [ctypes.c_size_t, ctypes.POINTER(ctypes.c_void_p)]),

@@ -151,6 +151,9 @@ def solve(
     tol=None,
     warm_start=None,
     save_final=True,
+    probes=None,
+    capture_footprints=None,
+    exit_radius=None,
 ):
     """Compute a new relative table directory on the GPU.
 
@@ -158,10 +161,26 @@ def solve(
     above max_working_gb (MemoryError, before anything is created) and too
     little disk (OSError), like free_dp.py:145-176.  `threads` is accepted
     for signature compatibility and recorded; the GPU does not use it.
+
+    The reference's GPU solve (gpu_relative.py:67-101) adds three keywords,
+    accepted here with its meaning and errors: `capture_footprints` =
+    (pursuer, evader) Footprints for a "rectangle_contact" configuration
+    (the capture field becomes the oriented-rectangle separation over every
+    heading); `exit_radius` = R in (0, extent): cells with x^2 + y^2 > R^2
+    start at and stay at R; `probes` = relative states [n, 5] (x, y, psi,
+    vP, vE) whose multilinear values are written to probes.f64 after every
+    frame.  `warm_start`, when given, replaces the initial field; the exit
+    still holds in every stage.
     """
     solve_started = time.perf_counter()
-    if config.capture_rule != "center_distance":
-        raise ValueError("This legacy free-space solver uses circular capture")
+    if config.capture_rule == "rectangle_contact" and capture_footprints is None:
+        raise ValueError("Rectangle capture requires explicit P/E footprints")
+    if config.capture_rule == "center_distance" and capture_footprints is not None:
+        raise ValueError("Declare rectangle_contact in the configuration")
+    if config.capture_rule not in ("center_distance", "rectangle_contact"):
+        raise ValueError("Unknown capture rule")
+    if exit_radius is not None and not 0 < exit_radius < grid.extent:
+        raise ValueError("Local exit radius must lie inside the numerical grid")
     _validate(config, grid, horizon, output_dt, order, cfl, threads)
     if (not np.isfinite([max_working_gb, disk_reserve_gb]).all()
             or max_working_gb <= 0 or disk_reserve_gb < 0):
@@ -176,7 +195,11 @@ def solve(
     times = output_times(horizon, output_dt)
     N = grid.states
     working = N * 12
-    storage = N * 4 * ((2 if save_final else 0) + (len(times) if history else 0))
+    probe_states = probe_indices = probe_weights = None
+    if probes is not None:
+        probe_states, probe_indices, probe_weights = probe_stencils(config, grid, probes)
+    storage = N * 4 * ((2 if save_final else 0) + (len(times) if history else 0)) + (
+        0 if probe_states is None else 8 * len(probe_states) * len(times))
     if working > max_working_gb * 1e9:
         raise MemoryError(
             f"Core arrays need {working / 1e9:.3f} GB, above guard {max_working_gb}"
@@ -200,7 +223,11 @@ def solve(
     output.mkdir(exist_ok=True)
     meta = {"schema": SCHEMA, "status": "running"}
     try:
-        solver.initialize(initial)
+        solver.set_exit(exit_radius)
+        if initial is not None:
+            solver.initialize(initial)
+        else:
+            solver.initialize_plane(capture_plane(config, grid, capture_footprints, exit_radius))
         allocation_seconds = time.perf_counter() - alloc_started
         meta.update({
             "schema": SCHEMA,
@@ -222,6 +249,11 @@ def solve(
             "history_saved": bool(history),
             "dtype": "float32",
             "target": "physical_capture_only",
+            "capture_rule": config.capture_rule,
+            "capture_footprints": None if capture_footprints is None else {
+                "pursuer": capture_footprints[0].to_dict(),
+                "evader": capture_footprints[1].to_dict()},
+            "local_exit_radius": exit_radius,
             "avoid": None,
             "tube_projection": "min over every internal update",
             "position_boundary":
@@ -239,10 +271,12 @@ def solve(
             "predicted_output_bytes": storage,
             "device": int(device),
             "status": "running",
+            "probe_states": None if probe_states is None else probe_states.tolist(),
         })
         (output / "meta.json").write_text(json.dumps(meta, indent=2) + "\n")
+        probe = None if probe_states is None else (probe_indices, probe_weights)
         meta.update(_run(solver, output, times, history=history, tol=tol,
-                         save_final=save_final))
+                         save_final=save_final, probe=probe))
         meta["allocation_seconds"] = allocation_seconds
         meta["status"] = "complete"
         if meta["frames"] != len(meta["times"]):
@@ -316,11 +350,86 @@ class _HistoryWriter:
             raise self.error
 
 
-def _run(solver, output, times, *, history, tol, save_final):
+def capture_plane(config, grid, capture_footprints=None, exit_radius=None):
+    """The initial (y, x) plane, or (psi, y, x) block for rectangle contact,
+    as the reference GPU solve builds it (gpu_relative.py:165-175): centre
+    distance minus the capture radius, or the oriented-rectangle separation
+    of an evader at (x, y, psi) from a pursuer at the origin; beyond the
+    local exit the value is the exit radius."""
+    n = grid.positions
+    dx = 2 * grid.extent / (n - 1)
+    coord = -grid.extent + np.arange(n) * dx
+    plane = (np.hypot(coord[:, None], coord[None, :]) - config.capture_radius).astype(np.float32)
+    xx, yy = np.meshgrid(coord, coord)
+    if capture_footprints is not None:
+        from ..local_game.geometry import rectangle_separation
+
+        psi = grid.axes(config)[2]
+        other = np.zeros((grid.headings, n, n, 4))
+        other[..., 0], other[..., 1], other[..., 2] = xx, yy, psi[:, None, None]
+        plane = rectangle_separation(np.zeros(4), other, *capture_footprints).astype(np.float32)
+    if exit_radius is not None:
+        plane = np.where(xx * xx + yy * yy > exit_radius ** 2, exit_radius,
+                         plane).astype(np.float32)
+    return plane
+
+
+def probe_stencils(config, grid, probes):
+    """Validated probe states and their 32-corner multilinear stencils over
+    the dense storage order (gpu_relative.py:178-214): positions and speeds
+    clamp the cell to the last interval, headings wrap.  Returns (states,
+    indices [n, 32] int64, weights [n, 32] float64)."""
+    states = np.asarray(probes, dtype=float)
+    if (states.ndim != 2 or states.shape[1] != 5 or len(states) > 100000
+            or not np.isfinite(states).all()):
+        raise ValueError("Probes must be finite relative states[n,5]")
+    shape = tuple(grid.shape)
+    axes = grid.axes(config)
+    corner = (np.arange(32)[:, None] >> np.arange(4, -1, -1)[None, :]) & 1  # [32, 5]
+    stride = np.ones(5, np.int64)
+    for k in range(3, -1, -1):
+        stride[k] = stride[k + 1] * shape[k + 1]
+    indices = np.zeros((len(states), 32), np.int64)
+    weights = np.ones((len(states), 32))
+    storage = states[:, [3, 4, 2, 1, 0]]  # (vP, vE, psi, y, x)
+    for k in range(5):
+        axis, n = np.asarray(axes[k], dtype=float), shape[k]
+        step = axis[1] - axis[0]
+        q = storage[:, k]
+        if k == 2:
+            f = np.mod(q + np.pi, 2 * np.pi) / step
+            cell = np.floor(f).astype(np.int64) % n
+            frac = f - np.floor(f)
+        else:
+            if np.any((q < axis[0]) | (q > axis[-1])):
+                raise ValueError("A probe lies outside the grid")
+            f = (q - axis[0]) / step
+            cell = np.minimum(np.floor(f).astype(np.int64), n - 2)
+            frac = f - cell
+        node = cell[:, None] + corner[None, :, k]
+        if k == 2:
+            node %= n
+        indices += node * stride[k]
+        weights *= np.where(corner[None, :, k] == 1, frac[:, None], 1 - frac[:, None])
+    return states, indices, weights
+
+
+def _run(solver, output, times, *, history, tol, save_final, probe=None):
     """Frame loop: advance to each output time, save the frame, log progress."""
     N = solver.cells
     host = np.empty(N, np.float32)
     write_seconds = update_seconds = transfer_seconds = 0.0
+    probe_seconds = 0.0
+    probe_file = (output / "probes.f64").open("wb") if probe is not None else None
+
+    def save_probes():
+        nonlocal probe_seconds
+        if probe_file is not None:
+            t0 = time.perf_counter()
+            solver.probe(*probe).tofile(probe_file)
+            probe_file.flush()
+            probe_seconds += time.perf_counter() - t0
+
     frames = 1
     converged_time = None
     kept_times = [float(times[0])]
@@ -330,6 +439,7 @@ def _run(solver, output, times, *, history, tol, save_final):
     progress = (output / "progress.jsonl").open("w")
     started = time.perf_counter()
     try:
+        save_probes()
         if history_file:
             writer = _HistoryWriter(solver, history_file, N)
             writer.submit()  # frame 0: the initial field
@@ -345,6 +455,7 @@ def _run(solver, output, times, *, history, tol, save_final):
             kept_times.append(float(solver.time if converged_time else goal))
             if writer:
                 writer.submit()
+            save_probes()
             if index % 5 == 0 or index == len(times) - 1 or converged_time:
                 resolved = int(np.isfinite(solver.arrival()).sum())
                 row = dict(time=kept_times[-1], steps=solver.steps,
@@ -365,6 +476,8 @@ def _run(solver, output, times, *, history, tol, save_final):
         finally:
             if history_file:
                 history_file.close()
+            if probe_file:
+                probe_file.close()
             log.close()
             progress.close()
     final_write = 0.0
@@ -384,6 +497,7 @@ def _run(solver, output, times, *, history, tol, save_final):
         "device_to_host_seconds": transfer_seconds,
         "history_write_seconds": write_seconds,
         "final_write_seconds": final_write,
+        "probe_seconds": probe_seconds,
         "elapsed_seconds": time.perf_counter() - started,
         "maximum_increase": increase,
         "last_step_residual": residual,

@@ -110,6 +110,37 @@ class RelativeSolver:
         _native.check(self._lib.pe_relative_init(self._h, ptr_i, ptr_a,
                                                  float(start_time)))
 
+    def initialize_plane(self, plane, start_time=0.0):
+        """Field = `plane` repeated over the outer axes (gpu_relative.py:42-45):
+        a (y, x) plane or a (psi, y, x) block in storage order."""
+        plane = np.ascontiguousarray(plane, dtype=np.float32).reshape(-1)
+        _native.check(self._lib.pe_relative_init_plane(self._h, plane.ctypes.data,
+                                                       plane.size, float(start_time)))
+
+    def set_exit(self, radius):
+        """Local exit (gpu_relative.py:96-101): cells with x^2 + y^2 > radius^2
+        are held at `radius` and never arrive.  The reference bakes radius^2
+        and radius into its kernel as 10-significant-digit literals; the same
+        rounded numbers are passed here.  None disables the exit."""
+        if radius is None:
+            r = r2 = 0.0
+        else:
+            radius = float(radius)
+            r, r2 = float(f"{radius:.9e}"), float(f"{radius ** 2:.9e}")
+        _native.check(self._lib.pe_relative_set_exit(self._h, r, r2))
+
+    def probe(self, indices, weights):
+        """sum_k weights[i, k] * field[indices[i, k]] over 32-corner stencils
+        (dense storage-order indices), summed in double on the device."""
+        indices = np.ascontiguousarray(indices, dtype=np.int64)
+        weights = np.ascontiguousarray(weights, dtype=np.float64)
+        if indices.ndim != 2 or indices.shape[1] != 32 or weights.shape != indices.shape:
+            raise ValueError("probe stencils must be [n, 32] index and weight arrays")
+        out = np.empty(len(indices), np.float64)
+        _native.check(self._lib.pe_relative_probe(self._h, len(indices), indices.ctypes.data,
+                                                  weights.ctypes.data, out.ctypes.data))
+        return out
+
     def set_stream(self, stream_ptr):
         _native.check(self._lib.pe_relative_set_stream(self._h, stream_ptr))
 
