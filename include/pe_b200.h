@@ -394,6 +394,14 @@ int pe_semilag_get_tile(const pe_semilag *h, int32_t *rows, int32_t *threads,
 int pe_semilag_kernel(const pe_semilag *h, int32_t *kernel);
 int pe_semilag_profile(pe_semilag *h, int enable);
 int pe_semilag_kernel_time(pe_semilag *h, double *total_ms, int64_t *launches);
+/* Arrival times of the tube field (PE_SL_TUBE only), as the ENO/LF path
+ * keeps them (native_relative.cpp:167-168): after every backup from the
+ * start time t, a cell whose value went from > 0 to <= 0 for the first time
+ * gets t + dt * prev / (prev - value).  host_arrival != NULL continues an
+ * earlier record (N floats, NaN = not arrived); NULL starts one: start_time
+ * where the current value is <= 0, NaN elsewhere. */
+int pe_semilag_track_arrival(pe_semilag *h, const float *host_arrival, double start_time);
+int pe_semilag_copy_arrival(pe_semilag *h, float *host_arrival);
 int pe_semilag_destroy(pe_semilag *h);
 
 /* ------------------------------------------------------------------------

@@ -34,6 +34,8 @@ struct pe_semilag {
   cudaStream_t own = nullptr, stream = nullptr;
   int64_t iterations = 0;
   bool initialized = false, policy_valid = false;
+  float *arrival = nullptr;  // first-crossing times (tube mode, when tracked)
+  double time = 0;           // start time of the next backup, for the arrival
   pe::LaunchTimer timer;  // launch times (profile / kernel_time)
 };
 
@@ -153,7 +155,7 @@ void release(pe_semilag *h) {
   for (void *ptr : {(void *)h->a, (void *)h->b, (void *)h->plane, (void *)h->pol_p,
                     (void *)h->pol_e, (void *)h->parc, (void *)h->earc,
                     (void *)h->emove, (void *)h->stats, (void *)h->pstep,
-                    (void *)h->estep, (void *)h->hint})
+                    (void *)h->estep, (void *)h->hint, (void *)h->arrival})
     cudaFree(ptr);
   if (h->host_stats) cudaFreeHost(h->host_stats);
   if (h->own) cudaStreamDestroy(h->own);
@@ -209,6 +211,11 @@ int backup(pe_semilag *h, bool policy) {
     if (rc) return rc;
   }
   std::swap(h->a, h->b);
+  if (h->arrival) {
+    PE_CUDA_TRY(pe::sl_arrival(h->g, h->b, h->a, h->arrival, h->time, h->dt, h->stream));
+    pe::count_launches(1);
+  }
+  h->time += h->dt;
   h->iterations++;
   h->policy_valid = policy;
   return PE_OK;
@@ -555,6 +562,38 @@ int pe_semilag_kernel_time(pe_semilag *h, double *total_ms, int64_t *launches) {
   if (rc) return rc;
   if (total_ms) *total_ms = h->timer.ms(0);
   if (launches) *launches = h->timer.launches(0);
+  return PE_OK;
+}
+
+int pe_semilag_track_arrival(pe_semilag *h, const float *host_arrival, double start_time) {
+  int rc = enter(h);
+  if (rc) return rc;
+  if (h->p.mode != PE_SL_TUBE) return fail(PE_EINVAL, "arrival times need the tube mode");
+  if (!h->initialized) return fail(PE_ESTATE, "track_arrival before init");
+  if (!std::isfinite(start_time)) return fail(PE_EINVAL, "start_time must be finite");
+  const size_t bytes = sizeof(float) * (size_t)h->g.n;
+  if (!h->arrival) PE_CUDA_TRY(cudaMalloc(&h->arrival, bytes));
+  if (host_arrival) {
+    PE_CUDA_TRY(cudaMemcpyAsync(h->arrival, host_arrival, bytes, cudaMemcpyHostToDevice,
+                                h->stream));
+  } else {
+    // arrival = start_time where the value is <= 0, NaN elsewhere
+    PE_CUDA_TRY(pe::sl_arrival_start(h->g, h->a, h->arrival, start_time, h->stream));
+    pe::count_launches(1);
+  }
+  PE_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  h->time = start_time;
+  return PE_OK;
+}
+
+int pe_semilag_copy_arrival(pe_semilag *h, float *host_arrival) {
+  int rc = enter(h);
+  if (rc) return rc;
+  if (!host_arrival) return fail(PE_EINVAL, "host_arrival is NULL");
+  if (!h->arrival) return fail(PE_ESTATE, "arrival is not tracked");
+  PE_CUDA_TRY(cudaMemcpyAsync(host_arrival, h->arrival, sizeof(float) * (size_t)h->g.n,
+                              cudaMemcpyDeviceToHost, h->stream));
+  PE_CUDA_TRY(cudaStreamSynchronize(h->stream));
   return PE_OK;
 }
 

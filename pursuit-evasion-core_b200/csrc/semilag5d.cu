@@ -191,6 +191,35 @@ cudaError_t sl_backup(const SLGrid &g, const SLBackup &b, cudaStream_t stream) {
   return cudaGetLastError();
 }
 
+__global__ void sl_arrival_kernel(const float *__restrict__ prev, const float *__restrict__ cur,
+                                  float *__restrict__ arrival, int64_t n, double t, double dt) {
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n;
+       j += (int64_t)gridDim.x * blockDim.x) {
+    const float p = prev[j], v = cur[j];
+    if (p > 0.f && v <= 0.f && isnan(arrival[j]))
+      arrival[j] = (float)(t + dt * (double)p / ((double)p - (double)v));
+  }
+}
+
+cudaError_t sl_arrival(const SLGrid &g, const float *prev, const float *cur, float *arrival,
+                       double t, double dt, cudaStream_t stream) {
+  sl_arrival_kernel<<<148 * 8, 256, 0, stream>>>(prev, cur, arrival, g.n, t, dt);
+  return cudaGetLastError();
+}
+
+__global__ void sl_arrival_start_kernel(const float *__restrict__ cur,
+                                        float *__restrict__ arrival, int64_t n, float t) {
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n;
+       j += (int64_t)gridDim.x * blockDim.x)
+    arrival[j] = cur[j] <= 0.f ? t : __int_as_float(0x7fc00000);
+}
+
+cudaError_t sl_arrival_start(const SLGrid &g, const float *cur, float *arrival,
+                             double start_time, cudaStream_t stream) {
+  sl_arrival_start_kernel<<<148 * 8, 256, 0, stream>>>(cur, arrival, g.n, (float)start_time);
+  return cudaGetLastError();
+}
+
 cudaError_t sl_init(const SLGrid &g, const float *plane, float *field,
                     cudaStream_t stream) {
   sl_init_kernel<<<148 * 16, 256, 0, stream>>>(plane, field, g.n, g.nx * g.nx);

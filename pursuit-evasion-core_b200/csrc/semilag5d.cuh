@@ -90,6 +90,15 @@ cudaError_t sl_backup_tiled(const SLGrid &g, const SLBackup &b, const SLTiled &t
 
 // Initial field: TUBE hypot(x, y) - radius; MINTIME 0 inside the capture
 // disk and 1 elsewhere.  plane: dense (y, x) values computed on the host.
+// First crossing of zero between two tube values (the arrival rule of the
+// ENO/LF path, native_relative.cpp:167-168): where prev > 0 >= cur and the
+// arrival is still NaN, arrival = t + dt * prev / (prev - cur).
+cudaError_t sl_arrival(const SLGrid &g, const float *prev, const float *cur, float *arrival,
+                       double t, double dt, cudaStream_t stream);
+// arrival = start_time where cur <= 0, NaN elsewhere.
+cudaError_t sl_arrival_start(const SLGrid &g, const float *cur, float *arrival,
+                             double start_time, cudaStream_t stream);
+
 cudaError_t sl_init(const SLGrid &g, const float *plane, float *field,
                     cudaStream_t stream);
 

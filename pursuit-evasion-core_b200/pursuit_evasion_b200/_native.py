@@ -293,6 +293,8 @@ SIGNATURES = {
                                            ctypes.POINTER(ctypes.c_int32), _I64P]),
     "pe_semilag_profile": (ctypes.c_int, [_P, ctypes.c_int]),
     "pe_semilag_kernel_time": (ctypes.c_int, [_P, _DP, _I64P]),
+    "pe_semilag_track_arrival": (ctypes.c_int, [_P, _P, ctypes.c_double]),
+    "pe_semilag_copy_arrival": (ctypes.c_int, [_P, _P]),
     "pe_semilag_destroy": (ctypes.c_int, [_P]),
     "pe_mlp_gemm": (ctypes.c_int, [_P, _P] + [ctypes.c_int] * 9 + [_P, _P, ctypes.c_int,
                                                                    _P, _P, _P]),

@@ -44,12 +44,14 @@ def _device_name(device):
     return torch.cuda.get_device_name(device)
 
 
-def candidates(narrowest, local_precision="float64"):
-    """Row counts to try for a bucket whose narrowest grid has `narrowest`
-    positions: exact kernel, those that give every thread of a 256-thread
-    CTA a cell; tiled float32 kernel, those up to the CTA's capacity."""
+def candidates(narrowest, local_precision="float64", widest=None):
+    """Row counts to try for a bucket whose grids have `narrowest` to
+    `widest` positions: exact kernel, those that give every thread of a
+    256-thread CTA a cell; tiled float32 kernel, those up to the capacity of
+    a CTA on the widest grid (one 4-cell chunk per thread)."""
     if local_precision == "float32":
-        cap = min(narrowest, 256 // ((narrowest + 3) // 4))
+        widest = narrowest if widest is None else max(widest, narrowest)
+        cap = min(narrowest, 256 // ((widest + 3) // 4))
         return sorted({min(r, cap) for r in CANDIDATE_ROWS if r <= narrowest} | {cap})
     rows = [r for r in CANDIDATE_ROWS if r <= narrowest and r * narrowest >= 256]
     return rows or [narrowest]
@@ -82,7 +84,8 @@ def tune(solves, *, device=0, local_precision="float32", per_bucket=6, trial_ste
             limits = [probe.info(i)["dt_limit"] for i in range(len(sample))]
         trial = [replace(s, horizon=trial_steps * lim) for s, lim in zip(sample, limits)]
         with BatchSolver(trial, local_precision=local_precision, device=device) as b:
-            for rows in candidates(min(s.grid.positions for s in trial), local_precision):
+            widths = [s.grid.positions for s in members]
+            for rows in candidates(min(widths), local_precision, max(widths)):
                 for i in range(len(trial)):
                     b.set_tile(i, rows)
                 best = None

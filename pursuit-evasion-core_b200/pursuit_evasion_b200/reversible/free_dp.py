@@ -154,6 +154,7 @@ def solve(
     probes=None,
     capture_footprints=None,
     exit_radius=None,
+    scheme="eno_lf",
 ):
     """Compute a new relative table directory on the GPU.
 
@@ -171,6 +172,16 @@ def solve(
     vP, vE) whose multilinear values are written to probes.f64 after every
     frame.  `warm_start`, when given, replaces the initial field; the exit
     still holds in every stage.
+
+    scheme="semi_lagrangian" fills the same table with the semi-Lagrangian
+    min-max backup (the tube form, V' = min(V, min_u max_w V(successor))):
+    each output interval is split into equal held-command steps no longer
+    than the interpolation CFL step, arrival times follow the same crossing
+    rule, and two extra files hold the optimal pursuer / evader actions of
+    the last backup (policy_p.u8, policy_e.u8: catalogue index
+    3 * acceleration + curvature, each in (-, 0, +) order) and residuals.f64
+    the sup-norm change of each frame's last backup.  It takes no `tol` and
+    no `exit_radius`.
     """
     solve_started = time.perf_counter()
     if config.capture_rule == "rectangle_contact" and capture_footprints is None:
@@ -181,6 +192,10 @@ def solve(
         raise ValueError("Unknown capture rule")
     if exit_radius is not None and not 0 < exit_radius < grid.extent:
         raise ValueError("Local exit radius must lie inside the numerical grid")
+    if scheme not in ("eno_lf", "semi_lagrangian"):
+        raise ValueError("scheme must be 'eno_lf' or 'semi_lagrangian'")
+    if scheme == "semi_lagrangian" and (tol is not None or exit_radius is not None):
+        raise ValueError("tol and exit_radius apply to scheme='eno_lf' only")
     _validate(config, grid, horizon, output_dt, order, cfl, threads)
     if (not np.isfinite([max_working_gb, disk_reserve_gb]).all()
             or max_working_gb <= 0 or disk_reserve_gb < 0):
@@ -194,12 +209,13 @@ def solve(
         raise FileExistsError(f"Preserve existing output: {output}")
     times = output_times(horizon, output_dt)
     N = grid.states
-    working = N * 12
+    working = N * (15 if scheme == "semi_lagrangian" else 12)
     probe_states = probe_indices = probe_weights = None
     if probes is not None:
         probe_states, probe_indices, probe_weights = probe_stencils(config, grid, probes)
     storage = N * 4 * ((2 if save_final else 0) + (len(times) if history else 0)) + (
-        0 if probe_states is None else 8 * len(probe_states) * len(times))
+        0 if probe_states is None else 8 * len(probe_states) * len(times)) + (
+        2 * N if scheme == "semi_lagrangian" else 0)
     if working > max_working_gb * 1e9:
         raise MemoryError(
             f"Core arrays need {working / 1e9:.3f} GB, above guard {max_working_gb}"
@@ -217,6 +233,15 @@ def solve(
         if initial.size != N or not np.isfinite(initial).all():
             raise ValueError("warm_start must be a finite field of grid.states cells")
 
+    if scheme == "semi_lagrangian":
+        return _solve_semilag(config, grid, output, times, initial, history=history,
+                              save_final=save_final, capture_footprints=capture_footprints,
+                              probe_states=probe_states,
+                              probe=None if probe_states is None else
+                              (probe_indices, probe_weights),
+                              device=device, working=working, storage=storage,
+                              solve_started=solve_started, horizon=horizon,
+                              output_dt=output_dt)
     alloc_started = time.perf_counter()
     solver = RelativeSolver(config, grid, order=order, cfl=cfl,
                             local_precision=local_precision, device=device)
@@ -249,6 +274,7 @@ def solve(
             "history_saved": bool(history),
             "dtype": "float32",
             "target": "physical_capture_only",
+            "scheme": "eno_lf",
             "capture_rule": config.capture_rule,
             "capture_footprints": None if capture_footprints is None else {
                 "pursuer": capture_footprints[0].to_dict(),
@@ -348,6 +374,171 @@ class _HistoryWriter:
             b.close()
         if self.error is not None:
             raise self.error
+
+
+def _solve_semilag(config, grid, output, times, initial, *, history, save_final,
+                   capture_footprints, probe_states, probe, device, working, storage,
+                   solve_started, horizon, output_dt):
+    """The table of free_dp.solve from the semi-Lagrangian tube backup."""
+    from .semilag import SemiLagrangianSolver, interpolation_cfl_dt
+
+    limit = interpolation_cfl_dt(config, grid)
+    N = grid.states
+    warm = initial is not None
+    if initial is None:
+        plane = capture_plane(config, grid, capture_footprints)
+        initial = np.ascontiguousarray(np.broadcast_to(plane, grid.shape)).reshape(-1)
+    output.mkdir(exist_ok=True)
+    meta = {"schema": SCHEMA, "status": "running"}
+    solver = None
+    files = []
+    try:
+        alloc_started = time.perf_counter()
+
+        def make(length):
+            steps = max(1, int(math.ceil(length / limit - 1e-9)))
+            return SemiLagrangianSolver(config, grid, dt=length / steps, mode="tube",
+                                        device=device), steps
+
+        solver, per_frame = make(output_dt)
+        segment = output_dt
+        solver.initialize(initial)
+        solver.track_arrival(start_time=0.0)
+        allocation_seconds = time.perf_counter() - alloc_started
+        meta.update({
+            "schema": SCHEMA,
+            "backend": "b200_cuda",
+            "scheme": "semi_lagrangian",
+            "local_precision": "float32",
+            "config": config_dict(config),
+            "physics": physics_signature(config),
+            "grid": grid.to_dict(),
+            "shape": list(grid.shape),
+            "state_order": ["x", "y", "psi", "vP", "vE"],
+            "axis_order": ["vP", "vE", "psi", "y", "x"],
+            "axes": [a.tolist() for a in grid.axes(config)],
+            "horizon": horizon,
+            "output_dt": output_dt,
+            "times": times.tolist(),
+            "history_saved": bool(history),
+            "dtype": "float32",
+            "target": "physical_capture_only",
+            "capture_rule": config.capture_rule,
+            "capture_footprints": None if capture_footprints is None else {
+                "pursuer": capture_footprints[0].to_dict(),
+                "evader": capture_footprints[1].to_dict()},
+            "local_exit_radius": None,
+            "avoid": None,
+            "tube_projection": "min over every internal update",
+            "position_boundary": "successors interpolated inside the grid, clamped at its edges",
+            "speed_boundary": "speed saturates at its limits along the held command",
+            "heading_boundary": "periodic",
+            "interpolation_cfl_dt": limit,
+            "policy_files": ["policy_p.u8", "policy_e.u8"],
+            "policy_catalogue": "3 * i_acceleration + i_curvature, each index over (-, 0, +)",
+            "source_sha256": _source_digest(),
+            "warm_start": warm,
+            "predicted_working_bytes": working,
+            "predicted_output_bytes": storage,
+            "device": int(device),
+            "status": "running",
+            "probe_states": None if probe_states is None else probe_states.tolist(),
+        })
+        (output / "meta.json").write_text(json.dumps(meta, indent=2) + "\n")
+        host = np.empty(N, np.float32)
+        history_file = (output / "fields.f32").open("wb") if history else None
+        probe_file = (output / "probes.f64").open("wb") if probe is not None else None
+        files = [f for f in (history_file, probe_file) if f is not None]
+        residuals = []
+        update_seconds = transfer_seconds = write_seconds = 0.0
+        started = time.perf_counter()
+
+        def save_frame():
+            nonlocal transfer_seconds, write_seconds
+            if history_file is None and probe_file is None:
+                return
+            t0 = time.perf_counter()
+            solver.value(host)
+            t1 = time.perf_counter()
+            transfer_seconds += t1 - t0
+            if history_file is not None:
+                host.tofile(history_file)
+            if probe_file is not None:
+                (host[probe[0]].astype(np.float64) * probe[1]).sum(1).tofile(probe_file)
+                probe_file.flush()
+            write_seconds += time.perf_counter() - t1
+
+        save_frame()
+        steps = 0
+        with (output / "progress.jsonl").open("w") as progress:
+            for index, goal in enumerate(times[1:], start=1):
+                length = float(goal - times[index - 1])
+                if abs(length - segment) > 1e-9 * max(1.0, segment):
+                    # a shorter last interval: continue on a solver with its step
+                    nxt, per_frame = make(length)
+                    nxt.initialize_device(solver.device_value_ptr())
+                    nxt.track_arrival(solver.arrival(), start_time=float(times[index - 1]))
+                    solver.close()
+                    solver, segment = nxt, length
+                t0 = time.perf_counter()
+                last = index == len(times) - 1
+                for k in range(per_frame):
+                    solver.backup(with_policy=last and k == per_frame - 1)
+                residuals.append(solver.residual())
+                update_seconds += time.perf_counter() - t0
+                steps += per_frame
+                save_frame()
+                if index % 5 == 0 or last:
+                    resolved = int(np.isfinite(solver.arrival()).sum())
+                    progress.write(json.dumps(dict(
+                        time=float(goal), steps=steps, resolved=resolved,
+                        elapsed_seconds=time.perf_counter() - started)) + "\n")
+                    progress.flush()
+        for f in files:
+            f.close()
+        files = []
+        (output / "solver.log").write_text(
+            f"semi_lagrangian steps={steps} frames={len(times)}\n")
+        np.asarray(residuals, np.float64).tofile(output / "residuals.f64")
+        t0 = time.perf_counter()
+        if save_final:
+            solver.value(host).tofile(output / "final.f32")
+            solver.arrival(host).tofile(output / "arrival.f32")
+        if len(times) > 1:
+            pol_p, pol_e = solver.policy()
+            np.ascontiguousarray(pol_p, np.uint8).tofile(output / "policy_p.u8")
+            np.ascontiguousarray(pol_e, np.uint8).tofile(output / "policy_e.u8")
+        final_write = time.perf_counter() - t0
+        timing = {
+            "states": N,
+            "working_array_bytes": working,
+            "step_dt": solver.dt,
+            "internal_steps": steps,
+            "frames": len(times),
+            "update_seconds": update_seconds,
+            "device_to_host_seconds": transfer_seconds,
+            "history_write_seconds": write_seconds,
+            "final_write_seconds": final_write,
+            "elapsed_seconds": time.perf_counter() - started,
+            "last_step_residual": residuals[-1] if residuals else 0.0,
+            "cell_backups_per_second": N * steps / max(update_seconds, 1e-12),
+        }
+        (output / "timing.json").write_text(json.dumps(timing) + "\n")
+        meta.update(timing)
+        meta["allocation_seconds"] = allocation_seconds
+        meta["status"] = "complete"
+    except Exception as exc:
+        meta.update(status="failed", failure=str(exc))
+        (output / "meta.json").write_text(json.dumps(meta, indent=2) + "\n")
+        raise RuntimeError(f"Relative solve failed: {exc}") from exc
+    finally:
+        for f in files:
+            f.close()
+        if solver is not None:
+            solver.close()
+    meta["total_wall_seconds"] = time.perf_counter() - solve_started
+    (output / "meta.json").write_text(json.dumps(meta, indent=2) + "\n")
+    return meta
 
 
 def capture_plane(config, grid, capture_footprints=None, exit_radius=None):

@@ -99,6 +99,23 @@ class SemiLagrangianSolver:
         """Initialise from a dense float32 field already on this device."""
         _native.check(self._lib.pe_semilag_init_device(self._h, ctypes.c_void_p(device_ptr)))
 
+    def track_arrival(self, arrival=None, start_time=0.0):
+        """Keep first-crossing times of the tube field from now on: a new
+        record (start_time where the value is <= 0) or `arrival` continued."""
+        ptr = None
+        if arrival is not None:
+            arrival = np.ascontiguousarray(arrival, dtype=np.float32).reshape(-1)
+            if arrival.size != self.cells:
+                raise ValueError("arrival has the wrong number of cells")
+            ptr = arrival.ctypes.data
+        _native.check(self._lib.pe_semilag_track_arrival(self._h, ptr, float(start_time)))
+
+    def arrival(self, out=None):
+        if out is None:
+            out = np.empty(self.cells, np.float32)
+        _native.check(self._lib.pe_semilag_copy_arrival(self._h, out.ctypes.data))
+        return out.reshape(self.shape)
+
     def backup(self, with_policy=False):
         _native.check(self._lib.pe_semilag_backup(self._h, int(with_policy)))
 

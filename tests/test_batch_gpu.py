@@ -124,9 +124,9 @@ def test_autotuner_picks_a_tile_per_bucket(tmp_path):
                           cache=tmp_path / "tiles.json")
     assert set(tiles) == {autotune.bucket_of(s.grid.positions) for s in solves}
     for bucket, rows in tiles.items():
-        narrowest = min(s.grid.positions for s in solves
-                        if autotune.bucket_of(s.grid.positions) == bucket)
-        assert rows in autotune.candidates(narrowest, "float32")
+        widths = [s.grid.positions for s in solves
+                  if autotune.bucket_of(s.grid.positions) == bucket]
+        assert rows in autotune.candidates(min(widths), "float32", max(widths))
     assert (tmp_path / "tiles.json").exists()
     with BatchSolver(solves[:2], local_precision="float32") as b:
         autotune.apply(b, tiles)

@@ -42,6 +42,9 @@ def test_buckets_and_candidates():
         assert tiled and all(1 <= r <= n and r * ((n + 3) // 4) <= 256 for r in tiled)
     assert autotune.candidates(17) == [16]
     assert autotune.candidates(49, "float32")[-1] == 19
+    # a bucket of 34- to 40-wide grids: every candidate fits a 40-wide CTA
+    assert autotune.candidates(34, "float32", 40)[-1] == 25
+    assert max(autotune.candidates(34, "float32", 40)) * 10 <= 256
 
 
 @pytest.mark.parametrize("field, value", [("order", 1), ("precision", _native.PE_LOCAL_F32),

@@ -125,3 +125,14 @@ def test_solve_refuses_bad_keywords_before_any_work(tmp_path):
     with pytest.raises(ValueError, match="Probes"):
         solve(A3, CONFIG1_GRID, out, probes=np.zeros((2, 4)))
     assert not out.exists()
+
+
+def test_solve_refuses_unknown_scheme_and_semi_lagrangian_extras(tmp_path):
+    out = tmp_path / "t"
+    with pytest.raises(ValueError, match="scheme"):
+        solve(A3, CONFIG1_GRID, out, scheme="weno")
+    with pytest.raises(ValueError, match="eno_lf"):
+        solve(A3, CONFIG1_GRID, out, scheme="semi_lagrangian", tol=1e-3)
+    with pytest.raises(ValueError, match="eno_lf"):
+        solve(A3, CONFIG1_GRID, out, scheme="semi_lagrangian", exit_radius=2.0)
+    assert not out.exists()
