@@ -212,6 +212,46 @@ int pe_relative_step_noalloc(const pe_relative_params *params,
                              void *cuda_stream, double *residual);
 
 /* ------------------------------------------------------------------------
+ * vP-slab shards of one relative 5D solve (grids larger than one GPU).
+ *
+ * The reference solves one grid in one process (native_relative.cpp:173-190
+ * step loop, run by free_dp.py:259-261); a shard runs the same exact stage
+ * (bit-identical per cell) over global vP slabs [vp_begin, vp_end) of that
+ * grid.  It holds `order` halo slabs on each side that has a neighbour
+ * (the ENO stencil along vP reaches `order` slabs); after every stage the
+ * caller copies the neighbours' edge slabs of the buffer just written
+ * (pe_relative_shard_buffer, padded layout, slab k of the buffer at
+ * (k - lo) * slab_floats floats) into those halos: peer copies or NCCL
+ * send/recv on the shard's stream.  Only PE_LOCAL_F64 precision.
+ * ------------------------------------------------------------------------ */
+typedef struct pe_relative_shard pe_relative_shard;
+
+int pe_relative_shard_create(const pe_relative_params *params, int32_t vp_begin,
+                             int32_t vp_end, pe_relative_shard **out);
+/* slabs[4] = {lo, hi, own_lo, own_hi}: buffer slabs [lo, hi) (owned plus
+ * halos) and owned slabs, global vP indices; slab_floats = padded floats
+ * of one slab. */
+int pe_relative_shard_layout(const pe_relative_shard *h, int32_t *slabs,
+                             int64_t *slab_floats);
+int pe_relative_shard_set_stream(pe_relative_shard *h, void *cuda_stream);
+/* initial = NULL: the circular capture field; else the dense values of
+ * buffer slabs [lo, hi) (host).  Arrival = start_time where <= 0. */
+int pe_relative_shard_init(pe_relative_shard *h, const float *initial, double start_time);
+/* Stage 0 (and, for order 2, stage 1) of one step of size dt; the step's
+ * time advances after its last stage. */
+int pe_relative_shard_stage(pe_relative_shard *h, int32_t stage, double dt);
+/* The device buffer the last stage wrote (the field before any stage). */
+int pe_relative_shard_buffer(const pe_relative_shard *h, float **device_buffer);
+/* Owned slabs of the field / arrival, dense, to host. */
+int pe_relative_shard_copy_field(pe_relative_shard *h, float *host_owned);
+int pe_relative_shard_copy_arrival(pe_relative_shard *h, float *host_owned);
+/* Sup-norm change of the owned cells in the last step, and the largest
+ * increase; combine over shards with a maximum. */
+int pe_relative_shard_stats(pe_relative_shard *h, double *residual, double *increase);
+int pe_relative_shard_synchronize(pe_relative_shard *h);
+int pe_relative_shard_destroy(pe_relative_shard *h);
+
+/* ------------------------------------------------------------------------
  * Batched relative 5D solves.
  *
  * Many independent free_dp-style solves -- each with its own RelativeGrid,

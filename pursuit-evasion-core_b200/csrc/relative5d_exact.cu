@@ -21,8 +21,8 @@ __global__ void __launch_bounds__(128)
   if (cell < g.nx * g.nx) {
     const int ix = cell % g.nx, iy = cell / g.nx;
     const int ip = blockIdx.y;
-    const int ie = blockIdx.z % g.nve, iv = blockIdx.z / g.nve;
-    const int64_t j = (int64_t)blockIdx.z * g.se + (int64_t)ip * g.sp +
+    const int ie = blockIdx.z % g.nve, iv = g.own_lo + (int)blockIdx.z / g.nve;
+    const int64_t j = ((int64_t)(iv - g.slab_lo) * g.nve + ie) * g.se + (int64_t)ip * g.sp +
                       (int64_t)iy * g.sy + ix;
     exact::cell_update<ORDER, BLEND>(g, s, ix, iy, ip, iv, ie, j, change_abs, change_up,
                                      bad);
@@ -44,7 +44,8 @@ __global__ void __launch_bounds__(128)
 cudaError_t rel5_stage_f64(const Rel5Grid &g, const Rel5Stage &s, int blend,
                            cudaStream_t stream) {
   const int threads = 128;
-  const dim3 grid((g.nx * g.nx + threads - 1) / threads, g.nh, g.nvp * g.nve);
+  const int slabs = g.own_n > 0 ? g.own_n : g.nvp;
+  const dim3 grid((g.nx * g.nx + threads - 1) / threads, g.nh, slabs * g.nve);
   if (g.order == 1)
     rel5_stage_exact_kernel<1, 0><<<grid, threads, 0, stream>>>(g, s);
   else if (blend)

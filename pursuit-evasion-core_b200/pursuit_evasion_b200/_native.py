@@ -293,6 +293,17 @@ SIGNATURES = {
                                            ctypes.POINTER(ctypes.c_int32), _I64P]),
     "pe_semilag_profile": (ctypes.c_int, [_P, ctypes.c_int]),
     "pe_semilag_kernel_time": (ctypes.c_int, [_P, _DP, _I64P]),
+    "pe_relative_shard_create": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32, _P]),
+    "pe_relative_shard_layout": (ctypes.c_int, [_P, _P, _P]),
+    "pe_relative_shard_set_stream": (ctypes.c_int, [_P, _P]),
+    "pe_relative_shard_init": (ctypes.c_int, [_P, _P, ctypes.c_double]),
+    "pe_relative_shard_stage": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_double]),
+    "pe_relative_shard_buffer": (ctypes.c_int, [_P, _P]),
+    "pe_relative_shard_copy_field": (ctypes.c_int, [_P, _P]),
+    "pe_relative_shard_copy_arrival": (ctypes.c_int, [_P, _P]),
+    "pe_relative_shard_stats": (ctypes.c_int, [_P, _P, _P]),
+    "pe_relative_shard_synchronize": (ctypes.c_int, [_P]),
+    "pe_relative_shard_destroy": (ctypes.c_int, [_P]),
     "pe_semilag_track_arrival": (ctypes.c_int, [_P, _P, ctypes.c_double]),
     "pe_semilag_copy_arrival": (ctypes.c_int, [_P, _P]),
     "pe_semilag_destroy": (ctypes.c_int, [_P]),
