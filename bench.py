@@ -277,12 +277,26 @@ def run_reference_arm(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def _timing_stream():
+    """The current torch stream when it is a created one; else a new stream
+    made current.  The solver handles read stream 0 as their own stream, so
+    events recorded on the legacy default stream would not bracket their
+    kernels."""
+    import torch
+
+    stream = torch.cuda.current_stream()
+    if stream.cuda_stream == 0:
+        stream = torch.cuda.Stream()
+        torch.cuda.set_stream(stream)
+    return stream
+
+
 def _world8d_run(grid, steps, fast):
     import torch
     from pursuit_evasion_b200.reversible.world_dp import WorldSolver
 
     with WorldSolver(a3_config(), grid, avoid=False, fast=fast) as s:
-        stream = torch.cuda.current_stream()
+        stream = _timing_stream()
         s.set_stream(stream.cuda_stream)
         s.init_contact((0.5, 0.3), (0.5, 0.3))
         for _ in range(3):
@@ -361,7 +375,7 @@ def semilag_section(with_cpu=True):
 
     grid = RelativeGrid(**GRID)
     with SemiLagrangianSolver(a3_config(), grid, mode="tube") as s:
-        stream = torch.cuda.current_stream()
+        stream = _timing_stream()
         s.set_stream(stream.cuda_stream)
         backups = math.ceil(HORIZON / s.dt - 1e-9)
         s.initialize()
@@ -428,7 +442,7 @@ def batch_section(seed=0, count=256):
     tiles = autotune.tune(solves, local_precision="float32", per_bucket=4, trial_steps=2,
                           repeats=1)
     with BatchSolver(solves, local_precision="float32") as b:
-        stream = torch.cuda.current_stream()
+        stream = _timing_stream()
         b.set_stream(stream.cuda_stream)
         autotune.apply(b, tiles)
         b.initialize()
@@ -501,7 +515,7 @@ def compact_section(backups=5, with_cpu=True):
     domain = PairDomain.build(p, e, 2.0)
     arena = CircleArena([], 3.25)
     a = packed_gpu_arrays(p, e, domain, max_gb=60)
-    stream = torch.cuda.current_stream()
+    stream = _timing_stream()
     a.set_stream(stream.cuda_stream)
     initialize_packed(a, p, e, domain, arena)
     backup_packed(a, p, e, domain)  # warm-up
@@ -707,7 +721,7 @@ def run_ours(args, world, rank, local):
     cells = grid.states
     solver = RelativeSolver(config, grid, local_precision=args.precision,
                             device=local)
-    stream = torch.cuda.current_stream()
+    stream = _timing_stream()
     solver.set_stream(stream.cuda_stream)
     stages_per_solve = None
 

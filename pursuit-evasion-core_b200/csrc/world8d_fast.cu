@@ -210,8 +210,23 @@ __global__ void __launch_bounds__(kThreads)
     }
     const int64_t j0 = (int64_t)o * inner;
     const float *__restrict__ src_o = s.src + j0;
+    // The pursuer-axis values (the same evader cell in the 16 neighbouring
+    // blocks, from L2 or HBM) of a thread's next cell are loaded while its
+    // current cell is computed, so their latency overlaps the arithmetic.
+    float ahead[16];
+    auto load_pursuer = [&](int e, float v[16]) {
+#pragma unroll
+      for (int k = 0; k < 4; k++)
+#pragma unroll
+        for (int m = 0; m < 4; m++) v[4 * k + m] = __ldg(src_o + poff[k][m] + e);
+    };
+    if (tid < inner) load_pursuer(tid, ahead);
 
     for (int e = tid; e < inner; e += kThreads) {
+      float nbv[16];
+#pragma unroll
+      for (int i = 0; i < 16; i++) nbv[i] = ahead[i];
+      if (e + kThreads < inner) load_pursuer(e + kThreads, ahead);
       int q7, q6, q5;
       int t = split(e, a.d7, q7);
       t = split(t, a.d6, q6);
@@ -221,12 +236,9 @@ __global__ void __launch_bounds__(kThreads)
       // pursuer axes: the same evader cell in the neighbouring blocks
 #pragma unroll
       for (int k = 0; k < 4; k++) {
-        const float m2 = __ldg(src_o + poff[k][0] + e);
-        const float m1 = __ldg(src_o + poff[k][1] + e);
-        const float p1 = __ldg(src_o + poff[k][2] + e);
-        const float p2 = __ldg(src_o + poff[k][3] + e);
         const int kind = k == 2 ? kPeriodic : (k == 3 ? kind_speed : kExtrapolated);
-        axis_slopes<ORDER>(m2, m1, f, p1, p2, qp[k], g.shape[k], kind, dlo[k], dhi[k]);
+        axis_slopes<ORDER>(nbv[4 * k], nbv[4 * k + 1], f, nbv[4 * k + 2], nbv[4 * k + 3],
+                           qp[k], g.shape[k], kind, dlo[k], dhi[k]);
       }
       // evader axes: shared memory
       const int qe[4] = {q4, q5, q6, q7};
