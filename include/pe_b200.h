@@ -215,14 +215,15 @@ int pe_relative_step_noalloc(const pe_relative_params *params,
  * vP-slab shards of one relative 5D solve (grids larger than one GPU).
  *
  * The reference solves one grid in one process (native_relative.cpp:173-190
- * step loop, run by free_dp.py:259-261); a shard runs the same exact stage
+ * step loop, run by free_dp.py:259-261); a shard runs the same stage
  * (bit-identical per cell) over global vP slabs [vp_begin, vp_end) of that
  * grid.  It holds `order` halo slabs on each side that has a neighbour
  * (the ENO stencil along vP reaches `order` slabs); after every stage the
  * caller copies the neighbours' edge slabs of the buffer just written
  * (pe_relative_shard_buffer, padded layout, slab k of the buffer at
  * (k - lo) * slab_floats floats) into those halos: peer copies or NCCL
- * send/recv on the shard's stream.  Only PE_LOCAL_F64 precision.
+ * send/recv on the shard's stream.  Each cell's update is the single-grid
+ * stage's of the same precision (PE_LOCAL_F64 exact, PE_LOCAL_F32 fast).
  * ------------------------------------------------------------------------ */
 typedef struct pe_relative_shard pe_relative_shard;
 

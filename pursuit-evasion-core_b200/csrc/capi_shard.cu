@@ -5,11 +5,12 @@
 // slab of nve * nh * nx * xp floats.  A shard owns global slabs
 // [own_lo, own_hi) and keeps `order` halo slabs on each side that has a
 // neighbour: the ENO stencil along vP reads at most `order` slabs away.
-// Stages run the exact kernel (relative5d_exact.cu) over the owned slabs
-// only, with global vP indices, so the speed boundary rule and the vP
-// values are those of the whole grid.  After each stage the caller refreshes
-// the halo slabs of the buffer just written from the neighbouring shards
-// (peer copies, NCCL send/recv); the handle only exposes that buffer.
+// Stages run the exact kernel (relative5d_exact.cu) or the float32 kernel
+// (relative5d_fast.cu) over the owned slabs only, with global vP indices,
+// so the speed boundary rule and the vP values are those of the whole grid.
+// After each stage the caller refreshes the halo slabs of the buffer just
+// written from the neighbouring shards (peer copies, NCCL send/recv); the
+// handle only exposes that buffer.
 #include <cmath>
 #include <cstring>
 #include <utility>
@@ -22,6 +23,7 @@
 struct pe_relative_shard {
   pe_relative_params p{};
   pe::Rel5Grid g{};  // global geometry; own_lo / own_n / slab_lo set
+  pe::Rel5Tile tile{};  // float32 stage tiling
   int lo = 0, hi = 0, own_lo = 0, own_hi = 0;
   double t = 0;
   int64_t steps = 0;
@@ -68,6 +70,7 @@ int read_stats(pe_relative_shard *h) {
   PE_CUDA_TRY(cudaMemcpyAsync(h->host_stats, h->stats, sizeof(pe::Rel5Stats),
                               cudaMemcpyDeviceToHost, h->stream));
   PE_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  if (h->host_stats->timeout) return fail(PE_ETIMEOUT, "a bounded device wait gave up");
   if (h->host_stats->nonfinite) return fail(PE_ENONFINITE, "Nonfinite field update");
   return PE_OK;
 }
@@ -94,8 +97,6 @@ int pe_relative_shard_create(const pe_relative_params *params, int32_t vp_begin,
   *out = nullptr;
   int rc = pe::rel5host::validate(params);
   if (rc) return rc;
-  if (params->precision != PE_LOCAL_F64)
-    return fail(PE_EINVAL, "vP shards run the exact stage: precision must be PE_LOCAL_F64");
   const int nvp = params->p_speeds, halo = params->order;
   if (vp_begin < 0 || vp_end > nvp || vp_begin >= vp_end)
     return fail(PE_EINVAL, "owned vP slabs must satisfy 0 <= begin < end <= p_speeds");
@@ -113,6 +114,7 @@ int pe_relative_shard_create(const pe_relative_params *params, int32_t vp_begin,
   h->g.own_n = vp_end - vp_begin;
   h->g.slab_lo = h->lo;
   h->slab_floats = h->g.sv;
+  h->tile = pe::rel5_default_tile(h->g);
   const int slabs = h->hi - h->lo, nh = h->g.nh;
   const size_t bytes = sizeof(float) * (size_t)h->g.sv * slabs;
   std::vector<double> sn(nh), cs(nh);
@@ -238,7 +240,9 @@ int pe_relative_shard_stage(pe_relative_shard *h, int32_t stage, double dt) {
   s.dt = dt;
   s.t = h->t;
   s.stats = h->stats;
-  PE_CUDA_TRY(pe::rel5_stage_f64(h->g, s, blend, h->stream));
+  PE_CUDA_TRY(h->p.precision == PE_LOCAL_F64
+                  ? pe::rel5_stage_f64(h->g, s, blend, h->stream)
+                  : pe::rel5_stage_f32(h->g, h->tile, s, blend, h->stream));
   pe::count_launches(1);
   h->last = s.dst;
   if (stage == h->g.order - 1) {

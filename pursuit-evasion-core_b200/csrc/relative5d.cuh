@@ -23,7 +23,7 @@ struct Rel5Grid {
   int64_t sy, sp, se, sv;  // padded strides of y, psi, vE, vP (x stride 1)
   double extent, dx, dphi, dvp, dve;
   double vp_lo, ve_lo, acc_p, acc_e, curv_p, curv_e;
-  // vP-slab shard (exact stage only): the stage updates global slabs
+  // vP-slab shard: the stage updates global slabs
   // [own_lo, own_lo + own_n) of a buffer whose first slab is global slab
   // slab_lo; own_n == 0 means the whole grid in one buffer
   int own_lo, own_n, slab_lo;

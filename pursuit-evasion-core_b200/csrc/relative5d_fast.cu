@@ -110,6 +110,7 @@ struct FastArgs {
   Rel5Grid g;
   Rel5Stage s;
   int rows, psi_chunk, slabs, chunks, xc, consumer_warps, items;
+  int vp_first, vp_count;  // the vP slabs this launch updates (a shard's own)
   float ihx, ihp, ihv, ihe;
   float dt;
 };
@@ -155,8 +156,8 @@ __device__ __forceinline__ Item decode_item(const FastArgs &a, int idx) {
   idx /= a.slabs;
   it.ie = idx % a.g.nve;
   idx /= a.g.nve;
-  it.iv = idx % a.g.nvp;
-  const int chunk = idx / a.g.nvp;
+  it.iv = a.vp_first + idx % a.vp_count;
+  const int chunk = idx / a.vp_count;
   it.y0 = slab * a.rows;
   it.r_eff = min(a.rows, a.g.nx - it.y0);
   it.p0 = chunk * a.psi_chunk;
@@ -193,7 +194,7 @@ __global__ void __launch_bounds__(TARGET_THREADS, 2)
   const bool producer = warp == a.consumer_warps;
   unsigned int *timeout = &a.s.stats->timeout;
   auto plane_index = [&](int v_idx, int e_idx, int psi) -> int64_t {
-    return ((int64_t)v_idx * g.nve + e_idx) * g.nh + psi;
+    return ((int64_t)(v_idx - g.slab_lo) * g.nve + e_idx) * g.nh + psi;
   };
 
   if (tid == 0) {
@@ -706,7 +707,9 @@ cudaError_t rel5_stage_f32(const Rel5Grid &g, const Rel5Tile &t,
   args.consumer_warps = (t.rows * args.xc + 31) / 32;
   args.slabs = (g.nx + t.rows - 1) / t.rows;
   args.chunks = (g.nh + t.psi_chunk - 1) / t.psi_chunk;
-  args.items = args.slabs * g.nve * g.nvp * args.chunks;
+  args.vp_first = g.own_n > 0 ? g.own_lo : 0;
+  args.vp_count = g.own_n > 0 ? g.own_n : g.nvp;
+  args.items = args.slabs * g.nve * args.vp_count * args.chunks;
   args.ihx = (float)(1.0 / g.dx);
   args.ihp = (float)(1.0 / g.dphi);
   args.ihv = (float)(1.0 / g.dvp);

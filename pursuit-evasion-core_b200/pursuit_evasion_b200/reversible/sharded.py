@@ -8,8 +8,9 @@ a neighbour, and after every stage the edge slabs of the buffer just written
 travel to the neighbours: `LocalExchange` for shards in one process (device
 copies), `DistExchange` for one shard per rank (torch.distributed P2P; NCCL
 over NVLink on GPUs).  The residual is the maximum over shards.  Each cell
-is updated by the exact stage, so a sharded solve equals the single-grid
-exact solve (and the reference executable) bit for bit.
+is updated by the single-grid stage of the chosen precision, so a sharded
+solve equals the single-grid solve bit for bit (with float64 local
+arithmetic, also the reference executable).
 
 The reference solves one grid in one process (native_relative.cpp:173-190);
 it has no sharded solve.
@@ -22,7 +23,7 @@ import ctypes
 import numpy as np
 
 from .. import _native
-from .relative_solver import _params, cfl_limit
+from .relative_solver import PRECISIONS, _params, cfl_limit
 
 
 def partition(p_speeds, parts, order=2):
@@ -70,13 +71,16 @@ class _DeviceSlabs:
 class RelativeShard:
     """One shard on one GPU: owned global vP slabs [vp_begin, vp_end)."""
 
-    def __init__(self, config, grid, vp_begin, vp_end, *, order=2, cfl=0.8, device=0):
+    def __init__(self, config, grid, vp_begin, vp_end, *, order=2, cfl=0.8,
+                 local_precision="float64", device=0):
+        if local_precision not in PRECISIONS:
+            raise ValueError("local_precision must be float32 or float64")
         self._lib = _native.library()
         self.grid = grid
         self.order = order
         self.device = device
         self._params = _params(config, grid, order=order, cfl=cfl,
-                               precision=_native.PE_LOCAL_F64, device=device)
+                               precision=PRECISIONS[local_precision], device=device)
         handle = ctypes.c_void_p()
         _native.check(self._lib.pe_relative_shard_create(
             ctypes.byref(self._params), int(vp_begin), int(vp_end), ctypes.byref(handle)))

@@ -1,7 +1,7 @@
 """vP-slab shards on the GPU (pe_relative_shard_*): several shards of one
 grid held by this process on cuda:0, their halos refreshed by device copies
-after every stage, against the single-grid exact solve and the oracle, bit
-for bit.  (Every GPU run here has one GPU: the NCCL exchange between ranks
+after every stage, against the single-grid solve of the same precision
+(exact and float32 kernels) and the oracle, bit for bit.  (Every GPU run here has one GPU: the NCCL exchange between ranks
 is covered by the gloo tests of the same driver.)"""
 
 import numpy as np
@@ -20,8 +20,8 @@ from tests.helpers import A3, CONFIG1_GRID, bits
 pytestmark = pytest.mark.gpu
 
 
-def sharded_frames(grid, parts, order, goals):
-    shards = [RelativeShard(A3, grid, b, e, order=order)
+def sharded_frames(grid, parts, order, goals, precision="float64"):
+    shards = [RelativeShard(A3, grid, b, e, order=order, local_precision=precision)
               for b, e in partition(grid.p_speeds, parts, order)]
     try:
         for s in shards:
@@ -38,8 +38,8 @@ def sharded_frames(grid, parts, order, goals):
             s.close()
 
 
-def single_frames(grid, order, goals):
-    with RelativeSolver(A3, grid, order=order, local_precision="float64") as s:
+def single_frames(grid, order, goals, precision="float64"):
+    with RelativeSolver(A3, grid, order=order, local_precision=precision) as s:
         s.initialize()
         frames = []
         for goal in goals:
@@ -48,13 +48,14 @@ def single_frames(grid, order, goals):
         return np.array(frames), s.arrival().ravel().copy(), s.steps, s.stats()[0]
 
 
+@pytest.mark.parametrize("precision", ["float64", "float32"])
 @pytest.mark.parametrize("grid, parts, order", [
     (CONFIG1_GRID, 2, 2), (CONFIG1_GRID, 3, 2), (CONFIG1_GRID, 7, 1),
     (RelativeGrid(33, 16, 9, 5, 4.0), 4, 2)])
-def test_shards_equal_single_grid_exact_solve(grid, parts, order):
+def test_shards_equal_single_grid_solve(grid, parts, order, precision):
     goals = (0.1, 0.2, 0.3)
-    got, arrival, steps, residual = sharded_frames(grid, parts, order, goals)
-    ref, ref_arrival, ref_steps, ref_residual = single_frames(grid, order, goals)
+    got, arrival, steps, residual = sharded_frames(grid, parts, order, goals, precision)
+    ref, ref_arrival, ref_steps, ref_residual = single_frames(grid, order, goals, precision)
     assert steps == ref_steps
     np.testing.assert_array_equal(bits(got), bits(ref))
     np.testing.assert_array_equal(bits(arrival), bits(ref_arrival))
