@@ -19,6 +19,8 @@ it has no sharded solve.
 from __future__ import annotations
 
 import ctypes
+import json
+from pathlib import Path
 
 import numpy as np
 
@@ -278,3 +280,130 @@ class ShardedSolver:
 
         with torch.cuda.stream(self._stream):
             return self.exchange.max_residual()
+
+
+def solve(config, grid, output, *, horizon=2.0, output_dt=0.1, order=2, cfl=0.8,
+          local_precision="float64", history=True, device=None, group=None,
+          shard_factory=None):
+    """The table directory of free_dp.solve (same files and layout, read by
+    RelativeTable) computed by one vP shard per rank of an initialised
+    torch.distributed group.  Every rank writes its own slabs of each frame
+    into the shared files (the ranks share a file system, as the GPUs of one
+    node do); rank 0 creates the directory and writes meta.json.
+    `shard_factory(begin, end)` replaces the GPU shard (tests use it)."""
+    import os
+    import time
+
+    import torch.distributed as dist
+
+    from .free_dp import SCHEMA, _validate, output_times, physics_signature
+    from .model import config_dict
+
+    started = time.perf_counter()
+    rank, world = dist.get_rank(group), dist.get_world_size(group)
+    _validate(config, grid, horizon, output_dt, order, cfl, 1)
+    ranges = partition(grid.p_speeds, world, order)
+    begin, end = ranges[rank]
+    output = Path(output).resolve()
+    times = output_times(horizon, output_dt)
+    N = grid.states
+    files = {"final.f32": N * 4, "arrival.f32": N * 4}
+    if history:
+        files["fields.f32"] = N * 4 * len(times)
+    error = None
+    if rank == 0:
+        try:
+            if output.exists() and any(output.iterdir()):
+                raise FileExistsError(f"Preserve existing output: {output}")
+            output.mkdir(parents=True, exist_ok=True)
+            for name, size in files.items():
+                with (output / name).open("wb") as f:
+                    f.truncate(size)
+        except Exception as exc:  # every rank learns of it before any work
+            error = exc
+    flag = [error is None]
+    dist.broadcast_object_list(flag, src=dist.get_global_rank(group, 0) if group else 0,
+                               group=group)
+    if error is not None:
+        raise error
+    if not flag[0]:
+        raise RuntimeError("rank 0 could not create the output directory")
+    if shard_factory is None:
+        import torch
+
+        dev = torch.cuda.current_device() if device is None else device
+
+        def shard_factory(b, e):
+            return RelativeShard(config, grid, b, e, order=order, cfl=cfl,
+                                 local_precision=local_precision, device=dev)
+
+    shard = shard_factory(begin, end)
+    try:
+        shard.initialize()
+        solver = ShardedSolver([shard], DistExchange(shard, group))
+        slab_bytes = (N // grid.p_speeds) * 4
+        offset = begin * slab_bytes
+        fds = {name: os.open(output / name, os.O_WRONLY) for name in files}
+        try:
+            def put(name, values, base=0):
+                os.pwrite(fds[name], np.ascontiguousarray(values, np.float32).tobytes(),
+                          base + offset)
+
+            if history:
+                put("fields.f32", shard.field())
+            update = 0.0
+            for k, goal in enumerate(times[1:], start=1):
+                t0 = time.perf_counter()
+                solver.advance(goal)
+                update += time.perf_counter() - t0
+                if history:
+                    put("fields.f32", shard.field(), k * N * 4)
+            put("final.f32", shard.field())
+            put("arrival.f32", shard.arrival())
+        finally:
+            for fd in fds.values():
+                os.close(fd)
+        residual = solver.residual()
+        steps = solver.steps
+    finally:
+        if hasattr(shard, "close"):
+            shard.close()
+    dist.barrier(group)
+    meta = {
+        "schema": SCHEMA,
+        "status": "complete",
+        "backend": "b200_cuda_vp_shards",
+        "local_precision": local_precision,
+        "config": config_dict(config),
+        "physics": physics_signature(config),
+        "grid": grid.to_dict(),
+        "shape": list(grid.shape),
+        "state_order": ["x", "y", "psi", "vP", "vE"],
+        "axis_order": ["vP", "vE", "psi", "y", "x"],
+        "axes": [a.tolist() for a in grid.axes(config)],
+        "horizon": horizon,
+        "output_dt": output_dt,
+        "times": times.tolist(),
+        "order": order,
+        "cfl": cfl,
+        "history_saved": bool(history),
+        "dtype": "float32",
+        "target": "physical_capture_only",
+        "capture_rule": config.capture_rule,
+        "avoid": None,
+        "tube_projection": "min over every internal update",
+        "position_boundary": "one-sided linear extrapolation; outside queries unresolved",
+        "speed_boundary": "acceleration restricted to inward or zero at speed limits",
+        "heading_boundary": "periodic",
+        "cfl_dt_limit": solver.cfl_dt_limit,
+        "internal_steps": steps,
+        "frames": len(times),
+        "last_step_residual": residual,
+        "vp_shards": [list(r) for r in ranges],
+        "update_seconds": update,
+        "total_wall_seconds": time.perf_counter() - started,
+    }
+    if rank == 0:
+        (output / "meta.json").write_text(json.dumps(meta, indent=2) + "\n")
+    dist.barrier(group)
+    return meta

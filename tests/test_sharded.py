@@ -140,3 +140,54 @@ def test_shard_argument_errors_before_any_device_work():
         RelativeShard(A3, CONFIG1_GRID, 0, 1)  # one slab with a neighbour, order 2
     with pytest.raises(ValueError, match="begin < end"):
         RelativeShard(A3, CONFIG1_GRID, 3, 9)
+
+
+def _table_rank(rank, world, port, folder, out):
+    sys.path.insert(0, str(REPO))
+    import datetime
+
+    import torch.distributed as dist
+
+    from pursuit_evasion_b200.reversible import sharded
+    from tests import oracle_lib
+
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank,
+                            world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        oracle = oracle_lib.load()
+        meta = sharded.solve(A3, CONFIG1_GRID, folder, horizon=0.2, output_dt=0.1,
+                             shard_factory=lambda b, e: OracleShard(oracle, A3, CONFIG1_GRID,
+                                                                    b, e))
+        out.put((rank, meta["internal_steps"], meta["vp_shards"]))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_sharded_table_on_gloo_ranks_equals_oracle_and_reads_as_a_table(oracle, tmp_path):
+    import torch.multiprocessing as mp
+
+    from pursuit_evasion_b200.reversible.relative_table import RelativeTable
+
+    frames, arrival, steps = reference(oracle, 2)
+    folder = tmp_path / "table"
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_table_rank, args=(r, 2, port, str(folder), out))
+             for r in range(2)]
+    for p in procs:
+        p.start()
+    results = sorted(out.get(timeout=180) for _ in procs)
+    for p in procs:
+        p.join(60)
+        assert p.exitcode == 0
+    assert all(r[1] == steps for r in results)
+    assert results[0][2] == [[0, 4], [4, 7]]
+    got = np.fromfile(folder / "fields.f32", np.float32).reshape(frames.shape)
+    np.testing.assert_array_equal(bits(got), bits(frames))
+    np.testing.assert_array_equal(bits(np.fromfile(folder / "final.f32", np.float32)),
+                                  bits(frames[-1]))
+    np.testing.assert_array_equal(bits(np.fromfile(folder / "arrival.f32", np.float32)),
+                                  bits(arrival))
+    table = RelativeTable(folder)
+    assert table.shape == tuple(CONFIG1_GRID.shape)

@@ -70,3 +70,29 @@ def test_shards_equal_oracle(oracle):
     np.testing.assert_array_equal(bits(got), bits(frames[1:]))
     np.testing.assert_array_equal(bits(got_arrival), bits(arrival))
 
+
+
+def test_sharded_table_with_one_nccl_rank_equals_free_dp_solve(tmp_path):
+    import socket
+
+    import torch.distributed as dist
+
+    from pursuit_evasion_b200.reversible import sharded
+    from pursuit_evasion_b200.reversible.free_dp import solve
+
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0,
+                            world_size=1)
+    try:
+        meta = sharded.solve(A3, CONFIG1_GRID, tmp_path / "shards", horizon=0.2,
+                             output_dt=0.1)
+    finally:
+        dist.destroy_process_group()
+    solve(A3, CONFIG1_GRID, tmp_path / "single", horizon=0.2, output_dt=0.1)
+    assert meta["vp_shards"] == [[0, 7]]
+    for name in ("fields.f32", "final.f32", "arrival.f32"):
+        np.testing.assert_array_equal(
+            bits(np.fromfile(tmp_path / "shards" / name, np.float32)),
+            bits(np.fromfile(tmp_path / "single" / name, np.float32)))
