@@ -326,7 +326,9 @@ typedef struct pe_world_params {
   double cfl;                    /* --cfl */
   int32_t order;                 /* --order, 1 or 2 */
   int32_t linear_speed_boundary; /* --linear-speed-boundary */
-  int32_t avoid_mode;            /* 0: none; 1: max(|xP|,|yP|) - arena + 1e-6 */
+  int32_t avoid_mode;            /* 0: none; 1: max(|xP|,|yP|) - arena + 1e-6;
+                                    2: -p_clear[xP, yP, thP] + 1e-6 (obstacle map,
+                                    gpu_map_game.py:64-66; pe_world_set_clearance) */
   int32_t device;
   int32_t fast; /* 0 (default): float32 in the reference's order, bit for bit
                    native_world.cpp; 1: reciprocal spacings and multiply-add
@@ -346,6 +348,15 @@ int pe_world_init_contact(pe_world *h, double p_length, double p_width,
                           double e_length, double e_width);
 /* The reference's square-arena surfaces (native_world.cpp:155-176). */
 int pe_world_init_square(pe_world *h);
+/* Obstacle map game (gpu_map_game.py:45-50, :64-66): each car's clearance
+ * per (x, y, heading) pose, positions^2 * headings floats in C order
+ * [x][y][heading] (host), as FootprintMap.clearance gives them
+ * (gpu_map_game.py:78-84).  Avoid mode 2 floors every update at
+ * -p_clear + 1e-6. */
+int pe_world_set_clearance(pe_world *h, const float *p_clear, const float *e_clear);
+/* Surfaces of the map game: max(min(hypot(dP - dE) - radius, e_clear),
+ * -p_clear + 1e-6); arrival 0 where <= 0. */
+int pe_world_init_map(pe_world *h);
 /* A host field (continuation, native_world.cpp:177-191). */
 int pe_world_init_field(pe_world *h, const float *field, const float *arrival,
                         double start_time);

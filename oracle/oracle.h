@@ -68,6 +68,11 @@ void po_w8_init_contact(const po_w8_cfg *c, double p_len, double p_wid,
                         double e_len, double e_wid, float *a, float *arrival);
 int po_w8_stage(const po_w8_cfg *c, const float *src, float *dst,
                 const float *base, float *arrival, float dt, double tau);
+/* Obstacle map game (clearances per (x, y, heading) pose of each car). */
+void po_w8_init_map(const po_w8_cfg *c, const float *p_clear, const float *e_clear,
+                    float *a, float *arrival);
+int po_w8_stage_clear(const po_w8_cfg *c, const float *src, float *dst, const float *base,
+                      float *arrival, float dt, double tau, const float *p_clear);
 /* The same stage in double precision on double fields (no arrival): the
  * rounding-free reference for float32 variants of the step. */
 int po_w8_stage_f64(const po_w8_cfg *c, const double *src, double *dst,

@@ -229,6 +229,34 @@ void po_w8_init_contact(const po_w8_cfg *c, double p_len, double p_wid,
  * previous value and the avoid floor are applied and arrival recorded. */
 int po_w8_stage(const po_w8_cfg *c, const float *src, float *dst,
                 const float *base, float *arrival, float dt, double tau) {
+  return po_w8_stage_clear(c, src, dst, base, arrival, dt, tau, NULL);
+}
+
+/* The obstacle map game's surfaces (gpu_map_game.py:45-50): centre-distance
+ * capture limited by the evader clearance, floored by the pursuer's. */
+void po_w8_init_map(const po_w8_cfg *c, const float *p_clear, const float *e_clear,
+                    float *a, float *arrival) {
+  w8_geom g;
+  w8_make(c, &g);
+  const float dx = 2 * c->extent / (c->n - 1);
+#pragma omp parallel for schedule(static)
+  for (size_t j = 0; j < g.n; j++) {
+    int q[8];
+    for (int k = 0; k < 8; k++) q[k] = (int)((j / g.stride[k]) % g.shape[k]);
+    const float cap = hypotf((q[0] - q[4]) * dx, (q[1] - q[5]) * dx) - c->radius;
+    const float p = p_clear[((size_t)q[0] * c->n + q[1]) * c->nh + q[2]];
+    const float e = e_clear[((size_t)q[4] * c->n + q[5]) * c->nh + q[6]];
+    const float v = fmaxf(fminf(cap, e), -p + 1e-6f);
+    a[j] = v;
+    if (arrival) arrival[j] = v <= 0 ? 0.0f : NAN;
+  }
+  w8_free(&g);
+}
+
+/* po_w8_stage with the map game's avoid floor -p_clear[xP, yP, thP] + 1e-6
+ * (gpu_map_game.py:64-66) when p_clear != NULL. */
+int po_w8_stage_clear(const po_w8_cfg *c, const float *src, float *dst, const float *base,
+                      float *arrival, float dt, double tau, const float *p_clear) {
   w8_geom g;
   w8_make(c, &g);
   const size_t inner = (size_t)c->nh * c->ne;
@@ -245,7 +273,8 @@ int po_w8_stage(const po_w8_cfg *c, const float *src, float *dst,
     const float fpx = vp * g.cs[q[2]], fpy = vp * g.sn[q[2]];
     const float wp = fabsf(vp) * c->kp;
     const float avoid =
-        c->avoid_square
+        p_clear ? -p_clear[((size_t)q[0] * c->n + q[1]) * c->nh + q[2]] + 1e-6f
+        : c->avoid_square
             ? fmaxf(fabsf(g.x[q[0]]), fabsf(g.x[q[1]])) - c->arena + 1e-6f
             : -INFINITY;
     for (int eh = 0; eh < c->nh; eh++) {

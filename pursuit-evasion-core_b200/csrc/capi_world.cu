@@ -17,6 +17,7 @@ struct pe_world {
   float *a = nullptr, *b = nullptr, *arrival = nullptr;
   float *x = nullptr, *cs = nullptr, *sn = nullptr, *pv = nullptr, *ev = nullptr;
   double *csd = nullptr, *snd = nullptr, *cdiff = nullptr, *sdiff = nullptr;
+  float *p_clear = nullptr, *e_clear = nullptr;  // obstacle clearances (avoid mode 2)
   pe::World8Stats *stats = nullptr, *host_stats = nullptr;
   cudaStream_t own = nullptr, stream = nullptr;
   double t = 0;
@@ -45,7 +46,7 @@ int validate(const pe_world_params *p) {
       p->p_speed_min >= p->p_speed_max || p->e_speed_min >= p->e_speed_max ||
       p->p_acceleration <= 0 || p->e_acceleration <= 0 || p->p_curvature <= 0 ||
       p->e_curvature <= 0 || p->extent <= 0 ||
-      (p->avoid_mode != 0 && p->avoid_mode != 1) || (p->fast != 0 && p->fast != 1))
+      p->avoid_mode < 0 || p->avoid_mode > 2 || (p->fast != 0 && p->fast != 1))
     return fail(PE_EINVAL, "Invalid arguments");
   // each car's block of cells is indexed with 32-bit integers on the device
   const int64_t block_p = (int64_t)p->positions * p->positions * p->headings * p->p_speeds;
@@ -101,7 +102,8 @@ void release(pe_world *h) {
   for (void *ptr : {(void *)h->a, (void *)h->b, (void *)h->arrival, (void *)h->x,
                     (void *)h->cs, (void *)h->sn, (void *)h->pv, (void *)h->ev,
                     (void *)h->csd, (void *)h->snd, (void *)h->cdiff,
-                    (void *)h->sdiff, (void *)h->stats})
+                    (void *)h->sdiff, (void *)h->stats, (void *)h->p_clear,
+                    (void *)h->e_clear})
     cudaFree(ptr);
   if (h->host_stats) cudaFreeHost(h->host_stats);
   if (h->own) cudaStreamDestroy(h->own);
@@ -136,6 +138,9 @@ int stage(pe_world *h, const float *src, float *dst, const float *base, float dt
   s.dt = dt;
   s.tau = h->t;
   s.stats = h->stats;
+  s.p_clear = h->p_clear;
+  if (h->g.avoid_mode == 2 && !h->p_clear)
+    return fail(PE_ESTATE, "avoid mode 2 needs pe_world_set_clearance first");
   cudaEvent_t e0 = h->timer.begin(h->stream);
   PE_CUDA_TRY(h->p.fast ? pe::world8_stage_fast(h->g, s, h->stream)
                         : pe::world8_stage(h->g, s, h->stream));
@@ -264,6 +269,39 @@ int pe_world_init_contact(pe_world *h, double p_length, double p_width,
   PE_CUDA_TRY(pe::world8_init_contact(h->g, h->csd, h->snd, h->cdiff, h->sdiff,
                                       p_length, p_width, e_length, e_width, h->a,
                                       h->arrival, h->stream));
+  pe::count_launches(1);
+  PE_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  h->t = 0;
+  h->steps = 0;
+  h->initialized = true;
+  return PE_OK;
+}
+
+int pe_world_set_clearance(pe_world *h, const float *p_clear, const float *e_clear) {
+  int rc = enter(h);
+  if (rc) return rc;
+  if (!p_clear || !e_clear) return fail(PE_EINVAL, "clearance arrays are NULL");
+  const size_t count = (size_t)h->g.n * h->g.n * h->g.nh;
+  for (size_t i = 0; i < count; i++)
+    if (!std::isfinite(p_clear[i]) || !std::isfinite(e_clear[i]))
+      return fail(PE_EINVAL, "non-finite clearance");
+  if (!h->p_clear) PE_CUDA_TRY(cudaMalloc(&h->p_clear, sizeof(float) * count));
+  if (!h->e_clear) PE_CUDA_TRY(cudaMalloc(&h->e_clear, sizeof(float) * count));
+  PE_CUDA_TRY(cudaMemcpyAsync(h->p_clear, p_clear, sizeof(float) * count,
+                              cudaMemcpyHostToDevice, h->stream));
+  PE_CUDA_TRY(cudaMemcpyAsync(h->e_clear, e_clear, sizeof(float) * count,
+                              cudaMemcpyHostToDevice, h->stream));
+  PE_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return PE_OK;
+}
+
+int pe_world_init_map(pe_world *h) {
+  int rc = enter(h);
+  if (rc) return rc;
+  if (!h->p_clear) return fail(PE_ESTATE, "pe_world_set_clearance before pe_world_init_map");
+  PE_CUDA_TRY(cudaMemsetAsync(h->stats, 0, sizeof(pe::World8Stats), h->stream));
+  PE_CUDA_TRY(pe::world8_init_map(h->g, (float)h->p.capture_radius, h->p_clear, h->e_clear,
+                                  h->a, h->arrival, h->stream));
   pe::count_launches(1);
   PE_CUDA_TRY(cudaStreamSynchronize(h->stream));
   h->t = 0;

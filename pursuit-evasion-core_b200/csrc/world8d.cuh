@@ -13,7 +13,8 @@ namespace pe {
 struct World8Grid {
   int n, nh, np, ne, order;
   int linear_speed;  // inward one-sided slopes at the speed bounds
-  int avoid_mode;    // 0: none; 1: square arena max(|xP|,|yP|) - arena + 1e-6
+  int avoid_mode;    // 0: none; 1: square arena max(|xP|,|yP|) - arena + 1e-6;
+                     // 2: obstacle clearance -p_clear[xP, yP, thP] + 1e-6
   int64_t cells;
   int64_t stride[8];
   int shape[8];
@@ -37,6 +38,7 @@ struct World8Stage {
   float dt;
   double tau;
   World8Stats *stats;
+  const float *p_clear;  // avoid_mode 2: pursuer clearance [xP][yP][thP]
 };
 
 // One stage in float32 arithmetic evaluated in the reference's order; the
@@ -66,6 +68,14 @@ cudaError_t world8_init_contact(const World8Grid &g, const double *cs,
 cudaError_t world8_init_square(const World8Grid &g, const float *x,
                                float radius, float *field, float *arrival,
                                cudaStream_t stream);
+
+// The obstacle map game's surfaces (gpu_map_game.py:45-50): centre-distance
+// capture limited by the evader's clearance, floored by the pursuer's
+// clearance: max(min(hypot(dxP - dxE) - r, e_clear), -p_clear + 1e-6), the
+// clearances per (x, y, heading) pose of each car.
+cudaError_t world8_init_map(const World8Grid &g, float radius, const float *p_clear,
+                            const float *e_clear, float *field, float *arrival,
+                            cudaStream_t stream);
 
 // arrival = start where field <= 0, NaN elsewhere (after a host upload).
 cudaError_t world8_init_arrival(const World8Grid &g, const float *field,

@@ -124,6 +124,39 @@ cudaError_t world8_init_square(const World8Grid &g, const float *x,
   return cudaGetLastError();
 }
 
+namespace {
+
+__global__ void world8_map_kernel(const World8Grid g, float radius,
+                                  const float *__restrict__ p_clear,
+                                  const float *__restrict__ e_clear, float *__restrict__ field,
+                                  float *__restrict__ arrival) {
+  const float dx = 2 * g.extent / (g.n - 1);
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < g.cells;
+       j += (int64_t)gridDim.x * blockDim.x) {
+    int q[8];
+    int64_t rest = j;
+    for (int k = 7; k >= 0; k--) {
+      q[k] = (int)(rest % g.shape[k]);
+      rest /= g.shape[k];
+    }
+    const float cap = hypotf((q[0] - q[4]) * dx, (q[1] - q[5]) * dx) - radius;
+    const float p = p_clear[(q[0] * g.n + q[1]) * g.nh + q[2]];
+    const float e = e_clear[(q[4] * g.n + q[5]) * g.nh + q[6]];
+    const float v = fmaxf(fminf(cap, e), -p + 1e-6f);
+    field[j] = v;
+    arrival[j] = v <= 0 ? 0.f : __int_as_float(0x7fc00000);
+  }
+}
+
+}  // namespace
+
+cudaError_t world8_init_map(const World8Grid &g, float radius, const float *p_clear,
+                            const float *e_clear, float *field, float *arrival,
+                            cudaStream_t stream) {
+  world8_map_kernel<<<148 * 8, 256, 0, stream>>>(g, radius, p_clear, e_clear, field, arrival);
+  return cudaGetLastError();
+}
+
 cudaError_t world8_init_arrival(const World8Grid &g, const float *field,
                                 float *arrival, float start,
                                 cudaStream_t stream) {

@@ -195,6 +195,8 @@ __global__ void __launch_bounds__(kThreads)
     if (g.avoid_mode == 1) {
       const float ax = fabsf(__ldg(s.x + qp[0])), ay = fabsf(__ldg(s.x + qp[1]));
       avoid = (ax < ay ? ay : ax) - g.arena + 1e-6f;
+    } else if (g.avoid_mode == 2) {
+      avoid = -__ldg(s.p_clear + (qp[0] * g.n + qp[1]) * g.nh + qp[2]) + 1e-6f;
     }
     // neighbour offsets along the pursuer axes, in cells
     int64_t poff[4][4];

@@ -145,6 +145,8 @@ __global__ void __launch_bounds__(256)
         if (g.avoid_mode == 1) {
           const float ax = fabsf(s.x[q[0]]), ay = fabsf(s.x[q[1]]);
           avoid = (ax < ay ? ay : ax) - g.arena + 1e-6f;
+        } else if (g.avoid_mode == 2) {
+          avoid = -s.p_clear[(q[0] * g.n + q[1]) * g.nh + q[2]] + 1e-6f;
         }
         value = tube < avoid ? avoid : tube;
         if (previous > 0 && value <= 0 && isnan(s.arrival[j]))

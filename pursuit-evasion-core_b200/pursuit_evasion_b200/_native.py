@@ -257,6 +257,8 @@ SIGNATURES = {
     "pe_world_create": (ctypes.c_int, [ctypes.POINTER(WorldParams),
                                        ctypes.POINTER(ctypes.c_void_p)]),
     "pe_world_init_contact": (ctypes.c_int, [_P] + [ctypes.c_double] * 4),
+    "pe_world_set_clearance": (ctypes.c_int, [_P, _P, _P]),
+    "pe_world_init_map": (ctypes.c_int, [_P]),
     "pe_world_init_square": (ctypes.c_int, [_P]),
     "pe_world_init_field": (ctypes.c_int, [_P, _P, _P, ctypes.c_double]),
     "pe_world_advance": (ctypes.c_int, [_P, ctypes.c_double, _I64P]),

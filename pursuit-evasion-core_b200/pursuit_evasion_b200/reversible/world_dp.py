@@ -103,14 +103,17 @@ def _params(config, grid, *, order, cfl, speed_boundary, avoid, device, fast=Fal
         e_acceleration=float(e.acceleration), e_curvature=float(e.max_curvature),
         cfl=float(cfl), order=int(order),
         linear_speed_boundary=int(speed_boundary == "linear"),
-        avoid_mode=1 if avoid else 0, device=int(device), fast=int(bool(fast)))
+        avoid_mode={False: 0, None: 0, True: 1, "square": 1, "clearance": 2}[avoid],
+        device=int(device), fast=int(bool(fast)))
 
 
 class WorldSolver:
     """Owning handle of one device-resident 8D field (pe_world_*).  `fast`
     selects the stage with reciprocal spacings and multiply-add contraction
     instead of the reference's operation order (bit for bit
-    native_world.cpp)."""
+    native_world.cpp).  `avoid`: True (or "square") for the square-arena
+    floor, False for none, "clearance" for the obstacle map game's floor
+    -p_clear + 1e-6 (gpu_map_game.py:64-66; set_clearance first)."""
 
     def __init__(self, config, grid, *, order=2, cfl=0.8, speed_boundary="linear",
                  avoid=True, device=0, fast=False):
@@ -156,6 +159,23 @@ class WorldSolver:
 
     def init_square(self):
         _native.check(self._lib.pe_world_init_square(self._h))
+
+    def set_clearance(self, p_clear, e_clear):
+        """Each car's obstacle clearance per (x, y, heading) grid pose,
+        [positions, positions, headings] (FootprintMap.clearance at the grid
+        poses, gpu_map_game.py:78-84)."""
+        n, nh = self.grid.positions, self.grid.headings
+        arrays = [np.ascontiguousarray(c, dtype=np.float32) for c in (p_clear, e_clear)]
+        for c in arrays:
+            if c.shape != (n, n, nh):
+                raise ValueError("clearance grids must be [positions, positions, headings]")
+        _native.check(self._lib.pe_world_set_clearance(self._h, arrays[0].ctypes.data,
+                                                       arrays[1].ctypes.data))
+
+    def init_map(self):
+        """The map game's surfaces (gpu_map_game.py:45-50): max(min(centre
+        distance - radius, e_clear), -p_clear + 1e-6)."""
+        _native.check(self._lib.pe_world_init_map(self._h))
 
     def init_field(self, field, arrival=None, start_time=0.0):
         field = np.ascontiguousarray(field, dtype=np.float32).reshape(-1)

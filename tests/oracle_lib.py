@@ -92,6 +92,9 @@ class Oracle:
                                            ctypes.c_double]),
             "po_w8_stage": (ctypes.c_int, [_P, _P, _P, _P, _P, ctypes.c_float,
                                            ctypes.c_double]),
+            "po_w8_stage_clear": (ctypes.c_int, [_P, _P, _P, _P, _P, ctypes.c_float,
+                                                 ctypes.c_double, _P]),
+            "po_w8_init_map": (None, [_P, _P, _P, _P, _P]),
             "po_sl_integrated_speed": (None, [ctypes.c_double] * 5 + [_P, _P]),
             "po_sl_successor": (None, [_P] + [ctypes.c_double] * 5
                                 + [ctypes.c_int, ctypes.c_int, _P]),
@@ -172,6 +175,24 @@ class Oracle:
                                     e_body[0], e_body[1], a.ctypes.data,
                                     arr.ctypes.data)
         return a, arr
+
+    def w8_init_map(self, cfg, p_clear, e_clear):
+        n = self.w8_cells(cfg)
+        a = np.zeros(n, np.float32)
+        arr = np.zeros(n, np.float32)
+        pc = np.ascontiguousarray(p_clear, np.float32)
+        ec = np.ascontiguousarray(e_clear, np.float32)
+        self.lib.po_w8_init_map(ctypes.addressof(cfg), pc.ctypes.data, ec.ctypes.data,
+                                a.ctypes.data, arr.ctypes.data)
+        return a, arr
+
+    def w8_stage_clear(self, cfg, src, dst, base, arrival, dt, tau, p_clear):
+        pc = np.ascontiguousarray(p_clear, np.float32)
+        return self.lib.po_w8_stage_clear(ctypes.addressof(cfg), src.ctypes.data,
+                                          dst.ctypes.data,
+                                          None if base is None else base.ctypes.data,
+                                          None if arrival is None else arrival.ctypes.data,
+                                          dt, tau, pc.ctypes.data)
 
     def w8_stage(self, cfg, src, dst, base, arrival, dt, tau):
         return self.lib.po_w8_stage(ctypes.addressof(cfg), src.ctypes.data,
