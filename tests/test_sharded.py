@@ -191,3 +191,49 @@ def test_sharded_table_on_gloo_ranks_equals_oracle_and_reads_as_a_table(oracle, 
                                   bits(arrival))
     table = RelativeTable(folder)
     assert table.shape == tuple(CONFIG1_GRID.shape)
+
+
+def _refuse_rank(rank, world, port, folder, out):
+    sys.path.insert(0, str(REPO))
+    import datetime
+
+    import torch.distributed as dist
+
+    from pursuit_evasion_b200.reversible import sharded
+    from tests import oracle_lib
+
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank,
+                            world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        oracle = oracle_lib.load()
+        try:
+            sharded.solve(A3, CONFIG1_GRID, folder, horizon=0.1, output_dt=0.1,
+                          shard_factory=lambda b, e: OracleShard(oracle, A3, CONFIG1_GRID,
+                                                                 b, e))
+            out.put((rank, "solved"))
+        except (FileExistsError, RuntimeError) as exc:
+            out.put((rank, type(exc).__name__))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_sharded_table_refuses_existing_output_on_every_rank(tmp_path):
+    """Rank 0 finds a non-empty folder; every rank stops before any work."""
+    import torch.multiprocessing as mp
+
+    folder = tmp_path / "table"
+    folder.mkdir()
+    (folder / "keep.txt").write_text("x")
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_refuse_rank, args=(r, 2, port, str(folder), out))
+             for r in range(2)]
+    for p in procs:
+        p.start()
+    results = sorted(out.get(timeout=180) for _ in procs)
+    for p in procs:
+        p.join(60)
+        assert p.exitcode == 0
+    assert results == [(0, "FileExistsError"), (1, "RuntimeError")]
+    assert sorted(x.name for x in folder.iterdir()) == ["keep.txt"]
