@@ -71,6 +71,13 @@ def workload_name():
             f"horizon {HORIZON} s cfl 0.8")
 
 
+def bench_config(cells):
+    """The `config` object of both arms' JSON lines (the same workload)."""
+    return {"workload": workload_name(), "cells": cells,
+            "unit_of_work": "one ENO2/LF RK2 stage update of one cell (cell-backup)",
+            "l2": "inputs larger than L2 (357.7 MB field), no flush"}
+
+
 # ---------------------------------------------------------------------------
 # clocks during the timed region
 class ClockSampler:
@@ -155,26 +162,52 @@ def profile_traffic():
     return None
 
 
-def reference_sample(cells_grid, steps, threads):
-    """Run the reference executable on the bench grid for `steps` RK2 steps;
-    returns (update_seconds, internal_steps)."""
-    from pursuit_evasion_b200.reversible.relative_solver import cfl_limit
-    from pursuit_evasion_b200.reversible.free_dp import RelativeGrid
+# reversible_free_a3 (configs/reversible_free_a3.json of the reference) as
+# plain numbers: the reference arm must not load this package.
+A3_LIMITS = {
+    "pursuer": dict(speed_min=-1.0, speed_max=2.0, acceleration=3.0, max_curvature=1.0),
+    "evader": dict(speed_min=-0.5, speed_max=1.0, acceleration=3.0, max_curvature=2.0),
+    "capture_radius": 0.3,
+}
 
-    config = a3_config()
-    grid = RelativeGrid(**GRID)
-    limit = cfl_limit(config, grid)
-    horizon = steps * limit
-    p, e = config.pursuer, config.evader
+
+def reference_cfl_dt(cfl=0.8):
+    """The CFL step limit of native_relative.cpp:76-81 for the bench grid,
+    restated in plain Python so that the reference arm imports nothing from
+    this package."""
+    import math
+
+    p, e = A3_LIMITS["pursuer"], A3_LIMITS["evader"]
+    g = GRID
+    dx = 2 * g["extent"] / (g["positions"] - 1)
+    dphi = 2 * math.pi / g["headings"]
+    dvp = (p["speed_max"] - p["speed_min"]) / (g["p_speeds"] - 1)
+    dve = (e["speed_max"] - e["speed_min"]) / (g["e_speeds"] - 1)
+    VP = max(abs(p["speed_min"]), abs(p["speed_max"]))
+    VE = max(abs(e["speed_min"]), abs(e["speed_max"]))
+    kp, ke = p["max_curvature"], e["max_curvature"]
+    total = ((VP + VE + VP * kp * g["extent"]) / dx + (VE + VP * kp * g["extent"]) / dx
+             + (VP * kp + VE * ke) / dphi + p["acceleration"] / dvp
+             + e["acceleration"] / dve)
+    return cfl / total
+
+
+def reference_sample(steps, threads):
+    """Run the reference executable (native_relative.cpp built from the
+    reference sources) on the bench grid for `steps` RK2 steps; returns
+    (update_seconds, internal_steps) from its own timing.json."""
+    horizon = steps * reference_cfl_dt()
+    p, e = A3_LIMITS["pursuer"], A3_LIMITS["evader"]
+    g = GRID
     out = Path(tempfile.mkdtemp(prefix="pe_refbench_"))
     options = {
-        "positions": grid.positions, "headings": grid.headings,
-        "p-speeds": grid.p_speeds, "e-speeds": grid.e_speeds,
-        "extent": grid.extent, "radius": config.capture_radius,
-        "p-min": p.speed_min, "p-max": p.speed_max, "e-min": e.speed_min,
-        "e-max": e.speed_max, "p-acceleration": p.acceleration,
-        "e-acceleration": e.acceleration, "p-curvature": p.max_curvature,
-        "e-curvature": e.max_curvature, "horizon": repr(horizon),
+        "positions": g["positions"], "headings": g["headings"],
+        "p-speeds": g["p_speeds"], "e-speeds": g["e_speeds"],
+        "extent": g["extent"], "radius": A3_LIMITS["capture_radius"],
+        "p-min": p["speed_min"], "p-max": p["speed_max"], "e-min": e["speed_min"],
+        "e-max": e["speed_max"], "p-acceleration": p["acceleration"],
+        "e-acceleration": e["acceleration"], "p-curvature": p["max_curvature"],
+        "e-curvature": e["max_curvature"], "horizon": repr(horizon),
         "output-dt": repr(horizon), "order": 2, "cfl": 0.8, "threads": threads,
         "history": 0, "output": str(out),
     }
@@ -190,16 +223,21 @@ def reference_sample(cells_grid, steps, threads):
 
 def oracle_sample(steps, threads):
     """The oracle port (oracle/relative5d.c) on the bench grid, `steps` RK2
-    steps; used only when the reference executable is not built."""
+    steps; used only when the reference executable is not built.  Like
+    reference_sample it imports nothing from this package."""
     import ctypes
+    from types import SimpleNamespace
+
     from tests import oracle_lib
-    from pursuit_evasion_b200.reversible.free_dp import RelativeGrid
 
     os.environ.setdefault("OMP_NUM_THREADS", str(threads))
     o = oracle_lib.load()
-    grid = RelativeGrid(**GRID)
-    cfg = o.rel_cfg(a3_config(), grid)
-    n = grid.states
+    config = SimpleNamespace(pursuer=SimpleNamespace(**A3_LIMITS["pursuer"]),
+                             evader=SimpleNamespace(**A3_LIMITS["evader"]),
+                             capture_radius=A3_LIMITS["capture_radius"])
+    cfg = o.rel_cfg(config, SimpleNamespace(**GRID))
+    n = int(np.prod([GRID[k] for k in ("p_speeds", "e_speeds", "headings")])
+            * GRID["positions"] ** 2)
     a = np.empty(n, np.float32)
     b = np.empty(n, np.float32)
     arr = np.empty(n, np.float32)
@@ -217,7 +255,7 @@ def cpu_baseline(steps=3):
     cells = int(np.prod([GRID["p_speeds"], GRID["e_speeds"], GRID["headings"],
                          GRID["positions"], GRID["positions"]]))
     if REF_EXE.exists():
-        seconds, taken = reference_sample(cells, steps, threads)
+        seconds, taken = reference_sample(steps, threads)
         kind = "reference"
         what = "native_relative.cpp built from the reference sources"
     else:
@@ -242,14 +280,14 @@ def run_reference_arm(args, world, rank):
     cells = int(np.prod(list(GRID.values())[:4]) * GRID["positions"])
     for _ in range(args.warmup):
         if REF_EXE.exists():
-            reference_sample(cells, steps_per_sample, threads)
+            reference_sample(steps_per_sample, threads)
         else:
             oracle_sample(steps_per_sample, threads)
     total_s = 0.0
     total_steps = 0
     for _ in range(args.steps):
         if REF_EXE.exists():
-            s, n = reference_sample(cells, steps_per_sample, threads)
+            s, n = reference_sample(steps_per_sample, threads)
         else:
             s, n = oracle_sample(steps_per_sample, threads)
         total_s += s
@@ -263,9 +301,12 @@ def run_reference_arm(args, world, rank):
         "ms_per_step": 1e3 * total_s / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 storage, f64 local", "data": "synthetic (deterministic grid)",
-        "config": {"workload": workload_name(), "cells": cells,
-                   "sample_rk2_steps_per_step": steps_per_sample,
-                   "parallelism": f"OpenMP {threads} threads"},
+        "config": bench_config(cells),
+        "run": {"stages_per_step": 2 * steps_per_sample,
+                "sample": (f"each bench step runs {steps_per_sample} RK2 steps of the same "
+                           "grid and physics; the metric is per cell-stage, so it compares "
+                           "with the full solve of the other arm"),
+                "parallelism": f"OpenMP {threads} threads"},
         "cpu_baseline": {
             "value": value, "unit": METRIC, "cores": threads, "kind": kind,
             "sample": (f"{steps_per_sample} RK2 steps of the bench grid per "
@@ -814,13 +855,9 @@ def run_ours(args, world, rank, local):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32" if args.precision == "float32" else "f32 storage, f64 local",
             "data": "synthetic (deterministic grid, no dataset)",
-            "config": {
-                "workload": workload_name(), "cells": cells,
-                "stages_per_step": stages_per_solve,
-                "precision": args.precision,
-                "l2": "inputs larger than L2 (357.7 MB field), no flush",
-                "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-            },
+            "config": bench_config(cells),
+            "run": {"stages_per_step": stages_per_solve, "precision": args.precision,
+                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
             "roofline": roofline,
             "e2e": {"value": e2e_value, "unit": METRIC,
                     "h2d_bytes_per_step": 4 * cells,

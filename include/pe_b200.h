@@ -197,13 +197,17 @@ int pe_relative_destroy(pe_relative *h);
  * max|field_out - field_in|.  The call synchronises `cuda_stream`.
  *
  * Scratch (the intermediate stage field, the heading tables, the reduction
- * words) lives in one fixed __device__ array of about 16.8 MB that every
- * GPU loading the library holds until exit; grids above
+ * words) lives in one fixed __device__ array of about 16.8 MB; grids above
  * PE_NOALLOC_MAX_CELLS cells or PE_NOALLOC_MAX_HEADINGS headings are
- * rejected with PE_EINVAL.  The first call on a device looks up the
- * array's device address; make that first call before any stream capture.
- * All calls share the array: calls that overlap on the GPU (other streams,
- * other host threads) race and must be serialised by the caller. */
+ * rejected with PE_EINVAL.  The CUDA runtime loads device code lazily, so
+ * the first call on a device reserves the array there (and looks up its
+ * device address); the device then holds it until the process exits.  A
+ * host that gives all device memory to its own pool should make one call
+ * on each device before taking the pool.  Every call copies the heading
+ * tables from host memory and synchronises `cuda_stream`, so it must never
+ * be called while that stream is being captured into a graph.  All calls
+ * share the array: calls that overlap on the GPU (other streams, other host
+ * threads) race and must be serialised by the caller. */
 #define PE_NOALLOC_MAX_CELLS 4194304
 #define PE_NOALLOC_MAX_HEADINGS 1024
 int pe_relative_step_noalloc(const pe_relative_params *params,

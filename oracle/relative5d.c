@@ -15,7 +15,8 @@
  *   po_rel_stage_f32 : float32 storage, double local arithmetic.  The
  *       operations are evaluated in the same order as the reference so that a
  *       non-contracting x86-64 build reproduces the reference executable bit
- *       for bit (checked by tests/test_oracle_relative.py).
+ *       for bit (checked by tests/test_oracle.py against the executable and
+ *       its golden vectors).
  *   po_rel_stage_f64 : double storage, the "FP64 oracle" used to report the
  *       max-abs error of float32-storage tables.
  *

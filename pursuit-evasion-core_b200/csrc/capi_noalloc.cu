@@ -8,7 +8,11 @@
 // behind its back.  For them this entry point keeps its scratch -- the RK2
 // intermediate stage field, the heading sine/cosine tables and the
 // reduction words -- in one file-scope __device__ array of fixed size,
-// which every GPU that loads this library holds until the process exits.
+// which every GPU that uses this entry point holds until the process exits.
+// The CUDA runtime loads a library's device code lazily (per translation
+// unit, on first use), so the array is reserved on a device by the first
+// call there, not when the library is loaded: a host that hands all device
+// memory to its own pool makes one call first (any small grid will do).
 //
 // The caller passes the field to advance, the field to write and the
 // arrival times, all in the dense table layout [vP, vE, psi, y, x].  The
@@ -113,20 +117,23 @@ extern "C" int pe_relative_step_noalloc(const pe_relative_params *params,
   g.curv_p = params->p_curvature;
   g.curv_e = params->e_curvature;
 
-  // Heading tables (native_relative.cpp:84-89) into the scratch array.
-  double trig[2 * kMaxHeadings];
+  // Heading tables (native_relative.cpp:84-89) into the scratch array:
+  // only the nh sines and nh cosines this grid uses are copied.
+  double sines[kMaxHeadings], cosines[kMaxHeadings];
   for (int k = 0; k < g.nh; k++) {
     const double q = -pi + k * g.dphi;
-    trig[k] = std::sin(q);
-    trig[kMaxHeadings + k] = std::cos(q);
+    sines[k] = std::sin(q);
+    cosines[k] = std::cos(q);
   }
   pe::Rel5Stats *stats = reinterpret_cast<pe::Rel5Stats *>(scratch);
   double *sn = scratch + kStatsDoubles;
   double *cs = sn + kMaxHeadings;
   float *stage = reinterpret_cast<float *>(scratch + kStageOffsetDoubles);
   PE_CUDA_TRY(cudaMemsetAsync(stats, 0, sizeof(pe::Rel5Stats), stream));
-  PE_CUDA_TRY(cudaMemcpyAsync(sn, trig, sizeof(double) * 2 * kMaxHeadings,
-                              cudaMemcpyHostToDevice, stream));
+  PE_CUDA_TRY(cudaMemcpyAsync(sn, sines, sizeof(double) * g.nh, cudaMemcpyHostToDevice,
+                              stream));
+  PE_CUDA_TRY(cudaMemcpyAsync(cs, cosines, sizeof(double) * g.nh, cudaMemcpyHostToDevice,
+                              stream));
 
   pe::Rel5Stage s{};
   s.arrival = arrival;
@@ -155,6 +162,7 @@ extern "C" int pe_relative_step_noalloc(const pe_relative_params *params,
   pe::Rel5Stats host{};
   PE_CUDA_TRY(cudaMemcpyAsync(&host, stats, sizeof host, cudaMemcpyDeviceToHost, stream));
   PE_CUDA_TRY(cudaStreamSynchronize(stream));
+  if (host.timeout) return fail(PE_ETIMEOUT, "a bounded device wait gave up");
   if (host.nonfinite) return fail(PE_ENONFINITE, "Nonfinite field update");
   if (residual) std::memcpy(residual, &host.residual, sizeof(double));
   return PE_OK;

@@ -282,6 +282,23 @@ class ShardedSolver:
             return self.exchange.max_residual()
 
 
+def _agree(error, group, what):
+    """Every rank of `group` learns whether any rank failed at this point.
+    The failing rank re-raises its own exception; the others raise
+    RuntimeError naming the first failing rank.  Each rank takes this
+    collective at the same points, so it never waits on a rank that left."""
+    import torch.distributed as dist
+
+    reports = [None] * dist.get_world_size(group)
+    dist.all_gather_object(reports, None if error is None else repr(error), group=group)
+    if error is not None:
+        raise error
+    failed = [(r, msg) for r, msg in enumerate(reports) if msg is not None]
+    if failed:
+        r, msg = failed[0]
+        raise RuntimeError(f"rank {r} failed during {what}: {msg}")
+
+
 def solve(config, grid, output, *, horizon=2.0, output_dt=0.1, order=2, cfl=0.8,
           local_precision="float64", history=True, device=None, group=None,
           shard_factory=None):
@@ -337,36 +354,53 @@ def solve(config, grid, output, *, horizon=2.0, output_dt=0.1, order=2, cfl=0.8,
             return RelativeShard(config, grid, b, e, order=order, cfl=cfl,
                                  local_precision=local_precision, device=dev)
 
-    shard = shard_factory(begin, end)
+    shard = None
+    fds = {}
     try:
-        shard.initialize()
-        solver = ShardedSolver([shard], DistExchange(shard, group))
-        slab_bytes = (N // grid.p_speeds) * 4
-        offset = begin * slab_bytes
-        fds = {name: os.open(output / name, os.O_WRONLY) for name in files}
+        # Set-up (the shard's device buffers, the initial field, the files):
+        # a rank that fails here tells the others before any collective of
+        # the solve, so no rank waits on a peer that has left.
+        error = None
         try:
-            def put(name, values, base=0):
-                os.pwrite(fds[name], np.ascontiguousarray(values, np.float32).tobytes(),
-                          base + offset)
+            shard = shard_factory(begin, end)
+            shard.initialize()
+            solver = ShardedSolver([shard], DistExchange(shard, group))
+            slab_bytes = (N // grid.p_speeds) * 4
+            offset = begin * slab_bytes
+            fds = {name: os.open(output / name, os.O_WRONLY) for name in files}
+        except Exception as exc:
+            error = exc
+        _agree(error, group, "shard set-up")
 
-            if history:
-                put("fields.f32", shard.field())
-            update = 0.0
-            for k, goal in enumerate(times[1:], start=1):
-                t0 = time.perf_counter()
-                solver.advance(goal)
-                update += time.perf_counter() - t0
+        def put(name, values, base=0):
+            os.pwrite(fds[name], np.ascontiguousarray(values, np.float32).tobytes(),
+                      base + offset)
+
+        # Frames: every rank reports after each frame (one small collective
+        # per frame), so a failure in a frame's steps or its write stops every
+        # rank at that frame boundary.
+        update = 0.0
+        for k, goal in enumerate(times, start=0):
+            error = None
+            try:
+                if k > 0:
+                    t0 = time.perf_counter()
+                    solver.advance(goal)
+                    update += time.perf_counter() - t0
                 if history:
                     put("fields.f32", shard.field(), k * N * 4)
-            put("final.f32", shard.field())
-            put("arrival.f32", shard.arrival())
-        finally:
-            for fd in fds.values():
-                os.close(fd)
+                if k == len(times) - 1:
+                    put("final.f32", shard.field())
+                    put("arrival.f32", shard.arrival())
+            except Exception as exc:
+                error = exc
+            _agree(error, group, f"frame {k}")
         residual = solver.residual()
         steps = solver.steps
     finally:
-        if hasattr(shard, "close"):
+        for fd in fds.values():
+            os.close(fd)
+        if shard is not None and hasattr(shard, "close"):
             shard.close()
     dist.barrier(group)
     meta = {

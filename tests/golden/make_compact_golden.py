@@ -19,13 +19,15 @@ Run in a container where the reference tree is mounted:
 """
 
 import importlib.util
+import os
 from pathlib import Path
 import sys
 
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
-REFERENCE = Path("/root/reference")
+# the reference tree: PE_REFERENCE_ROOT, by default where it is mounted here
+REFERENCE = Path(os.environ.get("PE_REFERENCE_ROOT", "/root/reference"))
 
 # (name, seed, p states, p actions, e states, e actions, exit radius, backups)
 CASES = [

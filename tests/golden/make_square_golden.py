@@ -54,9 +54,11 @@ def reference_queries(options, r, tmp):
     """value() and field() of the reference's LocalTable (dp/table.py:17-123,
     imported read-only from the reference tree) on the executable's fields,
     at seeded random states."""
+    import os
     import sys
 
-    sys.path.insert(0, "/root/reference/src")
+    sys.path.insert(0, os.path.join(os.environ.get("PE_REFERENCE_ROOT", "/root/reference"),
+                                    "src"))
     from pursuit_evasion.dp.grid import GridSpec, output_times
     from pursuit_evasion.dp.table import LocalTable
     from pursuit_evasion.model import GameConfig, Vehicle

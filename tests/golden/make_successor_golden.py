@@ -11,13 +11,15 @@ Also stores known answers of integrated_speed.
 Run where the reference is mounted:  python tests/golden/make_successor_golden.py
 """
 
+import os
 from pathlib import Path
 import sys
 
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
-sys.path.insert(0, "/root/reference/src")
+# the reference tree: PE_REFERENCE_ROOT, by default where it is mounted here
+sys.path.insert(0, os.path.join(os.environ.get("PE_REFERENCE_ROOT", "/root/reference"), "src"))
 
 from pursuit_evasion.reversible.model import (  # noqa: E402
     ReversibleConfig,

@@ -237,3 +237,58 @@ def test_sharded_table_refuses_existing_output_on_every_rank(tmp_path):
         assert p.exitcode == 0
     assert results == [(0, "FileExistsError"), (1, "RuntimeError")]
     assert sorted(x.name for x in folder.iterdir()) == ["keep.txt"]
+
+
+def _failing_rank(rank, world, port, folder, out):
+    sys.path.insert(0, str(REPO))
+    import datetime
+
+    import torch.distributed as dist
+
+    from pursuit_evasion_b200.reversible import sharded
+    from tests import oracle_lib
+
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank,
+                            world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        oracle = oracle_lib.load()
+
+        def factory(b, e):
+            if rank == 1:  # as pe_relative_shard_create failing on one GPU
+                raise MemoryError("shard buffers do not fit")
+            return OracleShard(oracle, A3, CONFIG1_GRID, b, e)
+
+        try:
+            sharded.solve(A3, CONFIG1_GRID, folder, horizon=0.2, output_dt=0.1,
+                          shard_factory=factory)
+            out.put((rank, "solved", ""))
+        except (MemoryError, RuntimeError) as exc:
+            out.put((rank, type(exc).__name__, str(exc)))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_shard_failure_on_one_rank_stops_every_rank(tmp_path):
+    """The shard factory fails on rank 1 only: rank 1 raises its own error,
+    rank 0 learns of it at the set-up agreement and raises too, and both
+    leave before any halo exchange (no rank waits for a peer that left)."""
+    import time
+
+    import torch.multiprocessing as mp
+
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_failing_rank, args=(r, 2, port, str(tmp_path / "t"), out))
+             for r in range(2)]
+    t0 = time.monotonic()
+    for p in procs:
+        p.start()
+    results = sorted(out.get(timeout=180) for _ in procs)
+    for p in procs:
+        p.join(60)
+        assert p.exitcode == 0
+    assert time.monotonic() - t0 < 50  # well inside the 60 s group timeout
+    assert results[0][:2] == (0, "RuntimeError")
+    assert "rank 1 failed during shard set-up" in results[0][2]
+    assert results[1][:2] == (1, "MemoryError")

@@ -7,9 +7,16 @@ buffers.
 
 Checked through the C ABI against the existing entry point (a
 PE_LOCAL_F64 handle's pe_relative_step) on two calls in a row: the fields
-and arrival times must be identical bit for bit, and the second call must
-not change the device's free memory.  This file sorts last so that a run
-stopping at the first failure has run every other test first."""
+and arrival times must be identical bit for bit.  The CUDA runtime loads
+the library's device code lazily, so the first call may reserve the fixed
+array (about 16 MB) on the device: that call may take at most the array
+plus a module's rounding, and the second call must not change the device's
+free memory at all.  This file sorts last so that a run stopping at the
+first failure has run every other test first."""
+
+# g_step_scratch in capi_noalloc.cu: stats words, 2 x 1024 heading doubles
+# and PE_NOALLOC_MAX_CELLS floats of stage field
+SCRATCH_BYTES = 8 * (4 + 2 * 1024) + 4 * 4194304
 
 import ctypes
 
@@ -47,6 +54,7 @@ def test_step_without_allocation_equals_handle_step_twice():
     torch.cuda.synchronize(device)
 
     residual = ctypes.c_double()
+    free_first, _ = torch.cuda.mem_get_info(device)
     rc = lib.pe_relative_step_noalloc(ctypes.byref(params), field_a.data_ptr(),
                                       field_b.data_ptr(), arrival.data_ptr(), 0.0, dt,
                                       stream, ctypes.byref(residual))
@@ -54,8 +62,11 @@ def test_step_without_allocation_equals_handle_step_twice():
     np.testing.assert_array_equal(field_b.cpu().numpy().view(np.uint32), v1.view(np.uint32))
     np.testing.assert_array_equal(arrival.cpu().numpy().view(np.uint32), a1.view(np.uint32))
     assert residual.value == np.abs(v1.astype(np.float64) - v0).max()
-
     free_before, _ = torch.cuda.mem_get_info(device)
+    # the first call reserves at most the array (plus 2 MiB pages of the
+    # lazily loaded module); nothing when the module was loaded already
+    assert 0 <= free_first - free_before <= SCRATCH_BYTES + (8 << 20)
+
     rc = lib.pe_relative_step_noalloc(ctypes.byref(params), field_b.data_ptr(),
                                       field_a.data_ptr(), arrival.data_ptr(), dt, dt,
                                       stream, None)
