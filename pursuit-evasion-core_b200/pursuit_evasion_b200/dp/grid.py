@@ -1,82 +1,93 @@
-"""Grid of the 6D square game, [xP, yP, thetaP, xE, yE, thetaE]
-(src/pursuit_evasion/dp/grid.py:9-100)."""
+"""Grid of the legacy 6D square game, state order [xP, yP, thetaP, xE, yE,
+thetaE].
+
+The interface is the reference's (dp/grid.py:9-100): the GridSpec fields
+and their defaults, its validation errors, the `shape` / `states` / `axes`
+/ `spacings` properties and the metadata keys of `to_dict`, which the table
+folders carry; and `output_times`.  The surfaces and the time-step bound
+that the reference's Python backends build here are computed by this
+package's C ABI (pe_square_init, pe_square_dt_limit), so they are not
+repeated in Python.
+"""
 
 from __future__ import annotations
 
-from dataclasses import asdict, dataclass
+from dataclasses import dataclass
+import math
 
 import numpy as np
 
-from ..model import GameConfig
+_STATE_ORDER = ("xP", "yP", "thetaP", "xE", "yE", "thetaE")
+_PERIODIC = (2, 5)
+
+
+def _is_count(n):
+    return isinstance(n, (int, np.integer)) and not isinstance(n, bool)
 
 
 @dataclass(frozen=True)
 class GridSpec:
+    """`positions` nodes per position axis on [-extent, extent] and
+    `headings` periodic heading nodes from -pi, for each car."""
+
     positions: int = 17
     headings: int = 16
     extent: float = 3.5
 
     def __post_init__(self):
-        counts = (self.positions, self.headings)
-        if (any(not isinstance(n, (int, np.integer)) or isinstance(n, bool) for n in counts)
-                or self.positions < 5 or self.headings < 4):
+        if not (_is_count(self.positions) and _is_count(self.headings)
+                and self.positions >= 5 and self.headings >= 4):
             raise ValueError("Grid counts must be integers with at least five position "
                              "samples and four periodic headings.")
-        if not np.isfinite(self.extent) or self.extent <= 0:
+        if not (math.isfinite(self.extent) and self.extent > 0):
             raise ValueError("Grid extent must be finite and positive.")
+
+    # per-car axes: position, position, heading
+    def _position_axis(self):
+        return np.linspace(-self.extent, self.extent, self.positions)
+
+    def _heading_axis(self):
+        # node k at k * 2 pi / headings - pi, rounded as the tables' writer does
+        return np.arange(self.headings) * 2 * np.pi / self.headings - np.pi
 
     @property
     def shape(self):
-        n, h = self.positions, self.headings
-        return (n, n, h, n, n, h)
+        car = (self.positions, self.positions, self.headings)
+        return car + car
 
     @property
     def states(self):
-        return self.positions ** 4 * self.headings ** 2
+        return int(np.prod(self.shape))
 
     @property
     def axes(self):
-        x = np.linspace(-self.extent, self.extent, self.positions)
-        theta = -np.pi + np.arange(self.headings) * 2 * np.pi / self.headings
-        return (x, x, theta, x, x, theta)
+        x, theta = self._position_axis(), self._heading_axis()
+        return (x, x, theta) * 2
 
     @property
     def spacings(self):
-        d = 2 * self.extent / (self.positions - 1)
-        h = 2 * np.pi / self.headings
-        return (d, d, h, d, d, h)
+        car = (2 * self.extent / (self.positions - 1),) * 2 + (2 * np.pi / self.headings,)
+        return car * 2
 
     def to_dict(self):
-        return dict(**asdict(self), shape=list(self.shape), states=self.states,
-                    spacings=list(self.spacings), periodic_axes=[2, 5],
-                    state_order=["xP", "yP", "thetaP", "xE", "yE", "thetaE"])
-
-
-def target_and_avoid(grid: GridSpec, config: GameConfig, dtype=np.float32):
-    """Target: capture or evader boundary fault; avoid: pursuer boundary
-    fault (signed, zero-sublevel convention, with a 1e-6 margin that makes a
-    pursuer exactly on the wall lose)."""
-    if grid.extent <= config.arena_half_width:
-        raise ValueError("The numerical domain must extend outside the physical square.")
-    x = np.asarray(grid.axes[0], dtype=dtype)
-    xp, yp = x[:, None, None, None, None, None], x[None, :, None, None, None, None]
-    xe, ye = x[None, None, None, :, None, None], x[None, None, None, None, :, None]
-    capture = np.sqrt((xp - xe) ** 2 + (yp - ye) ** 2) - config.capture_radius
-    e_fault = config.arena_half_width - np.maximum(abs(xe), abs(ye))
-    target = np.broadcast_to(np.minimum(capture, e_fault), grid.shape).copy()
-    avoid = np.broadcast_to(np.maximum(abs(xp), abs(yp)) - config.arena_half_width + 1e-6,
-                            grid.shape).copy()
-    return target.astype(dtype, copy=False), avoid.astype(dtype, copy=False)
+        return {
+            "positions": self.positions,
+            "headings": self.headings,
+            "extent": self.extent,
+            "shape": list(self.shape),
+            "states": self.states,
+            "spacings": list(self.spacings),
+            "periodic_axes": list(_PERIODIC),
+            "state_order": list(_STATE_ORDER),
+        }
 
 
 def output_times(horizon, output_dt):
-    if not np.isfinite([horizon, output_dt]).all() or horizon <= 0 or output_dt <= 0:
+    """Frame times 0, dt, 2 dt, ... up to and including `horizon` (the last
+    interval may be shorter)."""
+    if not (np.isfinite(horizon) and np.isfinite(output_dt) and horizon > 0
+            and output_dt > 0):
         raise ValueError("Horizon and output spacing must be finite and positive.")
-    times = np.minimum(np.arange(int(np.ceil(horizon / output_dt)) + 1) * output_dt, horizon)
-    return np.unique(times)
-
-
-def global_rate_bound(grid: GridSpec, config: GameConfig):
-    dx, _, dh, *_ = grid.spacings
-    return (2 * (config.pursuer.speed + config.evader.speed) / dx
-            + (config.pursuer.max_turn_rate + config.evader.max_turn_rate) / dh)
+    frames = int(np.ceil(horizon / output_dt))
+    times = [min(k * output_dt, horizon) for k in range(frames + 1)]
+    return np.array(sorted(set(times)))
