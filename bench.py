@@ -18,9 +18,11 @@ memory and the final field and arrival times read back every step.  The
 field (357.7 MB) is larger than the 126 MB L2, so no flush is needed between
 iterations.
 
-Multi-GPU (torchrun): every rank solves its own table (independent replicas,
-weak scaling, no data-path collective); `value` = all ranks' cell-backups over
-the slowest rank's device time.
+Multi-GPU (torchrun): by default the N ranks solve ONE table, each owning a
+range of pursuer-speed (vP) slabs, with NCCL halo exchanges after every stage
+(strong scaling: `value` = the table's cell-backups over the slowest rank's
+device time); `--mode replicas` gives every rank its own table instead (weak
+scaling, no data-path collective).
 
 --impl reference runs the reference's own CPU implementation of the path
 (native_relative.cpp compiled from the reference sources into
@@ -381,6 +383,61 @@ def world8d_section(steps=200):
             "last_residual": residual}
 
 
+def fp64_section(float32_table):
+    """The error of the float32 tables at the 3.0 s horizon against FP64
+    storage on the 89M-cell grid, on the 1/8-subsampled tile (every 8th x,
+    y and psi node, all speeds): the FP64-storage solve (the FP64 oracle's
+    stage on the GPU, bit-identical to it) to the same horizon, the bench's
+    own float32-local table (`float32_table`), and the exact path (float32
+    storage, double local arithmetic: the reference's arithmetic and the
+    default of free_dp.solve), whose device time is reported too."""
+    import torch
+    from pursuit_evasion_b200.reversible.fp64_table import RelativeSolverF64, subsampled_error
+    from pursuit_evasion_b200.reversible.free_dp import RelativeGrid, output_times
+    from pursuit_evasion_b200.reversible.relative_solver import RelativeSolver
+
+    grid = RelativeGrid(**GRID)
+    goals = output_times(HORIZON, OUTPUT_DT)[1:]
+    stream = _timing_stream()
+
+    def timed_solve(solver):
+        solver.set_stream(stream.cuda_stream)
+        solver.initialize()
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        for goal in goals:
+            solver.advance(goal)
+        t1.record(stream)
+        torch.cuda.synchronize()
+        return t0.elapsed_time(t1), solver.steps, solver.field()
+
+    with RelativeSolverF64(a3_config(), grid) as r:
+        ms64, steps64, reference = timed_solve(r)
+    with RelativeSolver(a3_config(), grid, local_precision="float64") as s:
+        ms_exact, steps, exact = timed_solve(s)
+    cells = grid.states
+    fast = np.asarray(float32_table).reshape(grid.shape)
+    return {
+        "workload": f"RelativeGrid(65,48,21,21,8.0) reversible_free_a3, CFL 0.8, {HORIZON} s = "
+                    f"{steps} RK2 steps; errors on every 8th x, y, psi node and all speeds",
+        "target_max_abs": 1e-4,
+        "float32_local_vs_fp64": subsampled_error(fast, reference, 8),
+        "exact_path_vs_fp64": subsampled_error(exact, reference, 8),
+        "exact_path": {"value": cells * 2 * steps / (ms_exact / 1e3), "unit": METRIC,
+                       "ms_per_rk2_step": ms_exact / steps,
+                       "note": "float32 storage, double local arithmetic in the reference's "
+                               "operation order (bit-identical to native_relative.cpp)"},
+        "fp64_storage_solve": {"ms_per_rk2_step": ms64 / steps64, "steps": steps64},
+    }
+
+
+# pair_value of csrc/semilag5d_tiled.cu: successor position (2 packed FMA
+# pairs, 8), floor and weights (3 packed adds and a subtraction, 8), three
+# packed bilinear lerps (18) and the heading lerp (3)
+SL_FLOPS_PER_EVAL = 37
+SL_SMEM_BYTES_PER_EVAL = 4 * 8 + 32
+
+
 def semilag_cpu_baseline(grid, dt, mode, sample_cells=1 << 17):
     """The FP64 oracle (oracle/semilag5d.c, OpenMP) on a bounded sample: one
     backup of `sample_cells` random cells of the same grid and field."""
@@ -430,11 +487,23 @@ def semilag_section(with_cpu=True):
         torch.cuda.synchronize()
         ms_total = t0.elapsed_time(t1)
         ms, n = s.kernel_time()
+        evaluations = s.evaluations()
         s.profile(False)
         dt, kernel = s.dt, s.kernel
     cells = grid.states
     peak, _ = measured_peaks()
     achieved = 8 * cells * n / (ms / 1e3) / 1e9
+    # On-chip rates of the tiled backup from its counted action-pair
+    # evaluations: each is SL_FLOPS_PER_EVAL FP32 operations and
+    # SL_SMEM_BYTES_PER_EVAL bytes of shared-memory reads (the 4 float2
+    # corners and the 32-byte pair entry), against the B200's FP32 and
+    # shared-memory peaks at the sampled SM clock.
+    seconds = ms / 1e3
+    sm_clock_ghz = 1.965
+    fp32_peak = 148 * 128 * 2 * sm_clock_ghz * 1e9
+    smem_peak = 148 * 128 * sm_clock_ghz * 1e9
+    flops = evaluations * SL_FLOPS_PER_EVAL / seconds
+    smem = evaluations * SL_SMEM_BYTES_PER_EVAL / seconds
     out = {"workload": f"semilag5d tube RelativeGrid(65,48,21,21,8.0) reversible_free_a3, "
                        f"dt {dt:.6f} s (interpolation CFL), {backups} backups = "
                        f"{HORIZON} s horizon, 9x9 held actions, {kernel} kernel",
@@ -444,7 +513,18 @@ def semilag_section(with_cpu=True):
                                  "fraction reported",
                         "achieved": achieved, "peak": peak, "unit": "GB/s",
                         "frac": achieved / peak,
-                        "algorithmic_bytes_per_launch": 8 * cells}}
+                        "algorithmic_bytes_per_launch": 8 * cells},
+           "on_chip": {"evaluations_per_cell": evaluations / (cells * n) if n else None,
+                       "flops_per_evaluation": SL_FLOPS_PER_EVAL,
+                       "achieved_tflops": flops / 1e12,
+                       "fp32_peak_tflops": fp32_peak / 1e12,
+                       "fp32_frac": flops / fp32_peak,
+                       "smem_bytes_per_evaluation": SL_SMEM_BYTES_PER_EVAL,
+                       "achieved_smem_tbs": smem / 1e12,
+                       "smem_peak_tbs": smem_peak / 1e12,
+                       "smem_frac": smem / smem_peak,
+                       "peaks": "148 SMs x (128 FP32 lanes x 2, 128 B shared memory) per "
+                                "clock at 1.965 GHz"}}
     if with_cpu:
         try:
             out["cpu_baseline"] = semilag_cpu_baseline(grid, dt, "tube")
@@ -740,6 +820,135 @@ def run_case(name, repeats):
     print(f"case {name}: ok", flush=True)
 
 
+def run_sharded(args, world, rank, local, *, backend="nccl", shard_factory=None, grid=None):
+    """`--gpus N` (N > 1, the default mode): ONE config-2 table solved by N
+    ranks, each owning a contiguous range of pursuer-speed (vP) slabs with
+    `order` halo slabs per neighbour, refreshed after every stage by NCCL
+    send/recv between neighbouring ranks; the residual is an all-reduce max
+    (pursuit_evasion_b200.reversible.sharded).  Strong scaling: the total
+    work is fixed, `value` = all cells x stages / the slowest rank's device
+    time.  `e2e` adds, per solve, each rank's upload of its buffer slabs of
+    the initial field and the read-back of its owned slabs of the final
+    field and arrival times.  The GPU stage kernel is the single-grid one, so
+    the table is bit-identical to the one-GPU solve.  The halo slabs are
+    copied into each rank's own buffer: every load of the stage kernel reads
+    this GPU's memory.  `backend`, `shard_factory` and `grid` let CPU tests
+    drive the same code with gloo ranks and oracle shards."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    from pursuit_evasion_b200.reversible.free_dp import RelativeGrid, output_times
+    from pursuit_evasion_b200.reversible.sharded import (
+        DistExchange, RelativeShard, ShardedSolver, partition)
+
+    gpu = backend == "nccl"
+    if gpu:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180),
+                                device_id=torch.device("cuda", local))
+    elif not dist.is_initialized():
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    grid = grid or RelativeGrid(**GRID)
+    ranges = partition(grid.p_speeds, world, 2)
+    begin, end = ranges[rank]
+    if shard_factory is None:
+        def shard_factory(b, e):
+            return RelativeShard(a3_config(), grid, b, e, local_precision=args.precision,
+                                 device=local)
+    shard = shard_factory(begin, end)
+    frame_times = output_times(HORIZON, OUTPUT_DT)[1:]
+    cells = grid.states
+    try:
+        solver = ShardedSolver([shard], DistExchange(shard))
+        stream = solver._stream  # the shard's stages and the NCCL exchanges
+
+        def one_solve(initial=None, read_back=False):
+            shard.initialize(initial)
+            solver.time, solver.steps = 0.0, 0
+            for goal in frame_times:
+                solver.advance(goal)
+            if read_back:
+                shard.field()
+                shard.arrival()
+
+        def timed(count, **kw):
+            """Device time of `count` solves on the solver's stream (CUDA
+            events), or wall time on CPU ranks."""
+            if gpu:
+                torch.cuda.synchronize()
+            dist.barrier()
+            if gpu:
+                t0, t1 = (torch.cuda.Event(enable_timing=True),
+                          torch.cuda.Event(enable_timing=True))
+                t0.record(stream)
+            else:
+                w0 = time.perf_counter()
+            for _ in range(count):
+                one_solve(**kw)
+            if gpu:
+                t1.record(stream)
+                torch.cuda.synchronize()
+                return t0.elapsed_time(t1)
+            return (time.perf_counter() - w0) * 1e3
+
+        for _ in range(args.warmup):
+            one_solve()
+        steps = solver.steps
+        clocks = ClockSampler(local) if gpu else None
+        if clocks:
+            clocks.start()
+        ms = timed(args.steps)
+        clock_info = clocks.stop() if clocks else None
+        e2e_ms = timed(args.steps, initial=shard_initial_field(grid), read_back=True)
+        t = torch.tensor([ms, e2e_ms], dtype=torch.float64,
+                         device=f"cuda:{local}" if gpu else "cpu")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, e2e_ms = t.tolist()
+        line = None
+        if rank == 0:
+            backups = cells * 2 * steps * args.steps
+            slab = cells // grid.p_speeds
+            own = [(e - b) * slab for b, e in ranges]
+            buf = [(min(grid.p_speeds, e + 2) - max(0, b - 2)) * slab for b, e in ranges]
+            line = {
+                "metric": METRIC, "value": backups / (ms / 1e3), "unit": METRIC,
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": ms / args.steps, "higher_is_better": True,
+                "scaling": "strong", "vs_baseline": None,
+                "dtype": "f32" if args.precision == "float32" else "f32 storage, f64 local",
+                "data": "synthetic (deterministic grid, no dataset)",
+                "config": bench_config(cells),
+                "run": {"stages_per_step": 2 * steps, "precision": args.precision,
+                        "parallelism": f"vP slabs x{world} (NCCL halo exchange)",
+                        "vp_ranges": [list(r) for r in ranges]},
+                "e2e": {"value": backups / (e2e_ms / 1e3), "unit": METRIC,
+                        "h2d_bytes_per_step": 4 * sum(buf),
+                        "d2h_bytes_per_step": 8 * sum(own),
+                        "ms_per_step": e2e_ms / args.steps},
+                "gpu_launches": int(world * 2 * steps * args.steps) if gpu else 0,
+                "clocks": clock_info,
+                "timing": "CUDA events on each rank's solve stream, max over ranks",
+            }
+            print(json.dumps(line), flush=True)
+        dist.barrier()
+        return line
+    finally:
+        if hasattr(shard, "close"):
+            shard.close()
+        if gpu:
+            dist.destroy_process_group()
+
+
+def shard_initial_field(grid):
+    """The capture field hypot(x, y) - r as a host array (the e2e input)."""
+    x = np.linspace(-grid.extent, grid.extent, grid.positions)
+    plane = (np.hypot(x[None, :], x[:, None]) - A3_LIMITS["capture_radius"]).astype(np.float32)
+    reps = grid.states // plane.size
+    return np.broadcast_to(plane, (reps,) + plane.shape).reshape(-1)
+
+
 def run_ours(args, world, rank, local):
     import torch
 
@@ -871,7 +1080,9 @@ def run_ours(args, world, rank, local):
         # side measurements are single-GPU; with replicas they would keep the
         # other ranks waiting at the final barrier
         if not args.no_sections and world == 1:
-            for key, fn in (("world8d", world8d_section),
+            final_table = host_field.numpy().copy()
+            for key, fn in (("fp64_error", lambda: fp64_section(final_table)),
+                            ("world8d", world8d_section),
                             ("semilag5d", lambda: semilag_section(not args.no_cpu_baseline)),
                             ("batch", batch_section),
                             ("compact8d", lambda: compact_section(
@@ -901,6 +1112,9 @@ def main():
     parser.add_argument("--steps", type=int, default=5)
     parser.add_argument("--warmup", type=int, default=3)
     parser.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    parser.add_argument("--mode", choices=["sharded", "replicas"], default="sharded",
+                        help="with --gpus N > 1: one table in vP slabs over the N ranks "
+                             "(strong scaling, default) or N independent tables")
     parser.add_argument("--precision", choices=["float32", "float64"],
                         default="float32")
     parser.add_argument("--no-cpu-baseline", action="store_true")
@@ -924,6 +1138,8 @@ def main():
     world, rank, local = dist_setup()
     if args.impl == "reference":
         run_reference_arm(args, world, rank)
+    elif world > 1 and args.mode == "sharded":
+        run_sharded(args, world, rank, local)
     else:
         run_ours(args, world, rank, local)
 
