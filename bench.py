@@ -545,9 +545,76 @@ def converge_section(samples, epochs):
     grid = RelativeGrid(**GRID)
     dt = interpolation_cfl_dt(a3_config(), grid)
     coarse = RelativeGrid(33, 24, 11, 11, GRID["extent"])
-    result, _ = time_to_converged(a3_config(), grid, dt=dt, tol=1e-5, samples=samples,
-                                  epochs=epochs, batch=8192, coarse_grid=coarse)
-    return result
+    result, net = time_to_converged(a3_config(), grid, dt=dt, tol=1e-5, samples=samples,
+                                    epochs=epochs, batch=8192, coarse_grid=coarse)
+    return result, net
+
+
+def learned_section(net5, samples, epochs, batch=8192, steps8d=200):
+    """The learned surrogate beyond the 5D warm start: (1) trained by the
+    package's kernels on 2^22 node samples of the 8D contact table
+    (WorldGrid(11,9,7,7,3.0) after `steps8d` RK2 steps from the rectangle
+    contact field), its error against that table on every node; (2) online
+    query latency of the 5D surrogate `net5` for batches of 4096 relative
+    states (encode + four tensor-core layers + head), CUDA events per query,
+    training charged separately."""
+    import torch
+    from pursuit_evasion_b200.learned.mlp import ValueMLP
+    from pursuit_evasion_b200.learned.train import (
+        WorldNodeSampler, predict_nodes, predict_states, train)
+    from pursuit_evasion_b200.reversible.world_dp import WorldGrid, WorldSolver
+
+    out = {}
+    grid = WorldGrid(11, 9, 7, 7, 3.0)
+    dev = torch.device("cuda", 0)
+    with WorldSolver(a3_config(), grid, avoid=False, fast=True) as w:
+        w.init_contact((0.5, 0.3), (0.5, 0.3))
+        for _ in range(steps8d):
+            w.step(w.dt_limit)
+        table = torch.from_numpy(w.field().reshape(-1)).to(dev)
+    net = ValueMLP(WorldNodeSampler.in_features, seed=0, max_batch=batch)
+    losses, train_s = train(net, WorldNodeSampler(a3_config(), grid, table), samples=samples,
+                            epochs=epochs, batch=batch)
+    net.set_batch(1 << 17)
+    pred = predict_nodes(net, WorldNodeSampler(a3_config(), grid),
+                         torch.empty(grid.states, device=dev), chunk=1 << 17)
+    err = (pred - table).abs()
+    out["world8d_training"] = {
+        "table": f"WorldGrid(11,9,7,7,3.0) contact game after {steps8d} RK2 steps "
+                 f"({grid.states} nodes)",
+        "samples": samples, "epochs": epochs, "batch": batch, "train_seconds": train_s,
+        "final_mse": losses[-1], "max_abs_error": float(err.max()),
+        "mean_abs_error": float(err.mean()),
+        "p99_abs_error": float(torch.quantile(err[::64], 0.99))}
+    del net, pred, table
+    if net5 is not None:
+        from pursuit_evasion_b200.reversible.free_dp import RelativeGrid
+
+        g5 = RelativeGrid(**GRID)
+        net5.set_batch(4096)
+        rng = np.random.default_rng(0)
+        lo = np.array([-g5.extent, -g5.extent, -np.pi, -1.0, -0.5])
+        hi = np.array([g5.extent, g5.extent, np.pi, 2.0, 1.0])
+        states = torch.tensor(rng.uniform(lo, hi, size=(4096, 5)), dtype=torch.float32,
+                              device=dev)
+        stream = torch.cuda.current_stream(dev)
+        for _ in range(10):
+            predict_states(net5, a3_config(), g5.extent, states)
+        times = []
+        for _ in range(200):
+            t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            t0.record(stream)
+            predict_states(net5, a3_config(), g5.extent, states)
+            t1.record(stream)
+            t1.synchronize()
+            times.append(t0.elapsed_time(t1))
+        times = np.array(times)
+        out["query_latency"] = {
+            "batch": 4096, "queries": len(times), "p50_ms": float(np.median(times)),
+            "p95_ms": float(np.quantile(times, 0.95)),
+            "states_per_s": 4096 / (float(np.median(times)) / 1e3),
+            "surrogate": "5D minimum-time surrogate of the converged section"}
+    return out
 
 
 def batch_section(seed=0, count=256):
@@ -1093,11 +1160,16 @@ def run_ours(args, world, rank, local):
                     line[key] = fn()
                 except Exception as exc:  # report, keep the headline line
                     line[key] = {"error": repr(exc)}
+            net5 = None
             if args.converge:
                 try:
-                    line["converged"] = converge_section(args.samples, args.epochs)
+                    line["converged"], net5 = converge_section(args.samples, args.epochs)
                 except Exception as exc:
                     line["converged"] = {"error": repr(exc)}
+                try:
+                    line["learned"] = learned_section(net5, args.samples, args.epochs)
+                except Exception as exc:
+                    line["learned"] = {"error": repr(exc)}
         print(json.dumps(line), flush=True)
     solver.close()
     if world > 1:

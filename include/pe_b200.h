@@ -216,6 +216,33 @@ int pe_relative_step_noalloc(const pe_relative_params *params,
                              void *cuda_stream, double *residual);
 
 /* ------------------------------------------------------------------------
+ * FP64-storage relative 5D solve: the exact ENO/LF stage of
+ * native_relative.cpp:38-172 with double values instead of float32 (the
+ * reference stores float32 only; its CPU restatement with double storage is
+ * the FP64 oracle po_rel_stage_f64 of oracle/relative5d.c, which this
+ * reproduces bit for bit).  It exists to measure the error of
+ * float32-storage tables against FP64 at sizes the CPU cannot reach.
+ * Dense layout [vP, vE, psi, y, x]; initial field hypot(x, y) - r in
+ * double; steps of min(cfl limit, goal - t) as pe_relative_advance; no
+ * arrival times.
+ * ------------------------------------------------------------------------ */
+typedef struct pe_relative_f64 pe_relative_f64;
+
+int pe_relative_f64_create(const pe_relative_params *params, pe_relative_f64 **out);
+int pe_relative_f64_destroy(pe_relative_f64 *h);
+int pe_relative_f64_set_stream(pe_relative_f64 *h, void *cuda_stream);
+int pe_relative_f64_initialize(pe_relative_f64 *h);
+int pe_relative_f64_step(pe_relative_f64 *h, double dt);
+int pe_relative_f64_advance(pe_relative_f64 *h, double goal, int64_t *steps_taken);
+int pe_relative_f64_time(const pe_relative_f64 *h, double *t, int64_t *steps,
+                         double *cfl_dt_limit);
+/* Waits; *residual = the last step's max |change|; PE_ENONFINITE if any
+ * update since initialisation was not finite. */
+int pe_relative_f64_stats(pe_relative_f64 *h, double *residual);
+/* Waits and copies the field (pe_relative_cells doubles) to host memory. */
+int pe_relative_f64_copy_field(pe_relative_f64 *h, double *host_dst);
+
+/* ------------------------------------------------------------------------
  * vP-slab shards of one relative 5D solve (grids larger than one GPU).
  *
  * The reference solves one grid in one process (native_relative.cpp:173-190
@@ -422,6 +449,12 @@ int pe_semilag_iterate(pe_semilag *h, int64_t max_iterations, double tol,
                        int32_t check_every, int64_t *iterations,
                        double *residual, int32_t *converged);
 int pe_semilag_residual(pe_semilag *h, double *residual);
+/* Waits; action-pair evaluations (one interpolated successor value each)
+ * of the tiled value backups since the last pe_semilag_init*: the probes,
+ * full reply scans and pruned replies of every live cell.  Divided by the
+ * cells and backups it is the work per cell behind the backup's on-chip
+ * rate; the generic kernel does not count (0). */
+int pe_semilag_evaluations(pe_semilag *h, int64_t *evaluations);
 int pe_semilag_copy_value(pe_semilag *h, float *host_value);
 /* Copy the value field into a dense device array on the handle's device. */
 int pe_semilag_copy_value_device(pe_semilag *h, float *device_value);

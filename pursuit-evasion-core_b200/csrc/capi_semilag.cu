@@ -459,6 +459,16 @@ int pe_semilag_residual(pe_semilag *h, double *residual) {
   return PE_OK;
 }
 
+int pe_semilag_evaluations(pe_semilag *h, int64_t *evaluations) {
+  int rc = enter(h);
+  if (rc) return rc;
+  if (!evaluations) return fail(PE_EINVAL, "evaluations is NULL");
+  rc = read_stats(h);
+  if (rc) return rc;
+  *evaluations = (int64_t)h->host_stats->evaluations;
+  return PE_OK;
+}
+
 int pe_semilag_copy_value(pe_semilag *h, float *host_value) {
   int rc = enter(h);
   if (rc) return rc;

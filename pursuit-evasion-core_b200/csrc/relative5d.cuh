@@ -40,6 +40,9 @@ struct Rel5Stats {
 struct Rel5Stage {
   const float *src;  // stage input
   float *dst;        // stage output (stage 2: also holds the step's old V)
+  // the same for the double-storage stage (rel5_stage_f64_storage)
+  const double *src64;
+  double *dst64;
   float *arrival;    // first-crossing time, NaN until the cell enters (padded)
   const double *sn, *cs;   // sin/cos of the heading axis, double
   const float *snf, *csf;  // the same, rounded to float
@@ -81,6 +84,17 @@ cudaError_t rel5_stage_f32(const Rel5Grid &g, const Rel5Tile &t,
 // built without contraction so it reproduces native_relative.cpp bit for bit.
 cudaError_t rel5_stage_f64(const Rel5Grid &g, const Rel5Stage &s, int blend,
                            cudaStream_t stream);
+
+// Double storage: the exact stage with double values in a dense layout
+// (g.xp == g.nx), no arrival times -- the FP64 oracle (po_rel_stage_f64 of
+// the CPU restatement) on the GPU, bit for bit.  Reads s.src64 (and s.dst64
+// for the blend), writes s.dst64.
+cudaError_t rel5_stage_f64_storage(const Rel5Grid &g, const Rel5Stage &s, int blend,
+                                   cudaStream_t stream);
+
+// Broadcast a dense (y, x) plane of double values over every (vP, vE, psi).
+cudaError_t rel5_broadcast_plane_f64(const Rel5Grid &g, const double *plane, double *field,
+                                     cudaStream_t stream);
 
 // Broadcast a (y, x) plane of initial values (dense, nx*nx) over every
 // (vP, vE, psi), zero the row padding, and set arrival = start_time where the

@@ -13,8 +13,20 @@ __device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
 __device__ __forceinline__ float2 sub2(float2 a, float2 b) {  // a - b
   return __ffma2_rn(b, f2(-1.f), a);
 }
+// ENO selection of the smaller second difference, ties to the second
+// argument (the reference's strict `<`): one compare on the magnitudes and
+// one select, written out so that no integer sign-masking is generated.
 __device__ __forceinline__ float eno_pick(float a, float b) {
-  return fabsf(a) < fabsf(b) ? a : b;
+  float r;
+  asm("{\n .reg .pred p;\n .reg .f32 ua, ub;\n abs.f32 ua, %1;\n abs.f32 ub, %2;\n"
+      " setp.lt.f32 p, ua, ub;\n selp.f32 %0, %1, %2, p;\n}"
+      : "=f"(r)
+      : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 pick2(float2 a, float2 b) {
+  return make_float2(eno_pick(a.x, b.x), eno_pick(a.y, b.y));
 }
 __device__ __forceinline__ float2 lo2(float4 v) { return make_float2(v.x, v.y); }
 __device__ __forceinline__ float2 hi2(float4 v) { return make_float2(v.z, v.w); }
@@ -103,6 +115,44 @@ __device__ __forceinline__ void slopes_x(const float w[8], int x0, int nx,
     for (int i = 0; i < 4; i++)
       if (i == i_end) lo[i] = hi[i] = e[i + 1];
   }
+}
+
+// slopes_x with the end rules at compile-time positions.  XR = nx mod 4
+// fixes which cell of its chunk x = nx - 1 is (IEND) and which window node
+// of its chunk x = nx - 2 is (KEND); the per-thread flags say whether this
+// chunk holds x = 0, the node KEND, or the cell IEND.  The results equal
+// slopes_x<ORDER, true> bit for bit.
+template <int ORDER, int XR>
+__device__ __forceinline__ void slopes_x_fixed(const float w[8], bool first, bool kend_chunk,
+                                               bool iend_chunk, float lo[4], float hi[4]) {
+  constexpr int KEND = XR >= 2 ? XR : XR + 4;
+  constexpr int IEND = (XR + 3) & 3;
+  float e[7];
+#pragma unroll
+  for (int i = 0; i < 7; i++) e[i] = w[i + 1] - w[i];
+  if (ORDER == 1) {
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      lo[i] = e[i + 1];
+      hi[i] = e[i + 2];
+    }
+  } else {
+    float d2[7];
+#pragma unroll
+    for (int k = 1; k < 7; k++) d2[k] = e[k] - e[k - 1];
+    float m[7];
+#pragma unroll
+    for (int k = 2; k < 7; k++) m[k] = eno_pick(d2[k - 1], d2[k]);
+    if (first) m[3] = d2[3];
+    if (kend_chunk) m[KEND + 1] = d2[KEND];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      lo[i] = fmaf(0.5f, m[i + 2], e[i + 1]);
+      hi[i] = fmaf(-0.5f, m[i + 3], e[i + 2]);
+    }
+  }
+  if (first) lo[0] = hi[0] = e[2];
+  if (iend_chunk) lo[IEND] = hi[IEND] = e[IEND + 1];
 }
 
 }  // namespace eno32

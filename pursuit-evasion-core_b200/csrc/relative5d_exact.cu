@@ -11,7 +11,7 @@
 namespace pe {
 namespace {
 
-template <int ORDER, int BLEND>
+template <int ORDER, int BLEND, typename T = float>
 __global__ void __launch_bounds__(128)
     rel5_stage_exact_kernel(const Rel5Grid g, const Rel5Stage s) {
   __shared__ double scratch[4];
@@ -24,8 +24,8 @@ __global__ void __launch_bounds__(128)
     const int ie = blockIdx.z % g.nve, iv = g.own_lo + (int)blockIdx.z / g.nve;
     const int64_t j = ((int64_t)(iv - g.slab_lo) * g.nve + ie) * g.se + (int64_t)ip * g.sp +
                       (int64_t)iy * g.sy + ix;
-    exact::cell_update<ORDER, BLEND>(g, s, ix, iy, ip, iv, ie, j, change_abs, change_up,
-                                     bad);
+    exact::cell_update<ORDER, BLEND, T>(g, s, ix, iy, ip, iv, ie, j, change_abs, change_up,
+                                        bad);
   }
   if (__syncthreads_or(bad) && threadIdx.x == 0)
     atomicOr(&s.stats->nonfinite, 1u);
@@ -39,7 +39,34 @@ __global__ void __launch_bounds__(128)
   }
 }
 
+__global__ void rel5_broadcast_f64_kernel(const double *__restrict__ plane,
+                                          double *__restrict__ field, int64_t n,
+                                          int64_t plane_size) {
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n;
+       j += (int64_t)gridDim.x * blockDim.x)
+    field[j] = plane[j % plane_size];
+}
+
 }  // namespace
+
+cudaError_t rel5_broadcast_plane_f64(const Rel5Grid &g, const double *plane, double *field,
+                                     cudaStream_t stream) {
+  rel5_broadcast_f64_kernel<<<148 * 16, 256, 0, stream>>>(plane, field, g.n, g.sp);
+  return cudaGetLastError();
+}
+
+cudaError_t rel5_stage_f64_storage(const Rel5Grid &g, const Rel5Stage &s, int blend,
+                                   cudaStream_t stream) {
+  const int threads = 128;
+  const dim3 grid((g.nx * g.nx + threads - 1) / threads, g.nh, g.nvp * g.nve);
+  if (g.order == 1)
+    rel5_stage_exact_kernel<1, 0, double><<<grid, threads, 0, stream>>>(g, s);
+  else if (blend)
+    rel5_stage_exact_kernel<2, 1, double><<<grid, threads, 0, stream>>>(g, s);
+  else
+    rel5_stage_exact_kernel<2, 0, double><<<grid, threads, 0, stream>>>(g, s);
+  return cudaGetLastError();
+}
 
 cudaError_t rel5_stage_f64(const Rel5Grid &g, const Rel5Stage &s, int blend,
                            cudaStream_t stream) {

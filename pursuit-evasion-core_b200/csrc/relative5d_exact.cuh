@@ -3,7 +3,9 @@
 //
 // Double local arithmetic evaluated in the order of the reference
 // executable (native_relative.cpp:38-67 slopes, :124-172 stage), float32
-// storage.  Every translation unit that includes this header is compiled
+// storage -- or, with T = double, double storage: the FP64 oracle of
+// oracle/relative5d.c (po_rel_stage_f64) on the GPU, used to measure the
+// error of float32-storage tables.  Every translation unit that includes this header is compiled
 // with -fmad=false (no multiply-add contraction, IEEE double division), so
 // each stored float equals the reference CPU's bit for bit.
 #pragma once
@@ -17,8 +19,8 @@ struct Slopes {
 };
 
 // One-axis ENO slopes at node j (native_relative.cpp:38-67).
-template <int ORDER>
-__device__ __forceinline__ Slopes eno_axis(const float *__restrict__ s,
+template <int ORDER, typename T>
+__device__ __forceinline__ Slopes eno_axis(const T *__restrict__ s,
                                            int64_t j, int64_t stride, int pos,
                                            int n, double h, bool periodic) {
   Slopes r;
@@ -80,17 +82,40 @@ __device__ __forceinline__ double block_max(double v, double *scratch) {
 // s.dst and the arrival time; accumulates the sup-norm change and the
 // largest increase of the step (stage 2 / RK1 only) and flags non-finite
 // updates.
-template <int ORDER, int BLEND>
+template <typename T>
+__device__ __forceinline__ const T *stage_src(const Rel5Stage &s);
+template <>
+__device__ __forceinline__ const float *stage_src<float>(const Rel5Stage &s) {
+  return s.src;
+}
+template <>
+__device__ __forceinline__ const double *stage_src<double>(const Rel5Stage &s) {
+  return s.src64;
+}
+template <typename T>
+__device__ __forceinline__ T *stage_dst(const Rel5Stage &s);
+template <>
+__device__ __forceinline__ float *stage_dst<float>(const Rel5Stage &s) {
+  return s.dst;
+}
+template <>
+__device__ __forceinline__ double *stage_dst<double>(const Rel5Stage &s) {
+  return s.dst64;
+}
+
+template <int ORDER, int BLEND, typename T = float>
 __device__ __forceinline__ void cell_update(const Rel5Grid &g, const Rel5Stage &s, int ix,
                                             int iy, int ip, int iv, int ie, int64_t j,
                                             double &change_abs, double &change_up,
                                             bool &bad) {
-  const float *__restrict__ src = s.src;
+  constexpr bool F64 = sizeof(T) == sizeof(double);
+  const T *__restrict__ src = stage_src<T>(s);
+  T *__restrict__ dstp = stage_dst<T>(s);
 
   const double x = -g.extent + ix * g.dx;
   const double y = -g.extent + iy * g.dx;
   if (s.exit_r2 > 0 && x * x + y * y > s.exit_r2) {  // held at the exit value
-    s.dst[j] = (float)s.exit_r;
+    dstp[j] = (T)s.exit_r;
     change_abs = change_up = 0;
     return;
   }
@@ -98,11 +123,11 @@ __device__ __forceinline__ void cell_update(const Rel5Grid &g, const Rel5Stage &
   const double wp = fabs(vp) * g.curv_p, we = fabs(ve) * g.curv_e;
   const double bx = ve * s.cs[ip] - vp, by = ve * s.sn[ip];
 
-  const Slopes sx = eno_axis<ORDER>(src, j, 1, ix, g.nx, g.dx, false);
-  const Slopes sy = eno_axis<ORDER>(src, j, g.sy, iy, g.nx, g.dx, false);
-  const Slopes sp = eno_axis<ORDER>(src, j, g.sp, ip, g.nh, g.dphi, true);
-  const Slopes sv = eno_axis<ORDER>(src, j, g.sv, iv, g.nvp, g.dvp, false);
-  const Slopes se = eno_axis<ORDER>(src, j, g.se, ie, g.nve, g.dve, false);
+  const Slopes sx = eno_axis<ORDER, T>(src, j, 1, ix, g.nx, g.dx, false);
+  const Slopes sy = eno_axis<ORDER, T>(src, j, g.sy, iy, g.nx, g.dx, false);
+  const Slopes sp = eno_axis<ORDER, T>(src, j, g.sp, ip, g.nh, g.dphi, true);
+  const Slopes sv = eno_axis<ORDER, T>(src, j, g.sv, iv, g.nvp, g.dvp, false);
+  const Slopes se = eno_axis<ORDER, T>(src, j, g.se, ie, g.nve, g.dve, false);
 
   const double gx = .5 * (sx.lo + sx.hi), gy = .5 * (sy.lo + sy.hi),
                gp = .5 * (sp.lo + sp.hi), gv = .5 * (sv.lo + sv.hi),
@@ -121,14 +146,22 @@ __device__ __forceinline__ void cell_update(const Rel5Grid &g, const Rel5Stage &
              g.acc_e * (se.hi - se.lo));
 
   const double old = src[j];
-  const double prev = BLEND ? (double)s.dst[j] : old;
+  const double prev = BLEND ? (double)dstp[j] : old;
   double value = old + s.dt * (H < 0. ? H : 0.);
   if (BLEND) value = .5 * (prev + value);
-  if (!isfinite(value)) {
+  if (F64) {  // double storage (po_rel_stage_f64): stored as computed, no arrival
+    if (!isfinite(value)) bad = true;
+    dstp[j] = (T)value;
+    if (BLEND || ORDER == 1) {
+      const double change = value - prev;
+      change_abs = fabs(change);
+      change_up = change > 0 ? change : 0;
+    }
+  } else if (!isfinite(value)) {
     bad = true;
   } else {
     const float stored = (float)value;
-    s.dst[j] = stored;
+    dstp[j] = (T)stored;
     if (BLEND || ORDER == 1) {
       const double change = (double)stored - prev;
       change_abs = fabs(change);

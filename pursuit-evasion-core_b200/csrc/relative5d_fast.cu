@@ -3,27 +3,42 @@
 //
 // Work decomposition.  A work item is `rows` consecutive y rows of one
 // (vP, vE) pair over `psi_chunk` consecutive headings; a persistent CTA walks
-// a strided list of items.  A thread owns one 16-byte chunk of 4 consecutive
-// x cells in one row.  For each heading step the CTA needs, in shared memory:
-//   * its own (vP, vE) plane, rows y0-2 .. y0+R+1 (the y halo), in a ring of
-//     6 slots: the current heading for the y and x neighbours and the heading
-//     two ahead to refill each thread's 5-heading register window;
-//   * the 8 neighbour planes (vE+-1, vE+-2, vP+-1, vP+-2) at the current
-//     heading, rows y0 .. y0+R-1, in a ring of 2 slots.
+// a strided list of items.  A consumer thread owns one 16-byte chunk of 4
+// consecutive x cells in one row and walks the item's headings.  For each
+// heading step k the CTA needs, in shared memory:
+//   * its own (vP, vE) plane at heading k, rows y0-2 .. y0+R+1 (the y halo),
+//     for the centre, x and y neighbours, and the plane at heading k+2, from
+//     which each thread takes its chunk to extend the heading differences;
+//     own planes live in a ring of 8 slots;
+//   * the 8 neighbour planes (vE+-1, vE+-2, vP+-1, vP+-2) at heading k, rows
+//     y0 .. y0+R-1 (and, on RK2 stage 2, the step's old value V of the same
+//     rows), in a ring of 2 neighbour sets.
 // All of it arrives by bulk asynchronous copies (the TMA engine,
-// cp.async.bulk) issued by a producer warp that runs ahead across items, and
-// completes on mbarriers.  Every wait is bounded: a wait that gives up sets
-// the handle's timeout flag instead of hanging.
+// cp.async.bulk) issued by a producer warp that runs up to two heading steps
+// ahead, across items.  Every copy of step k (the own plane k+2, or planes
+// -2..2 on an item's first step, and the neighbour set) completes on that
+// step's "full" barrier, and consumers release the step on its "empty"
+// barrier: one wait and one arrival per step.  The ring of 8 own slots makes
+// this safe: a plane's slot is refilled two steps after the plane's last use
+// (items have at least 4 headings).  Every wait is bounded: a wait that gives
+// up sets the handle's timeout flag instead of hanging, and a waiting thread
+// is suspended by the barrier instead of spinning.
 //
 // Arithmetic.  The 4 cells of a chunk are processed as two float2 pairs with
 // sm_100 packed FP32 instructions (__ffma2_rn / __fadd2_rn / __fmul2_rn).
-// Second differences are kept unscaled (h^2 * D2) and the ENO2 slope is
+// Second differences are kept unscaled (h^2 * D2) and the ENO2 slopes are
 // (first difference +- 0.5 * selected second difference) / h -- the
-// reference's dm + 0.5*h*D2 rewritten.  Along x the edge differences and the
-// ENO selection between neighbouring cells of a chunk are shared.  Results
-// agree with the double-local reference to float rounding except where an
-// ENO selection is tied to rounding; relative5d_exact.cu is the bit-exact
-// path.
+// reference's dm + 0.5*h*D2 rewritten.  Along the heading axis the first
+// and second differences and the ENO selection of an edge are computed once
+// and carried to the next heading (the low-side slope of heading k+1 is
+// formed with the high-side selection of heading k).  Along x the
+// differences and selections are shared between the cells of a chunk, and
+// the end rules sit at compile-time positions (nx mod 4).  Each axis'
+// slopes enter the update only as their sum (the centred gradient times 2h)
+// and their jump (hi - lo, the Lax-Friedrichs term), so the 1/(2h) scalings
+// are folded into per-item and per-heading coefficients.  Results agree with
+// the double-local reference to float rounding except where an ENO selection
+// is tied to rounding; relative5d_exact.cu is the bit-exact path.
 #include <algorithm>
 #include <cstdio>
 
@@ -35,15 +50,19 @@ namespace {
 
 using namespace eno32;
 
-constexpr int OWN_SLOTS = 6;
-constexpr int NB_SLOTS = 2;
+constexpr int OWN_SLOTS = 8;   // own-plane ring (power of two)
+constexpr int STEP_SLOTS = 2;  // neighbour sets and step barriers
 constexpr int NEIGHBOURS = 8;  // vE-2, vE-1, vE+1, vE+2, vP-2, vP-1, vP+1, vP+2
 // a neighbour set also holds, on RK2 stage 2, the item's rows of the
 // stage's old value V (the blend partner), prefetched with the neighbours
 constexpr int NB_PLANES = NEIGHBOURS + 1;
 constexpr int MAX_THREADS = 512;
 constexpr int TARGET_THREADS = 256;  // launch bound: two CTAs of 256 per SM
-constexpr unsigned WAIT_LIMIT = 1u << 22;
+constexpr int MIN_ITEM_STEPS = 4;    // own-ring reuse needs items of >= 4 headings
+// A try suspends the thread for up to SUSPEND_NS; WAIT_LIMIT tries bound a
+// wait to about two seconds.
+constexpr unsigned WAIT_LIMIT = 1u << 21;
+constexpr unsigned SUSPEND_NS = 1000;
 
 // ---------------------------------------------------------------- PTX helpers
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
@@ -65,14 +84,16 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
       : "memory");
 }
 
+// One try: returns once the phase of `parity` has completed, or after the
+// suspend-time hint expires.
 __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
   uint32_t done;
   asm volatile(
       "{\n .reg .pred p;\n"
-      " mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n"
       " selp.u32 %0, 1, 0, p;\n}"
       : "=r"(done)
-      : "r"(smem_u32(bar)), "r"(parity)
+      : "r"(smem_u32(bar)), "r"(parity), "r"(SUSPEND_NS)
       : "memory");
   return done != 0;
 }
@@ -96,6 +117,13 @@ __device__ __forceinline__ void fence_barrier_init() {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile(
+      "{\n .reg .b64 state;\n"
+      " mbarrier.arrive.shared::cta.b64 state, [%0];\n}" ::"r"(smem_u32(bar))
+      : "memory");
+}
+
 // Bounded wait for one mbarrier phase.  Returns false (and flags the handle)
 // when the limit is reached.
 __device__ __forceinline__ bool wait_phase(uint64_t *bar, uint32_t parity,
@@ -115,13 +143,6 @@ struct FastArgs {
   float dt;
 };
 
-__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
-  asm volatile(
-      "{\n .reg .b64 state;\n"
-      " mbarrier.arrive.shared::cta.b64 state, [%0];\n}" ::"r"(smem_u32(bar))
-      : "memory");
-}
-
 // Shared memory layout of one CTA.
 struct SmemLayout {
   int own_floats, nb_floats;
@@ -136,8 +157,8 @@ __host__ __device__ inline SmemLayout smem_layout(int rows, int xp, int headings
   L.nb_floats = rows * xp;
   L.own_off = 0;
   L.nb_off = OWN_SLOTS * L.own_floats;
-  L.bar_off = 4 * (L.nb_off + NB_SLOTS * NB_PLANES * L.nb_floats);
-  L.red_off = L.bar_off + 8 * 2 * (OWN_SLOTS + NB_SLOTS);
+  L.bar_off = 4 * (L.nb_off + STEP_SLOTS * NB_PLANES * L.nb_floats);
+  L.red_off = L.bar_off + 8 * 2 * STEP_SLOTS;
   L.trig_off = L.red_off + 4 * (MAX_THREADS / 32);
   L.bytes = L.trig_off + 4 * 2 * headings;
   return L;
@@ -165,27 +186,58 @@ __device__ __forceinline__ Item decode_item(const FastArgs &a, int idx) {
   return it;
 }
 
+__device__ __forceinline__ float2 ld2(const float *p) {
+  return *reinterpret_cast<const float2 *>(p);
+}
+__device__ __forceinline__ float4 ld4(const float *p) {
+  return *reinterpret_cast<const float4 *>(p);
+}
+
+// Sum and jump (hi + lo, hi - lo) of the ENO slopes of two cells along a
+// non-walked axis from their five values.
+template <int ORDER, bool GENERAL>
+__device__ __forceinline__ void sum_jump(float2 m2, float2 m1, float2 v, float2 p1, float2 p2,
+                                         int pos, int n, float2 &S, float2 &J) {
+  float2 lo, hi;
+  slope_pair<ORDER, GENERAL>(m2, m1, v, p1, p2, pos, n, lo, hi);
+  S = add2(lo, hi);
+  J = sub2(hi, lo);
+}
+
+// The same for the 4 cells of a chunk (two pairs) along a vertical or speed
+// axis, from the chunks of the four neighbouring nodes.
+template <int ORDER, bool GENERAL>
+__device__ __forceinline__ void sum_jump4(float4 m2, float4 m1, float4 v, float4 p1, float4 p2,
+                                          int pos, int n, float2 S[2], float2 J[2]) {
+  sum_jump<ORDER, GENERAL>(lo2(m2), lo2(m1), lo2(v), lo2(p1), lo2(p2), pos, n, S[0], J[0]);
+  sum_jump<ORDER, GENERAL>(hi2(m2), hi2(m1), hi2(v), hi2(p1), hi2(p2), pos, n, S[1], J[1]);
+}
+
+__device__ __forceinline__ float2 abs2(float2 v) { return make_float2(fabsf(v.x), fabsf(v.y)); }
+
 // Persistent, warp-specialised stage kernel.  Each CTA walks the items
 // blockIdx.x, blockIdx.x + gridDim.x, ...  Warps 0..consumer_warps-1 compute
 // 4-cell chunks; the last warp is the producer: its lane 0 issues every bulk
-// copy in the order the consumers need them, across item boundaries, waiting
-// on a ring slot's "empty" barrier (one arrival per consumer warp) before
-// refilling it.  Consumers wait on the slots' "full" barriers.  Own planes of
-// an item are numbered d = -2 .. steps+1; plane d is read at step d-2 (the
-// heading window refill) and at step d (centre, y and x neighbours).
-template <int ORDER, int BLEND>
+// copy in the order the consumers need them, across item boundaries.  Own
+// planes of an item are numbered d = -2 .. steps+1 and take ring slots in
+// issue order: plane d of an item whose first plane was the og-th issued
+// sits in slot (og + d + 2) mod 8.  Plane d is read at step d (centre, x and
+// y neighbours) and at step d-2 (heading differences); planes -2..1 only
+// start the item's heading differences at step 0.
+//
+// XR = nx mod 4 places the x end rules (see slopes_x_fixed).
+template <int ORDER, int BLEND, int XR>
 __global__ void __launch_bounds__(TARGET_THREADS, 2)
     rel5_stage_kernel(const FastArgs a) {
   extern __shared__ __align__(128) float smem[];
   const Rel5Grid &g = a.g;
   const int R = a.rows, XP = g.xp;
   const SmemLayout L = smem_layout(R, XP, g.nh);
-  float *own = smem + L.own_off;  // [6][R+4][XP]
-  float *nbr = smem + L.nb_off;   // [2][8][R][XP]
+  float *own = smem + L.own_off;  // [8][R+4][XP]
+  float *nbr = smem + L.nb_off;   // [2][9][R][XP]
   char *raw = reinterpret_cast<char *>(smem);
-  uint64_t *bars = reinterpret_cast<uint64_t *>(raw + L.bar_off);
-  uint64_t *own_full = bars, *own_empty = bars + OWN_SLOTS;
-  uint64_t *nb_full = bars + 2 * OWN_SLOTS, *nb_empty = nb_full + NB_SLOTS;
+  uint64_t *full = reinterpret_cast<uint64_t *>(raw + L.bar_off);
+  uint64_t *empty = full + STEP_SLOTS;
   float *red = reinterpret_cast<float *>(raw + L.red_off);
   float *trig = reinterpret_cast<float *>(raw + L.trig_off);  // [nh][cos, sin]
 
@@ -198,13 +250,9 @@ __global__ void __launch_bounds__(TARGET_THREADS, 2)
   };
 
   if (tid == 0) {
-    for (int i = 0; i < OWN_SLOTS; i++) {
-      mbar_init(&own_full[i], 1);
-      mbar_init(&own_empty[i], a.consumer_warps);
-    }
-    for (int i = 0; i < NB_SLOTS; i++) {
-      mbar_init(&nb_full[i], 1);
-      mbar_init(&nb_empty[i], a.consumer_warps);
+    for (int i = 0; i < STEP_SLOTS; i++) {
+      mbar_init(&full[i], 1);
+      mbar_init(&empty[i], a.consumer_warps);
     }
     fence_barrier_init();
   }
@@ -220,7 +268,7 @@ __global__ void __launch_bounds__(TARGET_THREADS, 2)
 
   if (producer) {
     if (lane == 0) {
-      unsigned og = 0, ng = 0;  // own planes / neighbour sets issued so far
+      unsigned og = 0, gs = 0;  // own planes / steps issued so far
       for (int idx = blockIdx.x; idx < a.items && alive; idx += gridDim.x) {
         const Item it = decode_item(a, idx);
         const int row_lo = max(0, it.y0 - 2), row_hi = min(g.nx, it.y0 + it.r_eff + 2);
@@ -240,80 +288,84 @@ __global__ void __launch_bounds__(TARGET_THREADS, 2)
             nb_count += ok;
           }
         }
-        auto issue_own = [&](int d) {
-          const int slot = (int)(og % OWN_SLOTS);
-          const unsigned use = og / OWN_SLOTS;
-          if (use > 0) alive &= wait_phase(&own_empty[slot], (uint32_t)((use - 1) & 1), timeout);
-          if (!alive) return;
+        for (int k = 0; k < it.steps; k++) {
+          const int slot = (int)(gs & 1u);
+          // the slot's previous step (gs - 2) must be released first
+          if (gs >= STEP_SLOTS)
+            alive = wait_phase(&empty[slot], ((gs >> 1) - 1) & 1u, timeout);
+          if (!alive) break;
           fence_async_shared();
-          const int psi = ((it.p0 + d) % g.nh + g.nh) % g.nh;
-          mbar_expect_tx(&own_full[slot], own_bytes);
-          bulk_load(own + slot * L.own_floats + own_dst,
-                    own_src + plane_index(it.iv, it.ie, psi) * PP, own_bytes,
-                    &own_full[slot]);
-          og++;
-        };
-        auto issue_nb = [&](int k) {
-          const int slot = (int)(ng % NB_SLOTS);
-          const unsigned use = ng / NB_SLOTS;
-          if (use > 0) alive &= wait_phase(&nb_empty[slot], (uint32_t)((use - 1) & 1), timeout);
-          if (!alive) return;
-          fence_async_shared();
-          mbar_expect_tx(&nb_full[slot], nb_bytes * (nb_count + (BLEND ? 1 : 0)));
+          const int d_first = k == 0 ? -2 : k + 2;
+          const int n_own = k + 3 - d_first;
+          mbar_expect_tx(&full[slot], (uint32_t)n_own * own_bytes +
+                                          nb_bytes * (nb_count + (BLEND ? 1 : 0)));
+          for (int d = d_first; d <= k + 2; d++) {
+            const int psi = ((it.p0 + d) % g.nh + g.nh) % g.nh;
+            bulk_load(own + (og & (OWN_SLOTS - 1)) * L.own_floats + own_dst,
+                      own_src + plane_index(it.iv, it.ie, psi) * PP, own_bytes, &full[slot]);
+            og++;
+          }
+          float *set = nbr + slot * NB_PLANES * L.nb_floats;
           for (int q = 0; q < NEIGHBOURS; q++)
             if (nb_e[q] >= 0)
-              bulk_load(nbr + (slot * NB_PLANES + q) * L.nb_floats,
+              bulk_load(set + q * L.nb_floats,
                         a.s.src + plane_index(nb_v[q], nb_e[q], it.p0 + k) * PP +
                             (int64_t)it.y0 * XP,
-                        nb_bytes, &nb_full[slot]);
+                        nb_bytes, &full[slot]);
           // the blend partner V of this step's rows: read here before any
           // consumer writes them (they wait for this set first)
           if (BLEND)
-            bulk_load(nbr + (slot * NB_PLANES + NEIGHBOURS) * L.nb_floats,
+            bulk_load(set + NEIGHBOURS * L.nb_floats,
                       a.s.dst + plane_index(it.iv, it.ie, it.p0 + k) * PP +
                           (int64_t)it.y0 * XP,
-                      nb_bytes, &nb_full[slot]);
-          ng++;
-        };
-        for (int d = -2; d <= 1 && alive; d++) issue_own(d);
-        for (int k = 0; k < it.steps && alive; k++) {
-          issue_own(k + 2);
-          if (alive) issue_nb(k);
+                      nb_bytes, &full[slot]);
+          gs++;
         }
       }
-      // Every issued copy is consumed by the consumer warps, which wait for
-      // it; after a timeout wait (bounded) for the last one before exiting.
-      if (!alive && og > 0)
-        wait_phase(&own_full[(og - 1) % OWN_SLOTS], (uint32_t)(((og - 1) / OWN_SLOTS) & 1),
-                   timeout);
+      // After a timeout, let the copies already issued (the last two steps'
+      // sets at most) land before the CTA exits.
+      if (!alive)
+        for (unsigned q = gs > STEP_SLOTS ? gs - STEP_SLOTS : 0; q < gs; q++)
+          wait_phase(&full[q & 1u], (q >> 1) & 1u, timeout);
     }
   } else {
     const int r = tid / a.xc, c = tid % a.xc;
     const int x0 = 4 * c;
     const float ext = (float)g.extent, dxf = (float)g.dx;
     const float ap = (float)g.acc_p, ae = (float)g.acc_e;
+    // half reciprocal spacings: a centred gradient is (lo + hi) * h?s
+    const float hxs = 0.5f * a.ihx, hps = 0.5f * a.ihp, hvs = 0.5f * a.ihv, hes = 0.5f * a.ihe;
     float xs[4];
 #pragma unroll
     for (int i = 0; i < 4; i++) xs[i] = fmaf((float)(x0 + i), dxf, -ext);
-    const float2 negx_a = make_float2(-xs[0], -xs[1]), negx_b = make_float2(-xs[2], -xs[3]);
-    const float2 absx_a = make_float2(fabsf(xs[0]), fabsf(xs[1]));
-    const float2 absx_b = make_float2(fabsf(xs[2]), fabsf(xs[3]));
-    const float hx = 0.5f * a.ihx, hp = 0.5f * a.ihp, hv = 0.5f * a.ihv, he = 0.5f * a.ihe;
+    // -x * hxs per cell (the -x*gy term of y*gx - x*gy - gp), |x| per cell
+    const float2 nxs[2] = {make_float2(-xs[0] * hxs, -xs[1] * hxs),
+                           make_float2(-xs[2] * hxs, -xs[3] * hxs)};
+    const float2 absx[2] = {make_float2(fabsf(xs[0]), fabsf(xs[1])),
+                            make_float2(fabsf(xs[2]), fabsf(xs[3]))};
+    constexpr int IEND = (XR + 3) & 3;
+    constexpr int KEND = XR >= 2 ? XR : XR + 4;
+    const bool first = x0 == 0;
+    const bool kend_chunk = x0 == g.nx - KEND;
+    const bool iend_chunk = x0 == g.nx - 1 - IEND;
     const float dt = a.dt;
     const bool has_exit = a.s.exit_keep != nullptr;
     const float exit_r = (float)a.s.exit_r;
     const int ctr = (r + 2) * XP + x0;  // this chunk in an own slot
     const int nbo = r * XP + x0;        // this chunk in a neighbour slot
-    const bool tail = x0 + 4 > g.nx;                // chunk holds row padding
     float2 finite_acc = f2(0.f);
-    unsigned og = 0, ng = 0;
+    unsigned og = 0, gs = 0;
 
-    for (int idx = blockIdx.x; idx < a.items; idx += gridDim.x) {
+    for (int idx = blockIdx.x; idx < a.items && alive; idx += gridDim.x) {
       const Item it = decode_item(a, idx);
       const bool active = r < it.r_eff;
       const int iy = it.y0 + r;
-      const bool y_edge = iy < 2 || iy + 2 >= g.nx;
-      const int2 keep = has_exit ? a.s.exit_keep[iy] : make_int2(0, 0);
+      // warps holding a row within two of a y end take the general y rules
+      // (warp-uniform: the warp's first and last active rows)
+      const int rw0 = (32 * warp) / a.xc;
+      const int rw1 = min((32 * warp + 31) / a.xc, it.r_eff - 1);
+      const bool y_general = it.y0 + rw0 < 2 || it.y0 + rw1 + 2 >= g.nx;
+      const int2 keep = has_exit && active ? a.s.exit_keep[iy] : make_int2(0, 0);
       const float vp = (float)(g.vp_lo + it.iv * g.dvp);
       const float ve = (float)(g.ve_lo + it.ie * g.dve);
       const float wp = fabsf(vp) * (float)g.curv_p;
@@ -325,169 +377,184 @@ __global__ void __launch_bounds__(TARGET_THREADS, 2)
       const bool v_slope_inner = it.iv >= 2 && it.iv + 2 < g.nvp;
       const bool e_slope_inner = it.ie >= 2 && it.ie + 2 < g.nve;
       const float y = fmaf((float)iy, dxf, -ext);
-      const float ap_coef = (wp + we) * a.ihp, av_coef = ap * a.ihv, ae_coef = ae * a.ihe;
-      const float2 ay_a = __fmul2_rn(__fmul2_rn(f2(wp), absx_a), f2(a.ihx));
-      const float2 ay_b = __fmul2_rn(__fmul2_rn(f2(wp), absx_b), f2(a.ihx));
-      const float wy = wp * fabsf(y) * a.ihx;
-      const int64_t out0 =
-          plane_index(it.iv, it.ie, it.p0) * PP + (int64_t)iy * XP + x0;
+      const float ys = y * hxs;
+      // Coefficients of the update, per item.  The Hamiltonian is
+      //   bx*gx + by*gy - wp*|y*gx - x*gy - gp| + we*|gp| + speed terms
+      // with g = (lo + hi) * h?s, and the Lax-Friedrichs term
+      //   sum_axis alpha_axis * h?s * (hi - lo)
+      // with alpha = |bx| + wp|y|, |by| + wp|x|, wp + we, ap, ae.
+      const float wes = we * hps;                       // * |S_psi|
+      const float kv_in = -ap * hvs, ke_in = ae * hes;  // * |S_v|, |S_e| (inner)
+      const float dap = (wp + we) * hps, dav = ap * hvs, dae = ae * hes;
+      const float dax0 = wp * fabsf(y) * hxs;  // + |bx| * hxs per heading
+      const float2 day0[2] = {__fmul2_rn(f2(wp * hxs), absx[0]),
+                              __fmul2_rn(f2(wp * hxs), absx[1])};  // + |by| * hxs
+      const unsigned base = og;  // issue index of own plane d = -2
+      og += it.steps + 4;
+      const int64_t out0 = plane_index(it.iv, it.ie, it.p0) * PP + (int64_t)iy * XP + x0;
       float *gdst = a.s.dst + out0;
       float *garr = a.s.arrival + out0;
-      const unsigned base = og;  // global index of own plane d = -2
+      auto own_at = [&](unsigned q) -> const float * {
+        return own + (q & (OWN_SLOTS - 1)) * L.own_floats + ctr;
+      };
 
-      // Heading window: this chunk at headings k-2 .. k+2.
-      float4 win[5];
+      // Step 0's set holds planes -2..2: start the heading differences.
+      if (alive) alive = wait_phase(&full[gs & 1u], (gs >> 1) & 1u, timeout);
+      // carried along the headings, per pair of cells: VN = V(k+1),
+      // ER = V(k+1) - V(k), D2 = second difference at k (ORDER 2), LO = low
+      // slope of heading k
+      float2 VN[2], ER[2], D2[2], LO[2];
+      if (active) {  // lanes past the item's rows read nothing
+        const float4 vm2 = ld4(own_at(base)), vm1 = ld4(own_at(base + 1));
+        const float4 v0 = ld4(own_at(base + 2)), vp1 = ld4(own_at(base + 3));
 #pragma unroll
-      for (int d = 0; d < 5; d++) {
-        const unsigned q = base + d;
-        const int slot = (int)(q % OWN_SLOTS);
-        if (alive) alive &= wait_phase(&own_full[slot], (uint32_t)((q / OWN_SLOTS) & 1), timeout);
-        win[d] = *reinterpret_cast<const float4 *>(own + slot * L.own_floats + ctr);
+        for (int h = 0; h < 2; h++) {
+          const float2 a_m2 = h ? hi2(vm2) : lo2(vm2), a_m1 = h ? hi2(vm1) : lo2(vm1);
+          const float2 a_0 = h ? hi2(v0) : lo2(v0), a_p1 = h ? hi2(vp1) : lo2(vp1);
+          const float2 el = sub2(a_0, a_m1);
+          ER[h] = sub2(a_p1, a_0);
+          VN[h] = a_p1;
+          if (ORDER == 1) {
+            LO[h] = el;
+            D2[h] = f2(0.f);
+          } else {
+            const float2 dm = sub2(el, sub2(a_m1, a_m2));
+            D2[h] = sub2(ER[h], el);
+            LO[h] = __ffma2_rn(f2(0.5f), pick2(dm, D2[h]), el);
+          }
+        }
       }
 
-      // ring positions, advanced by one per step: the refill plane k+2 (slot
-      // and phase parity), the centre plane k, the neighbour set
-      int rslot = (int)((base + 5) % OWN_SLOTS);  // plane 3, read at k = 1
-      uint32_t rpar = (uint32_t)(((base + 5) / OWN_SLOTS) & 1);
-      int cslot = (int)((base + 2) % OWN_SLOTS);
-      int ns = (int)(ng % NB_SLOTS);
-      uint32_t npar = (uint32_t)((ng / NB_SLOTS) & 1);
+      // two steps per iteration let the carried heading state alternate
+      // registers; stage 2's larger body keeps one (no spills)
+#pragma unroll(BLEND ? 1 : 2)
       for (int k = 0; k < it.steps; k++) {
-        if (k > 0) {
-          if (alive) alive &= wait_phase(&own_full[rslot], rpar, timeout);
-#pragma unroll
-          for (int d = 0; d < 4; d++) win[d] = win[d + 1];
-          win[4] = *reinterpret_cast<const float4 *>(own + rslot * L.own_floats + ctr);
-        }
-        if (alive) alive &= wait_phase(&nb_full[ns], npar, timeout);
-
+        const unsigned slot = gs & 1u;
+        if (k > 0 && alive) alive = wait_phase(&full[slot], (gs >> 1) & 1u, timeout);
         if (active && alive) {
-          const float *o0 = own + cslot * L.own_floats + ctr;
-          const float *nb = nbr + ns * NB_PLANES * L.nb_floats + nbo;
-          const float4 C = win[2];
-          const float2 v_a = lo2(C), v_b = hi2(C);
+          const float *o0 = own_at(base + k + 2);  // centre plane k
+          const float *nb = nbr + slot * NB_PLANES * L.nb_floats + nbo;
+          const float4 C = ld4(o0);
+          const float4 VNEW = ld4(own_at(base + k + 4));  // plane k+2
 
-          // x: window x0-2 .. x0+5
-          const float2 xl = *reinterpret_cast<const float2 *>(o0 - 2);
-          const float2 xr = *reinterpret_cast<const float2 *>(o0 + 4);
-          const float w[8] = {xl.x, xl.y, C.x, C.y, C.z, C.w, xr.x, xr.y};
-          float xlo[4], xhi[4];
-          // every warp holds chunks at both x ends: the end rules as selects
-          // cost less than running both variants of a divergent branch
-          slopes_x<ORDER, true>(w, x0, g.nx, xlo, xhi);
-          const float2 lx_a = make_float2(xlo[0], xlo[1]), lx_b = make_float2(xlo[2], xlo[3]);
-          const float2 hx_a = make_float2(xhi[0], xhi[1]), hx_b = make_float2(xhi[2], xhi[3]);
+          // heading k: cos, sin
+          const float cs_k = trig[2 * (it.p0 + k)], sn_k = trig[2 * (it.p0 + k) + 1];
+          const float bx = fmaf(ve, cs_k, -vp), by = ve * sn_k;
+          const float cx = bx * hxs, cy = by * hxs;
+          const float dax = fmaf(fabsf(bx), hxs, dax0);
+          const float aby = fabsf(by) * hxs;
 
+          // Accumulators per pair: A = linear terms and dissipation, T =
+          // y*gx - x*gy - gp, Hs = the absolute-value and speed terms.
+          float2 A[2], T[2], Hs[2];
+
+          // x: window x0-2 .. x0+5 (end rules at compile-time positions)
+          {
+            const float2 xl = ld2(o0 - 2), xr = ld2(o0 + 4);
+            const float w[8] = {xl.x, xl.y, C.x, C.y, C.z, C.w, xr.x, xr.y};
+            float xlo[4], xhi[4];
+            slopes_x_fixed<ORDER, XR>(w, first, kend_chunk, iend_chunk, xlo, xhi);
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+              const float2 lo = make_float2(xlo[2 * h], xlo[2 * h + 1]);
+              const float2 hi = make_float2(xhi[2 * h], xhi[2 * h + 1]);
+              const float2 S = add2(lo, hi), J = sub2(hi, lo);
+              A[h] = __ffma2_rn(f2(dax), J, __fmul2_rn(f2(cx), S));
+              T[h] = __fmul2_rn(f2(ys), S);
+            }
+          }
           // y: rows iy-2 .. iy+2 of heading k
-          float2 ly_a, ly_b, hy_a, hy_b;
           {
-            const float4 m2 = *reinterpret_cast<const float4 *>(o0 - 2 * XP);
-            const float4 m1 = *reinterpret_cast<const float4 *>(o0 - XP);
-            const float4 p1 = *reinterpret_cast<const float4 *>(o0 + XP);
-            const float4 p2 = *reinterpret_cast<const float4 *>(o0 + 2 * XP);
-            if (y_edge) {
-              slope_pair<ORDER, true>(lo2(m2), lo2(m1), v_a, lo2(p1), lo2(p2), iy, g.nx, ly_a, hy_a);
-              slope_pair<ORDER, true>(hi2(m2), hi2(m1), v_b, hi2(p1), hi2(p2), iy, g.nx, ly_b, hy_b);
-            } else {
-              slope_pair<ORDER, false>(lo2(m2), lo2(m1), v_a, lo2(p1), lo2(p2), iy, g.nx, ly_a, hy_a);
-              slope_pair<ORDER, false>(hi2(m2), hi2(m1), v_b, hi2(p1), hi2(p2), iy, g.nx, ly_b, hy_b);
+            const float4 m2 = ld4(o0 - 2 * XP), m1 = ld4(o0 - XP);
+            const float4 p1 = ld4(o0 + XP), p2 = ld4(o0 + 2 * XP);
+            float2 S[2], J[2];
+            if (y_general)
+              sum_jump4<ORDER, true>(m2, m1, C, p1, p2, iy, g.nx, S, J);
+            else
+              sum_jump4<ORDER, false>(m2, m1, C, p1, p2, iy, g.nx, S, J);
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+              const float2 day = __fadd2_rn(day0[h], f2(aby));
+              A[h] = __ffma2_rn(f2(cy), S[h], A[h]);
+              A[h] = __ffma2_rn(day, J[h], A[h]);
+              T[h] = __ffma2_rn(nxs[h], S[h], T[h]);
             }
           }
-          // psi: periodic, from the register window
-          float2 lp_a, lp_b, hp_a, hp_b;
-          slope_pair<ORDER, false>(lo2(win[0]), lo2(win[1]), v_a, lo2(win[3]), lo2(win[4]), 2, 5, lp_a, hp_a);
-          slope_pair<ORDER, false>(hi2(win[0]), hi2(win[1]), v_b, hi2(win[3]), hi2(win[4]), 2, 5, lp_b, hp_b);
-          // vE and vP: neighbour slots
-          float2 le_a, le_b, he_a, he_b, lv_a, lv_b, hv_a, hv_b;
-          {
-            const float4 m2 = *reinterpret_cast<const float4 *>(nb + 0 * L.nb_floats);
-            const float4 m1 = *reinterpret_cast<const float4 *>(nb + 1 * L.nb_floats);
-            const float4 p1 = *reinterpret_cast<const float4 *>(nb + 2 * L.nb_floats);
-            const float4 p2 = *reinterpret_cast<const float4 *>(nb + 3 * L.nb_floats);
-            if (e_slope_inner) {
-              slope_pair<ORDER, false>(lo2(m2), lo2(m1), v_a, lo2(p1), lo2(p2), it.ie, g.nve, le_a, he_a);
-              slope_pair<ORDER, false>(hi2(m2), hi2(m1), v_b, hi2(p1), hi2(p2), it.ie, g.nve, le_b, he_b);
+          // psi: extend the carried differences with heading k+2
+#pragma unroll
+          for (int h = 0; h < 2; h++) {
+            const float2 vnew = h ? hi2(VNEW) : lo2(VNEW);
+            const float2 en = sub2(vnew, VN[h]);  // V(k+2) - V(k+1)
+            float2 hi, lo_next;
+            if (ORDER == 1) {
+              hi = ER[h];
+              lo_next = ER[h];
             } else {
-              slope_pair<ORDER, true>(lo2(m2), lo2(m1), v_a, lo2(p1), lo2(p2), it.ie, g.nve, le_a, he_a);
-              slope_pair<ORDER, true>(hi2(m2), hi2(m1), v_b, hi2(p1), hi2(p2), it.ie, g.nve, le_b, he_b);
+              const float2 d2n = sub2(en, ER[h]);
+              const float2 pr = pick2(D2[h], d2n);
+              hi = __ffma2_rn(f2(-0.5f), pr, ER[h]);
+              lo_next = __ffma2_rn(f2(0.5f), pr, ER[h]);
+              D2[h] = d2n;
+            }
+            const float2 S = add2(LO[h], hi), J = sub2(hi, LO[h]);
+            LO[h] = lo_next;
+            ER[h] = en;
+            VN[h] = vnew;
+            T[h] = __ffma2_rn(f2(-hps), S, T[h]);
+            A[h] = __ffma2_rn(f2(dap), J, A[h]);
+            Hs[h] = __fmul2_rn(f2(wes), abs2(S));
+          }
+          // vE and vP: neighbour planes
+          {
+            const float4 m2 = ld4(nb + 0 * L.nb_floats), m1 = ld4(nb + 1 * L.nb_floats);
+            const float4 p1 = ld4(nb + 2 * L.nb_floats), p2 = ld4(nb + 3 * L.nb_floats);
+            float2 S[2], J[2];
+            if (e_slope_inner)
+              sum_jump4<ORDER, false>(m2, m1, C, p1, p2, it.ie, g.nve, S, J);
+            else
+              sum_jump4<ORDER, true>(m2, m1, C, p1, p2, it.ie, g.nve, S, J);
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+              A[h] = __ffma2_rn(f2(dae), J[h], A[h]);
+              if (e_inner) {
+                Hs[h] = __ffma2_rn(f2(ke_in), abs2(S[h]), Hs[h]);
+              } else {  // max(elo*ge, ehi*ge), ge = S * hes
+                const float2 ge = __fmul2_rn(f2(hes), S[h]);
+                Hs[h] = __fadd2_rn(Hs[h], make_float2(fmaxf(elo * ge.x, ehi * ge.x),
+                                                      fmaxf(elo * ge.y, ehi * ge.y)));
+              }
             }
           }
           {
-            const float4 m2 = *reinterpret_cast<const float4 *>(nb + 4 * L.nb_floats);
-            const float4 m1 = *reinterpret_cast<const float4 *>(nb + 5 * L.nb_floats);
-            const float4 p1 = *reinterpret_cast<const float4 *>(nb + 6 * L.nb_floats);
-            const float4 p2 = *reinterpret_cast<const float4 *>(nb + 7 * L.nb_floats);
-            if (v_slope_inner) {
-              slope_pair<ORDER, false>(lo2(m2), lo2(m1), v_a, lo2(p1), lo2(p2), it.iv, g.nvp, lv_a, hv_a);
-              slope_pair<ORDER, false>(hi2(m2), hi2(m1), v_b, hi2(p1), hi2(p2), it.iv, g.nvp, lv_b, hv_b);
-            } else {
-              slope_pair<ORDER, true>(lo2(m2), lo2(m1), v_a, lo2(p1), lo2(p2), it.iv, g.nvp, lv_a, hv_a);
-              slope_pair<ORDER, true>(hi2(m2), hi2(m1), v_b, hi2(p1), hi2(p2), it.iv, g.nvp, lv_b, hv_b);
+            const float4 m2 = ld4(nb + 4 * L.nb_floats), m1 = ld4(nb + 5 * L.nb_floats);
+            const float4 p1 = ld4(nb + 6 * L.nb_floats), p2 = ld4(nb + 7 * L.nb_floats);
+            float2 S[2], J[2];
+            if (v_slope_inner)
+              sum_jump4<ORDER, false>(m2, m1, C, p1, p2, it.iv, g.nvp, S, J);
+            else
+              sum_jump4<ORDER, true>(m2, m1, C, p1, p2, it.iv, g.nvp, S, J);
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+              A[h] = __ffma2_rn(f2(dav), J[h], A[h]);
+              if (p_inner) {
+                Hs[h] = __ffma2_rn(f2(kv_in), abs2(S[h]), Hs[h]);
+              } else {  // min(plo*gv, phi*gv), gv = S * hvs
+                const float2 gv = __fmul2_rn(f2(hvs), S[h]);
+                Hs[h] = __fadd2_rn(Hs[h], make_float2(fminf(plo * gv.x, phi * gv.x),
+                                                      fminf(plo * gv.y, phi * gv.y)));
+              }
             }
           }
 
-          // Hamiltonian + dissipation (native_relative.cpp:144-157).
-          const int ip = it.p0 + k;
-          const float bx = fmaf(ve, trig[2 * ip], -vp);
-          const float by = ve * trig[2 * ip + 1];
-          const float2 bx2 = f2(bx), by2 = f2(by);
-          const float ax_coef = fmaf(fabsf(bx), a.ihx, wy);  // alpha_x / h
-          const float aby = fabsf(by) * a.ihx;
-          const float4 prev4 =
-              BLEND ? *reinterpret_cast<const float4 *>(nb + NEIGHBOURS * L.nb_floats) : C;
-
+          const float4 prev4 = BLEND ? ld4(nb + NEIGHBOURS * L.nb_floats) : C;
           float2 out[2];
 #pragma unroll
           for (int h = 0; h < 2; h++) {
-            const float2 lx = h ? lx_b : lx_a, hxv = h ? hx_b : hx_a;
-            const float2 ly = h ? ly_b : ly_a, hy = h ? hy_b : hy_a;
-            const float2 lp = h ? lp_b : lp_a, hpv = h ? hp_b : hp_a;
-            const float2 lv = h ? lv_b : lv_a, hvv = h ? hv_b : hv_a;
-            const float2 le = h ? le_b : le_a, hev = h ? he_b : he_a;
-            const float2 v = h ? v_b : v_a;
-            const float2 negx = h ? negx_b : negx_a;
-            const float2 ay = __fadd2_rn(h ? ay_b : ay_a, f2(aby));
-            // centred gradients g = (lo + hi) / (2h); jumps hi - lo (unscaled)
-            const float2 gx = __fmul2_rn(__fadd2_rn(lx, hxv), f2(hx));
-            const float2 gy = __fmul2_rn(__fadd2_rn(ly, hy), f2(hx));
-            const float2 gpn = __fmul2_rn(__fadd2_rn(lp, hpv), f2(-hp));  // -gp
-            const float2 gv = __fmul2_rn(__fadd2_rn(lv, hvv), f2(hv));
-            const float2 ge = __fmul2_rn(__fadd2_rn(le, hev), f2(he));
-            float2 H = __ffma2_rn(by2, gy, __fmul2_rn(bx2, gx));
-            float2 t = __ffma2_rn(f2(y), gx, gpn);  // y*gx - gp
-            t = __ffma2_rn(negx, gy, t);             // - x*gy
-            float hs[2] = {H.x, H.y};
-            const float ts[2] = {t.x, t.y}, gps[2] = {gpn.x, gpn.y};
-            const float gvs[2] = {gv.x, gv.y}, ges[2] = {ge.x, ge.y};
-#pragma unroll
-            for (int l = 0; l < 2; l++) {
-              hs[l] = fmaf(-wp, fabsf(ts[l]), hs[l]);
-              hs[l] = fmaf(we, fabsf(gps[l]), hs[l]);
-            }
-            if (p_inner) {
-#pragma unroll
-              for (int l = 0; l < 2; l++) hs[l] = fmaf(-ap, fabsf(gvs[l]), hs[l]);
-            } else {
-#pragma unroll
-              for (int l = 0; l < 2; l++) hs[l] += fminf(plo * gvs[l], phi * gvs[l]);
-            }
-            if (e_inner) {
-#pragma unroll
-              for (int l = 0; l < 2; l++) hs[l] = fmaf(ae, fabsf(ges[l]), hs[l]);
-            } else {
-#pragma unroll
-              for (int l = 0; l < 2; l++) hs[l] += fmaxf(elo * ges[l], ehi * ges[l]);
-            }
-            H = make_float2(hs[0], hs[1]);
-            // dissipation: sum alpha_k/h_k * (hi - lo)_k
-            float2 diss = __fmul2_rn(f2(ax_coef), sub2(hxv, lx));
-            diss = __ffma2_rn(ay, sub2(hy, ly), diss);
-            diss = __ffma2_rn(f2(ap_coef), sub2(hpv, lp), diss);
-            diss = __ffma2_rn(f2(av_coef), sub2(hvv, lv), diss);
-            diss = __ffma2_rn(f2(ae_coef), sub2(hev, le), diss);
-            H = __ffma2_rn(f2(0.5f), diss, H);
+            const float2 v = h ? hi2(C) : lo2(C);
+            // H = A + Hs - wp * |T|
+            const float2 Hsum = __ffma2_rn(f2(-wp), abs2(T[h]), __fadd2_rn(A[h], Hs[h]));
             float2 value =
-                __ffma2_rn(f2(dt), make_float2(fminf(H.x, 0.f), fminf(H.y, 0.f)), v);
+                __ffma2_rn(f2(dt), make_float2(fminf(Hsum.x, 0.f), fminf(Hsum.y, 0.f)), v);
             const float2 prev = BLEND ? (h ? hi2(prev4) : lo2(prev4)) : v;
             if (BLEND) value = __fmul2_rn(f2(0.5f), __fadd2_rn(prev, value));
             if (has_exit) {  // cells beyond the local exit hold the exit value
@@ -495,27 +562,34 @@ __global__ void __launch_bounds__(TARGET_THREADS, 2)
               if (ix < keep.x || ix > keep.y) value.x = exit_r;
               if (ix + 1 < keep.x || ix + 1 > keep.y) value.y = exit_r;
             }
-            if (tail && x0 + 2 * h + 1 >= g.nx) {  // row padding stays 0
-              if (x0 + 2 * h >= g.nx) value.x = 0.f;
-              value.y = 0.f;
-            }
-            finite_acc = __ffma2_rn(value, f2(0.f), finite_acc);
             out[h] = value;
+          }
+          if (iend_chunk) {  // row padding past x = nx-1 stays 0
+            if (IEND < 1) out[0].y = 0.f;
+            if (IEND < 2) out[1].x = 0.f;
+            if (IEND < 3) out[1].y = 0.f;
+          }
+#pragma unroll
+          for (int h = 0; h < 2; h++) {
+            const float2 value = out[h];
+            finite_acc = __ffma2_rn(value, f2(0.f), finite_acc);
             if (BLEND || ORDER == 1) {
+              const float2 prev = BLEND ? (h ? hi2(prev4) : lo2(prev4)) : (h ? hi2(C) : lo2(C));
               const float2 change = sub2(value, prev);
               residual = fmaxf(residual, fmaxf(fabsf(change.x), fabsf(change.y)));
               // First crossing of zero (native_relative.cpp:167-168).  The
               // update never increases a cell, so a crossing has
-              // prev * value <= 0 with prev > 0.
+              // prev * value <= 0 with prev > 0; padding holds 0 and never
+              // crosses.
               const float2 sgn = __fmul2_rn(prev, value);
               if (sgn.x <= 0.f || sgn.y <= 0.f) {
                 const float pv[2] = {prev.x, prev.y}, nv[2] = {value.x, value.y};
 #pragma unroll
                 for (int l = 0; l < 2; l++) {
-                  float *slot = garr + 2 * h + l;
-                  if (pv[l] > 0.f && nv[l] <= 0.f && x0 + 2 * h + l < g.nx && isnan(*slot))
-                    *slot = (float)(a.s.t + a.s.dt * (double)pv[l] /
-                                                ((double)pv[l] - (double)nv[l]));
+                  float *slot_p = garr + 2 * h + l;
+                  if (pv[l] > 0.f && nv[l] <= 0.f && isnan(*slot_p))
+                    *slot_p = (float)(a.s.t + a.s.dt * (double)pv[l] /
+                                                  ((double)pv[l] - (double)nv[l]));
                 }
               }
             }
@@ -523,35 +597,13 @@ __global__ void __launch_bounds__(TARGET_THREADS, 2)
           *reinterpret_cast<float4 *>(gdst) =
               make_float4(out[0].x, out[0].y, out[1].x, out[1].y);
         }
-        // Release plane k (and the window-only planes at the item's ends) and
-        // this step's neighbour set.
+        // Release this step's set (and the own planes it finished).
         __syncwarp();
-        if (lane == 0) {
-          if (k == 0) {
-            mbar_arrive(&own_empty[(int)(base % OWN_SLOTS)]);
-            mbar_arrive(&own_empty[(int)((base + 1) % OWN_SLOTS)]);
-          }
-          mbar_arrive(&own_empty[cslot]);
-          if (k == it.steps - 1) {
-            mbar_arrive(&own_empty[(int)((base + it.steps + 2) % OWN_SLOTS)]);
-            mbar_arrive(&own_empty[(int)((base + it.steps + 3) % OWN_SLOTS)]);
-          }
-          mbar_arrive(&nb_empty[ns]);
-        }
-        ng++;
+        if (lane == 0) mbar_arrive(&empty[slot]);
+        gs++;
         gdst += PP;
         garr += PP;
-        if (k > 0 && ++rslot == OWN_SLOTS) {
-          rslot = 0;
-          rpar ^= 1u;
-        }
-        if (++cslot == OWN_SLOTS) cslot = 0;
-        if (++ns == NB_SLOTS) {
-          ns = 0;
-          npar ^= 1u;
-        }
       }
-      og = base + it.steps + 4;
     }
     bad = !(isfinite(finite_acc.x) && isfinite(finite_acc.y));
   }
@@ -575,20 +627,19 @@ __global__ void __launch_bounds__(TARGET_THREADS, 2)
 
 int g_last_resident = 0;
 
-template <int ORDER, int BLEND>
-cudaError_t launch(const FastArgs &args, size_t smem, int threads,
-                   cudaStream_t stream) {
+template <int ORDER, int BLEND, int XR>
+cudaError_t launch_xr(const FastArgs &args, size_t smem, int threads, cudaStream_t stream) {
   // Resident CTAs per SM for this (shared memory, block size); recomputed
   // when either changes.
   static int configured_smem = 0, configured_threads = 0;
   static int resident = 0;
   if (configured_smem != (int)smem || configured_threads != threads || resident == 0) {
-    cudaError_t e = cudaFuncSetAttribute(rel5_stage_kernel<ORDER, BLEND>,
+    cudaError_t e = cudaFuncSetAttribute(rel5_stage_kernel<ORDER, BLEND, XR>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &resident, rel5_stage_kernel<ORDER, BLEND>, threads, smem);
+        &resident, rel5_stage_kernel<ORDER, BLEND, XR>, threads, smem);
     if (e != cudaSuccess) return e;
     if (resident < 1) return cudaErrorInvalidConfiguration;
     configured_smem = (int)smem;
@@ -599,8 +650,18 @@ cudaError_t launch(const FastArgs &args, size_t smem, int threads,
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   const int blocks = std::min(args.items, sms * resident);
   g_last_resident = resident;
-  rel5_stage_kernel<ORDER, BLEND><<<blocks, threads, smem, stream>>>(args);
+  rel5_stage_kernel<ORDER, BLEND, XR><<<blocks, threads, smem, stream>>>(args);
   return cudaGetLastError();
+}
+
+template <int ORDER, int BLEND>
+cudaError_t launch(const FastArgs &args, size_t smem, int threads, cudaStream_t stream) {
+  switch (args.g.nx & 3) {
+    case 0: return launch_xr<ORDER, BLEND, 0>(args, smem, threads, stream);
+    case 1: return launch_xr<ORDER, BLEND, 1>(args, smem, threads, stream);
+    case 2: return launch_xr<ORDER, BLEND, 2>(args, smem, threads, stream);
+    default: return launch_xr<ORDER, BLEND, 3>(args, smem, threads, stream);
+  }
 }
 
 __global__ void rel5_init_kernel(const float *__restrict__ plane, int64_t plane_size,
@@ -682,14 +743,19 @@ Rel5Tile rel5_default_tile(const Rel5Grid &g) {
       t.rows = rows;
     }
   }
-  // Heading chunks of 24 measured fastest on the 65x48x21x21 grid (B200).
-  t.psi_chunk = g.nh < 24 ? g.nh : 24;
+  // Heading chunks of about 24 (fastest on the 65x48x21x21 grid, B200),
+  // balanced so that the last chunk is not short.
+  const int chunks = (g.nh + 23) / 24;
+  t.psi_chunk = (g.nh + chunks - 1) / chunks;
   return t;
 }
 
 bool rel5_tile_valid(const Rel5Grid &g, const Rel5Tile &t) {
   if (t.rows < 1 || t.rows > g.nx || t.psi_chunk < 1 || t.psi_chunk > g.nh)
     return false;
+  // every item (the last heading chunk too) needs MIN_ITEM_STEPS headings
+  const int tail = g.nh % t.psi_chunk;
+  if (t.psi_chunk < MIN_ITEM_STEPS || (tail != 0 && tail < MIN_ITEM_STEPS)) return false;
   const int consumer_warps = (t.rows * (g.xp / 4) + 31) / 32;
   if (32 * (consumer_warps + 1) > TARGET_THREADS) return false;
   return rel5_fast_smem_bytes(g, t) <= 227 * 1024;

@@ -37,6 +37,9 @@ struct SLStats {
   unsigned long long residual;  // bits of a non-negative double
   unsigned int nonfinite;
   unsigned int pad;
+  // interpolated action-pair evaluations of the tiled kernel's live cells
+  // (probes, full reply scans and pruned replies) since the last reset
+  unsigned long long evaluations;
 };
 
 struct SLBackup {

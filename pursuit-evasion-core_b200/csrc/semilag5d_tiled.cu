@@ -150,9 +150,10 @@ __device__ __forceinline__ float extended(const float *raw_plane, int gx, int gy
 //      once its reply maximum reaches `best`.
 __device__ __forceinline__ void minmax_cell(const float2 *ring, const SLPair *pairs, float2 P,
                                             float2 Q, int hu, int he, bool live, float &best,
-                                            int &bu, int &be) {
+                                            int &bu, int &be, unsigned &evals) {
   bu = hu;
   be = he;
+  evals += live ? 9u : 0u;
   float probe[9];
 #pragma unroll
   for (int u = 0; u < 9; u++) probe[u] = pair_value(ring, pairs[u * 9 + he], P, Q);
@@ -172,6 +173,7 @@ __device__ __forceinline__ void minmax_cell(const float2 *ring, const SLPair *pa
   const int first = (cand >> hu) & 1u ? hu : arg;
   // C1
   if (__any_sync(0xffffffffu, cand != 0)) {
+    evals += cand ? 8u : 0u;
     float w = probe[0];
 #pragma unroll
     for (int u = 1; u < 9; u++) w = first == u ? probe[u] : w;
@@ -203,6 +205,7 @@ __device__ __forceinline__ void minmax_cell(const float2 *ring, const SLPair *pa
     if (!cand) continue;
     const int ue = uj == 0 ? he : uj - (uj <= he);
     const float v = pair_value(ring, pairs[up * 9 + ue], P, Q);
+    evals++;
     if (v > worst) {
       worst = v;
       wue = ue;
@@ -240,6 +243,7 @@ __global__ void __launch_bounds__(SL_TILED_MAX_THREADS, 1)
   const int lane = tid & 31, warp = tid >> 5, nwarps = nthreads >> 5;
   float change = 0.f;
   bool bad = false;
+  unsigned long long evals_total = 0;
 
   for (int64_t item = blockIdx.x; item < plan.items; item += gridDim.x) {
     int64_t rest = item;
@@ -409,9 +413,11 @@ __global__ void __launch_bounds__(SL_TILED_MAX_THREADS, 1)
         const float X = (float)col - center, Y = (float)iy - center;
         float best = MODE == SL_TUBE ? cur : INFINITY;
         int bu, be;
+        unsigned evals = 0;
         minmax_cell(ring, pairs, make_float2(X, Y), make_float2(Y, -X),
                     (h >> 4) < 9 ? (h >> 4) : 4, (h & 15) < 9 ? (h & 15) : 4,
-                    valid && !captured, best, bu, be);
+                    valid && !captured, best, bu, be, evals);
+        evals_total += evals;
         if (valid) {
           float out;
           if (MODE == SL_TUBE) {
@@ -444,8 +450,11 @@ __global__ void __launch_bounds__(SL_TILED_MAX_THREADS, 1)
   }
 
   if (__syncthreads_or(bad) && tid == 0) atomicOr(&b.stats->nonfinite, 1u);
-  for (int off = 16; off > 0; off >>= 1)
+  for (int off = 16; off > 0; off >>= 1) {
     change = fmaxf(change, __shfl_xor_sync(0xffffffffu, change, off));
+    evals_total += __shfl_xor_sync(0xffffffffu, evals_total, off);
+  }
+  if ((tid & 31) == 0 && evals_total) atomicAdd(&b.stats->evaluations, evals_total);
   __shared__ float warp_max[SL_TILED_MAX_THREADS / 32];
   if ((tid & 31) == 0) warp_max[tid >> 5] = change;
   __syncthreads();

@@ -192,6 +192,18 @@ SIGNATURES = {
     "pe_relative_step_noalloc": (ctypes.c_int, [ctypes.POINTER(RelativeParams), _P, _P,
                                                 _P, ctypes.c_double, ctypes.c_double,
                                                 _P, _DP]),
+    "pe_relative_f64_create": (
+        ctypes.c_int,
+        [ctypes.POINTER(RelativeParams), ctypes.POINTER(ctypes.c_void_p)],
+    ),
+    "pe_relative_f64_destroy": (ctypes.c_int, [_P]),
+    "pe_relative_f64_set_stream": (ctypes.c_int, [_P, _P]),
+    "pe_relative_f64_initialize": (ctypes.c_int, [_P]),
+    "pe_relative_f64_step": (ctypes.c_int, [_P, ctypes.c_double]),
+    "pe_relative_f64_advance": (ctypes.c_int, [_P, ctypes.c_double, _I64P]),
+    "pe_relative_f64_time": (ctypes.c_int, [_P, _DP, _I64P, _DP]),
+    "pe_relative_f64_stats": (ctypes.c_int, [_P, _DP]),
+    "pe_relative_f64_copy_field": (ctypes.c_int, [_P, _P]),
     "pe_batch_create": (ctypes.c_int, [ctypes.POINTER(RelativeParams), _DP, ctypes.c_int32,
                                        ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p)]),
     "pe_batch_set_tile": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32]),
@@ -282,6 +294,7 @@ SIGNATURES = {
                                           ctypes.c_int32, _I64P, _DP,
                                           ctypes.POINTER(ctypes.c_int32)]),
     "pe_semilag_residual": (ctypes.c_int, [_P, _DP]),
+    "pe_semilag_evaluations": (ctypes.c_int, [_P, _I64P]),
     "pe_semilag_copy_value": (ctypes.c_int, [_P, _P]),
     "pe_semilag_copy_value_device": (ctypes.c_int, [_P, _P]),
     "pe_semilag_copy_policy": (ctypes.c_int, [_P, _P, _P]),

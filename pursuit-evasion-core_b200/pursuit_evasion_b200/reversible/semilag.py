@@ -132,6 +132,13 @@ class SemiLagrangianSolver:
         _native.check(self._lib.pe_semilag_residual(self._h, ctypes.byref(r)))
         return r.value
 
+    def evaluations(self):
+        """Action-pair evaluations of the tiled value backups since the last
+        initialisation (0 for the generic kernel)."""
+        n = ctypes.c_int64()
+        _native.check(self._lib.pe_semilag_evaluations(self._h, ctypes.byref(n)))
+        return n.value
+
     def value(self, out=None):
         out = np.empty(self.cells, np.float32) if out is None else out
         _native.check(self._lib.pe_semilag_copy_value(self._h, out.ctypes.data))

@@ -209,3 +209,97 @@ def test_history_written_while_solving_equals_synchronous_frames(tmp_path):
             s.advance(float(goal))
             expected.append(s.field().ravel().copy())
     np.testing.assert_array_equal(written.view(np.uint32), np.array(expected).view(np.uint32))
+
+
+@pytest.mark.parametrize("positions", [10, 11, 12, 13])
+def test_fast_path_x_end_rules_for_every_row_length(oracle, positions):
+    """The float32 stage places its x end rules by nx mod 4 (one compiled
+    variant per residue): each residue tracks the double-local oracle."""
+    grid = RelativeGrid(positions, 8, 5, 4, 3.0)
+    cfg = oracle.rel_cfg(A3, grid)
+    ref_frames, _, ref_steps = oracle.rel_solve_f32(cfg, 0.2, 0.1)
+    frames, _, steps = gpu_frames(A3, grid, 0.2, 0.1, 2, "float32")
+    assert steps == ref_steps
+    assert_fast_close(frames, ref_frames)
+
+
+def test_fast_path_does_not_depend_on_the_tile():
+    """Each cell's float32 update is the same arithmetic whatever the work
+    item (rows per item, headings per item): results are bit-identical over
+    tiles, including one-row items and four-heading items, and tiles whose
+    last heading chunk is shorter than four headings are refused."""
+    grid = RelativeGrid(17, 12, 7, 7, 4.0)
+    results = []
+    for tile in (None, (1, 4), (5, 6), (17, 12), (3, 8)):
+        with RelativeSolver(A3, grid, local_precision="float32") as s:
+            if tile is not None:
+                s.set_tile(*tile)
+                assert s.tile()[:2] == tile
+            s.initialize()
+            s.advance(0.15)
+            results.append((s.field().copy(), s.arrival().copy()))
+    for field, arrival in results[1:]:
+        np.testing.assert_array_equal(bits(field), bits(results[0][0]))
+        np.testing.assert_array_equal(bits(arrival), bits(results[0][1]))
+    with RelativeSolver(A3, grid, local_precision="float32") as s:
+        with pytest.raises(ValueError):
+            s.set_tile(4, 5)  # 12 headings = 5 + 5 + 2: a 2-heading item
+
+
+@pytest.mark.parametrize("name", sorted(GOLDEN)[:2] + ["readme-o1", "readme-o2"])
+def test_fp64_storage_solve_equals_fp64_oracle_bitwise(oracle, name):
+    """The FP64-storage solve (the exact stage with double values, which
+    measures float32 tables at full size) equals the CPU FP64 oracle
+    po_rel_stage_f64 bit for bit, frame driver included."""
+    from pursuit_evasion_b200.reversible.fp64_table import RelativeSolverF64
+
+    if name.startswith("readme"):
+        config, grid, horizon, output_dt = A3, CONFIG1_GRID, 0.2, 0.1
+        order = int(name[-1])
+    else:
+        case = GOLDEN[name]
+        config, grid = case["config"], case["grid"]
+        horizon, output_dt, order = case["horizon"], case["output_dt"], case["order"]
+    final, steps = oracle.rel_solve_f64(oracle.rel_cfg(config, grid, order=order), horizon,
+                                        output_dt)
+    times = np.minimum(np.arange(1, int(np.ceil(horizon / output_dt - 1e-10)) + 1)
+                       * output_dt, horizon)
+    with RelativeSolverF64(config, grid, order=order) as s:
+        s.initialize()
+        for goal in times:
+            s.advance(goal)
+        got = s.field().ravel()
+        assert s.steps == steps
+        assert s.residual() > 0
+    np.testing.assert_array_equal(got.view(np.uint64), final.view(np.uint64))
+
+
+def test_fp64_table_error_of_float32_tables_on_the_subsampled_tile(oracle):
+    """On a 33x24x9x9 grid over 0.5 s: the FP64-storage solve equals the
+    CPU FP64 oracle bit for bit, the reference-arithmetic float32 table's
+    error against it (every 2nd x, y, psi; all speeds) equals the oracle's
+    own float32-vs-FP64 error, and the float32-local table stays within
+    twice that error (max 4.7e-4, mean 1.3e-6 for the reference
+    arithmetic)."""
+    from pursuit_evasion_b200.reversible.fp64_table import RelativeSolverF64, subsampled_error
+
+    grid = RelativeGrid(33, 24, 9, 9, 6.0)
+    cfg = oracle.rel_cfg(A3, grid)
+    frames, _, _ = oracle.rel_solve_f32(cfg, 0.5, 0.5)
+    final64, _ = oracle.rel_solve_f64(cfg, 0.5, 0.5)
+    with RelativeSolverF64(A3, grid) as r:
+        r.initialize()
+        r.advance(0.5)
+        ref = r.field()
+    np.testing.assert_array_equal(ref.ravel().view(np.uint64), final64.view(np.uint64))
+    expected = subsampled_error(frames[-1].reshape(grid.shape), ref, step=2)
+    errors = {}
+    for precision in ("float64", "float32"):
+        with RelativeSolver(A3, grid, local_precision=precision) as s:
+            s.initialize()
+            s.advance(0.5)
+            errors[precision] = subsampled_error(s.field(), ref, step=2)
+    assert errors["float64"] == expected
+    assert expected["nodes"] == 9 * 9 * 12 * 17 * 17
+    assert errors["float32"]["max_abs"] <= 2 * expected["max_abs"]
+    assert errors["float32"]["mean_abs"] <= 2 * expected["mean_abs"]
