@@ -216,6 +216,44 @@ int pe_relative_step_noalloc(const pe_relative_params *params,
                              void *cuda_stream, double *residual);
 
 /* ------------------------------------------------------------------------
+ * Vehicle geometry of the compact contact game (grid construction).
+ * Replaces the reference's OpenMP geometry library (local_game/
+ * native_geometry.cpp:8-117 batch_clearance / batch_backups /
+ * batch_actions, :221-246 configuration_connections, bound by
+ * local_game/native.py:110-230 GeometryEngine).  A model is one car's
+ * limits, rectangle and control period (the reference's parameter vector
+ * [speed_min, speed_max, acceleration, max_curvature, length, width,
+ * control_dt]); obstacles are circles [x, y, r] in a square arena of half
+ * width `half_width`; states are [x, y, heading, signed speed].  Host
+ * buffers in and out; the queries run one GPU thread each in double
+ * precision.
+ * ------------------------------------------------------------------------ */
+typedef struct pe_vehicle_model {
+  double speed_min, speed_max, acceleration, max_curvature;
+  double length, width, control_dt;
+} pe_vehicle_model;
+
+/* Signed rectangle clearance to the walls and circles of each state. */
+int pe_geometry_clearance(const pe_vehicle_model *model, const double *states, int64_t n,
+                          const double *circles, int32_t n_circles, double half_width,
+                          double *out, int32_t device);
+/* 1 where the state is clear and one full-braking arc to rest is clear. */
+int pe_geometry_backup_safe(const pe_vehicle_model *model, const double *states, int64_t n,
+                            const double *circles, int32_t n_circles, double half_width,
+                            uint8_t *out, int32_t device);
+/* For every state and control [a, k]: next[n][na][4] the held-control arc
+ * over dt, ok[n][na] = the arc is clear and its end is backup safe. */
+int pe_geometry_actions(const pe_vehicle_model *model, const double *states, int64_t n,
+                        const double *controls, int32_t n_controls, double dt,
+                        const double *circles, int32_t n_circles, double half_width,
+                        uint8_t *ok, double *next, int32_t device);
+/* 1 where the straight configuration path from[i] -> to[i] is clear. */
+int pe_geometry_connections(const pe_vehicle_model *model, const double *from,
+                            const double *to, int64_t n, const double *circles,
+                            int32_t n_circles, double half_width, uint8_t *out,
+                            int32_t device);
+
+/* ------------------------------------------------------------------------
  * FP64-storage relative 5D solve: the exact ENO/LF stage of
  * native_relative.cpp:38-172 with double values instead of float32 (the
  * reference stores float32 only; its CPU restatement with double storage is

@@ -120,7 +120,7 @@ def time_relative(precision, steps=10):
     dev = torch.device("cuda", 0)
     x = torch.linspace(-g["extent"], g["extent"], n, dtype=torch.float64)
     plane = (torch.hypot(x[None, :], x[:, None]) - A3["radius"]).float()
-    a = plane.to(dev).repeat(N // (n * n))
+    a = plane.reshape(-1).to(dev).repeat(N // (n * n))
     b = torch.empty_like(a)
     arrival = torch.full_like(a, float("nan"))
     angles = [-math.pi + i * 2 * math.pi / h for i in range(h)]

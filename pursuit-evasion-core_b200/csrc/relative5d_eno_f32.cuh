@@ -143,16 +143,19 @@ __device__ __forceinline__ void slopes_x_fixed(const float w[8], bool first, boo
     float m[7];
 #pragma unroll
     for (int k = 2; k < 7; k++) m[k] = eno_pick(d2[k - 1], d2[k]);
-    if (first) m[3] = d2[3];
-    if (kend_chunk) m[KEND + 1] = d2[KEND];
+    // selects, not branches: the flagged chunks sit in every warp
+    m[3] = first ? d2[3] : m[3];
+    m[KEND + 1] = kend_chunk ? d2[KEND] : m[KEND + 1];
 #pragma unroll
     for (int i = 0; i < 4; i++) {
       lo[i] = fmaf(0.5f, m[i + 2], e[i + 1]);
       hi[i] = fmaf(-0.5f, m[i + 3], e[i + 2]);
     }
   }
-  if (first) lo[0] = hi[0] = e[2];
-  if (iend_chunk) lo[IEND] = hi[IEND] = e[IEND + 1];
+  lo[0] = first ? e[2] : lo[0];
+  hi[0] = first ? e[2] : hi[0];
+  lo[IEND] = iend_chunk ? e[IEND + 1] : lo[IEND];
+  hi[IEND] = iend_chunk ? e[IEND + 1] : hi[IEND];
 }
 
 }  // namespace eno32

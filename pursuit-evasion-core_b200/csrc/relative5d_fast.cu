@@ -17,8 +17,8 @@
 // cp.async.bulk) issued by a producer warp that runs up to two heading steps
 // ahead, across items.  Every copy of step k (the own plane k+2, or planes
 // -2..2 on an item's first step, and the neighbour set) completes on that
-// step's "full" barrier, and consumers release the step on its "empty"
-// barrier: one wait and one arrival per step.  The ring of 8 own slots makes
+// step's "full" barrier, and every consumer thread releases the step on its
+// "empty" barrier: one wait and one arrival per step.  The ring of 8 own slots makes
 // this safe: a plane's slot is refilled two steps after the plane's last use
 // (items have at least 4 headings).  Every wait is bounded: a wait that gives
 // up sets the handle's timeout flag instead of hanging, and a waiting thread
@@ -213,7 +213,6 @@ __device__ __forceinline__ void sum_jump4(float4 m2, float4 m1, float4 v, float4
   sum_jump<ORDER, GENERAL>(hi2(m2), hi2(m1), hi2(v), hi2(p1), hi2(p2), pos, n, S[1], J[1]);
 }
 
-__device__ __forceinline__ float2 abs2(float2 v) { return make_float2(fabsf(v.x), fabsf(v.y)); }
 
 // Persistent, warp-specialised stage kernel.  Each CTA walks the items
 // blockIdx.x, blockIdx.x + gridDim.x, ...  Warps 0..consumer_warps-1 compute
@@ -252,7 +251,7 @@ __global__ void __launch_bounds__(TARGET_THREADS, 2)
   if (tid == 0) {
     for (int i = 0; i < STEP_SLOTS; i++) {
       mbar_init(&full[i], 1);
-      mbar_init(&empty[i], a.consumer_warps);
+      mbar_init(&empty[i], 32 * a.consumer_warps);
     }
     fence_barrier_init();
   }
@@ -444,9 +443,12 @@ __global__ void __launch_bounds__(TARGET_THREADS, 2)
           const float dax = fmaf(fabsf(bx), hxs, dax0);
           const float aby = fabsf(by) * hxs;
 
-          // Accumulators per pair: A = linear terms and dissipation, T =
-          // y*gx - x*gy - gp, Hs = the absolute-value and speed terms.
-          float2 A[2], T[2], Hs[2];
+          // Accumulators per pair: A and D = linear terms and dissipation
+          // (x and y; heading and speeds: two shorter dependency chains),
+          // T = y*gx - x*gy - gp, Hs = the absolute-value and speed terms
+          // (scalar FMAs take |S| as an operand).
+          float2 A[2], D[2], T[2];
+          float Hs[2][2];
 
           // x: window x0-2 .. x0+5 (end rules at compile-time positions)
           {
@@ -501,8 +503,9 @@ __global__ void __launch_bounds__(TARGET_THREADS, 2)
             ER[h] = en;
             VN[h] = vnew;
             T[h] = __ffma2_rn(f2(-hps), S, T[h]);
-            A[h] = __ffma2_rn(f2(dap), J, A[h]);
-            Hs[h] = __fmul2_rn(f2(wes), abs2(S));
+            D[h] = __fmul2_rn(f2(dap), J);
+            Hs[h][0] = wes * fabsf(S.x);
+            Hs[h][1] = wes * fabsf(S.y);
           }
           // vE and vP: neighbour planes
           {
@@ -515,13 +518,14 @@ __global__ void __launch_bounds__(TARGET_THREADS, 2)
               sum_jump4<ORDER, true>(m2, m1, C, p1, p2, it.ie, g.nve, S, J);
 #pragma unroll
             for (int h = 0; h < 2; h++) {
-              A[h] = __ffma2_rn(f2(dae), J[h], A[h]);
+              D[h] = __ffma2_rn(f2(dae), J[h], D[h]);
               if (e_inner) {
-                Hs[h] = __ffma2_rn(f2(ke_in), abs2(S[h]), Hs[h]);
+                Hs[h][0] = fmaf(ke_in, fabsf(S[h].x), Hs[h][0]);
+                Hs[h][1] = fmaf(ke_in, fabsf(S[h].y), Hs[h][1]);
               } else {  // max(elo*ge, ehi*ge), ge = S * hes
                 const float2 ge = __fmul2_rn(f2(hes), S[h]);
-                Hs[h] = __fadd2_rn(Hs[h], make_float2(fmaxf(elo * ge.x, ehi * ge.x),
-                                                      fmaxf(elo * ge.y, ehi * ge.y)));
+                Hs[h][0] += fmaxf(elo * ge.x, ehi * ge.x);
+                Hs[h][1] += fmaxf(elo * ge.y, ehi * ge.y);
               }
             }
           }
@@ -535,13 +539,14 @@ __global__ void __launch_bounds__(TARGET_THREADS, 2)
               sum_jump4<ORDER, true>(m2, m1, C, p1, p2, it.iv, g.nvp, S, J);
 #pragma unroll
             for (int h = 0; h < 2; h++) {
-              A[h] = __ffma2_rn(f2(dav), J[h], A[h]);
+              D[h] = __ffma2_rn(f2(dav), J[h], D[h]);
               if (p_inner) {
-                Hs[h] = __ffma2_rn(f2(kv_in), abs2(S[h]), Hs[h]);
+                Hs[h][0] = fmaf(kv_in, fabsf(S[h].x), Hs[h][0]);
+                Hs[h][1] = fmaf(kv_in, fabsf(S[h].y), Hs[h][1]);
               } else {  // min(plo*gv, phi*gv), gv = S * hvs
                 const float2 gv = __fmul2_rn(f2(hvs), S[h]);
-                Hs[h] = __fadd2_rn(Hs[h], make_float2(fminf(plo * gv.x, phi * gv.x),
-                                                      fminf(plo * gv.y, phi * gv.y)));
+                Hs[h][0] += fminf(plo * gv.x, phi * gv.x);
+                Hs[h][1] += fminf(plo * gv.y, phi * gv.y);
               }
             }
           }
@@ -551,8 +556,10 @@ __global__ void __launch_bounds__(TARGET_THREADS, 2)
 #pragma unroll
           for (int h = 0; h < 2; h++) {
             const float2 v = h ? hi2(C) : lo2(C);
-            // H = A + Hs - wp * |T|
-            const float2 Hsum = __ffma2_rn(f2(-wp), abs2(T[h]), __fadd2_rn(A[h], Hs[h]));
+            // H = A + D + Hs - wp * |T|
+            const float2 Hs2 = make_float2(fmaf(-wp, fabsf(T[h].x), Hs[h][0]),
+                                           fmaf(-wp, fabsf(T[h].y), Hs[h][1]));
+            const float2 Hsum = __fadd2_rn(__fadd2_rn(A[h], D[h]), Hs2);
             float2 value =
                 __ffma2_rn(f2(dt), make_float2(fminf(Hsum.x, 0.f), fminf(Hsum.y, 0.f)), v);
             const float2 prev = BLEND ? (h ? hi2(prev4) : lo2(prev4)) : v;
@@ -597,9 +604,9 @@ __global__ void __launch_bounds__(TARGET_THREADS, 2)
           *reinterpret_cast<float4 *>(gdst) =
               make_float4(out[0].x, out[0].y, out[1].x, out[1].y);
         }
-        // Release this step's set (and the own planes it finished).
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&empty[slot]);
+        // Release this step's set (and the own planes it finished): each
+        // thread after its own reads, so no lane waits on another.
+        mbar_arrive(&empty[slot]);
         gs++;
         gdst += PP;
         garr += PP;

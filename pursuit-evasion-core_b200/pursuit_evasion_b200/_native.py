@@ -160,6 +160,13 @@ _P = ctypes.c_void_p
 _I64P = ctypes.POINTER(ctypes.c_int64)
 _DP = ctypes.POINTER(ctypes.c_double)
 
+class VehicleModel(ctypes.Structure):
+    """pe_vehicle_model: one car's limits, rectangle and control period."""
+    _fields_ = [(name, ctypes.c_double) for name in (
+        "speed_min", "speed_max", "acceleration", "max_curvature", "length", "width",
+        "control_dt")]
+
+
 # name -> (restype, argtypes)
 SIGNATURES = {
     "pe_version": (ctypes.c_int, []),
@@ -192,6 +199,19 @@ SIGNATURES = {
     "pe_relative_step_noalloc": (ctypes.c_int, [ctypes.POINTER(RelativeParams), _P, _P,
                                                 _P, ctypes.c_double, ctypes.c_double,
                                                 _P, _DP]),
+    "pe_geometry_clearance": (ctypes.c_int, [ctypes.POINTER(VehicleModel), _P,
+                                             ctypes.c_int64, _P, ctypes.c_int32,
+                                             ctypes.c_double, _P, ctypes.c_int32]),
+    "pe_geometry_backup_safe": (ctypes.c_int, [ctypes.POINTER(VehicleModel), _P,
+                                               ctypes.c_int64, _P, ctypes.c_int32,
+                                               ctypes.c_double, _P, ctypes.c_int32]),
+    "pe_geometry_actions": (ctypes.c_int, [ctypes.POINTER(VehicleModel), _P, ctypes.c_int64,
+                                           _P, ctypes.c_int32, ctypes.c_double, _P,
+                                           ctypes.c_int32, ctypes.c_double, _P, _P,
+                                           ctypes.c_int32]),
+    "pe_geometry_connections": (ctypes.c_int, [ctypes.POINTER(VehicleModel), _P, _P,
+                                               ctypes.c_int64, _P, ctypes.c_int32,
+                                               ctypes.c_double, _P, ctypes.c_int32]),
     "pe_relative_f64_create": (
         ctypes.c_int,
         [ctypes.POINTER(RelativeParams), ctypes.POINTER(ctypes.c_void_p)],

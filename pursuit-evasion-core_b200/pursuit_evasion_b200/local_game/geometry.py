@@ -2,8 +2,10 @@
 value (src/pursuit_evasion/local_game/geometry.py:15-70,
 reversible/footprint_map.py:11-30), as used by the compact contact game.
 
-Obstacle clearance and BARN map loading (geometry.py:76-160) belong to grid
-construction and are not part of this package."""
+`CircleArena.clearance` is the signed separation of a car's rectangle from
+the walls and circles (geometry.py:131-152), used on the host when queries
+are sampled; grid construction asks the GPU engine of local_game/engine.py.
+Loading BARN occupancy maps (geometry.py:76-129) stays with the caller."""
 
 from __future__ import annotations
 
@@ -71,6 +73,26 @@ class CircleArena:
     def from_dict(cls, d):
         return cls(d["circles"], d["half_width"], Footprint(**d["pursuer"]),
                    Footprint(**d["evader"]), d.get("source"))
+
+    def clearance(self, poses, role="pursuer"):
+        """Signed separation of `role`'s rectangle at poses [..., >= 3]
+        (x, y, heading) from the arena walls and every circle; <= 0 means
+        contact."""
+        s = np.asarray(poses, float)
+        body = getattr(self, role)
+        c, q = np.cos(s[..., 2]), np.sin(s[..., 2])
+        half_x = (body.length * np.abs(c) + body.width * np.abs(q)) / 2
+        half_y = (body.length * np.abs(q) + body.width * np.abs(c)) / 2
+        out = np.minimum(self.half_width - np.abs(s[..., 0]) - half_x,
+                         self.half_width - np.abs(s[..., 1]) - half_y)
+        for cx, cy, r in self.circles:
+            dx, dy = cx - s[..., 0], cy - s[..., 1]
+            along = np.abs(dx * c + dy * q) - body.length / 2
+            across = np.abs(dy * c - dx * q) - body.width / 2
+            inside = np.minimum(np.maximum(along, across), 0)
+            out = np.minimum(out, np.hypot(np.maximum(along, 0), np.maximum(across, 0))
+                             + inside - r)
+        return out
 
     def capture_value(self, state):
         s = np.asarray(state)

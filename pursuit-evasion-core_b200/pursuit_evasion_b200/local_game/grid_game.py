@@ -12,10 +12,12 @@ the device (the reference launches two kernels per 256-state chunk and
 pursuer action, and in the memory-saving packed mode copies every output
 tile through the host).
 
-Grid construction from an arena (`make_grid`, which needs the reference's
-native geometry engine for legality and held-control successors) is not
-part of this package: build the `VehicleGrid` arrays with the reference's
-tools (or load a saved grid) and hand them over.
+Grid construction from an arena (`make_grid`, :158-196) asks the vehicle
+geometry (legality with a braking backup, held-control arcs, clear
+configuration paths) of local_game/engine.py, whose queries run on the GPU
+(csrc/vehicle_geometry_exact.cu); a grid bound to that geometry
+(`bind_geometry`) falls back, for states without multilinear support, to
+their nearest connected grid states (:38-79).
 """
 
 from __future__ import annotations
@@ -81,9 +83,59 @@ class VehicleGrid:
         ids = self.dense_to_compact[inds]
         w = np.where(ids >= 0, w, 0)
         mass = w.sum(1)
+        missing = valid & (mass <= 1e-9)
         valid &= mass > 1e-9
         w = np.divide(w, mass[:, None], out=np.zeros_like(w), where=mass[:, None] > 1e-9)
-        return np.maximum(ids, 0).astype(np.int32), w.astype(np.float32), valid, shape, mass
+        ids = np.maximum(ids, 0).astype(np.int32)
+        w = w.astype(np.float32)
+        if missing.any() and getattr(self, "_engine", None) is not None:
+            unique, inverse = np.unique(flat[missing], axis=0, return_inverse=True)
+            inverse = np.asarray(inverse).reshape(-1)
+            ni, nw, nv = self._nearest_supported(unique)
+            ids[missing], w[missing], valid[missing] = ni[inverse], nw[inverse], nv[inverse]
+        return ids, w, valid, shape, mass
+
+    def bind_geometry(self, arena, limits, role, dt=0.05, device=0):
+        """Attach the car's geometry: stencils of unsupported states then fall
+        back to nearby grid states reachable along a clear straight path."""
+        from .engine import GeometryEngine
+
+        self._engine = GeometryEngine(arena, limits, role, control_dt=dt, device=device)
+        self._tree = None
+        return self
+
+    def _nearest_supported(self, states, neighbours=64):
+        """Up to 16 of the `neighbours` nearest grid states (in position,
+        heading direction and speed, each scaled by its grid step) that a
+        clear straight configuration path reaches, weighted by inverse
+        squared feature distance; (ids, weights, valid)."""
+        from scipy.spatial import cKDTree
+
+        step_x = self.axes[0][1] - self.axes[0][0]
+        step_h = 2 * np.sin(np.pi / len(self.axes[2]))  # chord between headings
+        step_v = np.min(np.diff(self.axes[3]))
+
+        def features(s):
+            return np.column_stack([s[:, 0] / step_x, s[:, 1] / step_x,
+                                    np.cos(s[:, 2]) / step_h, np.sin(s[:, 2]) / step_h,
+                                    s[:, 3] / step_v])
+
+        if self._tree is None:
+            self._tree = cKDTree(features(self.states))
+        k = min(neighbours, len(self.states))
+        dist, index = self._tree.query(features(states), k=k)
+        dist, index = dist.reshape(len(states), k), index.reshape(len(states), k)
+        reach = self._engine.connections(np.repeat(states, k, axis=0),
+                                         self.states[index].reshape(-1, 4)).reshape(index.shape)
+        # the first 16 reachable neighbours in distance order
+        order = np.argsort(~reach, axis=1, kind="stable")[:, :STENCIL]
+        keep = np.take_along_axis(reach, order, 1)
+        ids = np.where(keep, np.take_along_axis(index, order, 1), 0).astype(np.int32)
+        inv = np.where(keep, 1.0 / np.maximum(np.take_along_axis(dist, order, 1), 1e-8) ** 2,
+                       0.0)
+        total = inv.sum(1, keepdims=True)
+        w = np.divide(inv, total, out=np.zeros_like(inv), where=total > 0).astype(np.float32)
+        return ids, w, keep.any(1)
 
     def save(self, path):
         np.savez_compressed(
@@ -100,12 +152,42 @@ class VehicleGrid:
                                     "weights", "allowed", "retained_mass")])
 
 
-def make_grid(arena, limits, role, *, position_step=0.3, headings=8, speeds=None, dt=0.05):
-    """Grid construction needs the reference's native geometry engine
-    (legality, held-control arcs with braking backups); not provided."""
-    raise NotImplementedError(
-        "make_grid needs the reference geometry engine; build the VehicleGrid "
-        "with the reference and pass it here (VehicleGrid.load)")
+def make_grid(arena, limits, role, *, position_step=0.3, headings=8, speeds=None, dt=0.05,
+              device=0):
+    """One car's vehicle grid in `arena` (grid_game.py:158-196): positions
+    every `position_step` across the arena (plus one node beyond each wall),
+    `headings` periodic headings from -pi and the given signed speeds; the
+    states that are clear with a braking backup are kept, and for each of
+    the 9 held controls (acceleration in {-A, 0, A} x curvature in {-K, 0,
+    K}) the successor after `dt` with its 16-vertex stencil, allowed where
+    the arc is clear, ends backup safe and has support."""
+    from .engine import GeometryEngine
+
+    if speeds is None:
+        speeds = [-1, 0, 0.5, 1, 2] if role == "pursuer" else [-0.5, 0, 0.25, 0.5, 1]
+    cells = int(round(2 * arena.half_width / position_step))
+    x = (np.arange(cells + 2) - (cells + 1) / 2) * position_step
+    heading = np.arange(headings) * 2 * np.pi / headings - np.pi
+    axes = (x, x, heading, np.array(speeds, float))
+    lattice = np.stack(np.meshgrid(*axes, indexing="ij"), -1).reshape(-1, 4)
+    engine = GeometryEngine(arena, limits, role, control_dt=dt, device=device)
+    legal = engine.backup_safe(lattice)
+    dense_to_compact = np.full(len(lattice), -1, np.int32)
+    dense_to_compact[legal] = np.arange(int(legal.sum()), dtype=np.int32)
+    kept = lattice[legal]
+    A, K = limits.acceleration, limits.max_curvature
+    controls = np.array([[a, k] for a in (-A, 0.0, A) for k in (-K, 0.0, K)], float)
+    grid = VehicleGrid(axes, kept, dense_to_compact, controls, None, None, None,
+                       None).bind_geometry(arena, limits, role, dt, device)
+    allowed, successor_states = engine.actions(kept, controls, dt)
+    ids, w, supported, _, mass = grid.stencil(successor_states)
+    grid.successors = ids.reshape(len(kept), len(controls), STENCIL)
+    grid.weights = w.reshape(len(kept), len(controls), STENCIL)
+    grid.allowed = allowed & supported.reshape(allowed.shape)
+    grid.retained_mass = mass.reshape(allowed.shape)
+    if not grid.allowed.any(axis=1).all():
+        raise ValueError("A retained state has no legal interpolable action")
+    return grid
 
 
 @dataclass

@@ -89,3 +89,16 @@ def test_packed_query_reads_the_product_stencil(cg):
     expected = np.einsum("na,nb,nab->n", pw, ew, dense[pi[:, :, None], ei[:, None, :]])
     np.testing.assert_allclose(
         cg.query_packed(flat, pi, pw, ei, ew, domain, n_e), expected, atol=1e-12)
+
+
+def test_arena_clearance_equals_the_reference_values():
+    """Signed rectangle clearance from walls and circles on the host, against
+    the reference CircleArena.clearance at golden random states."""
+    from pathlib import Path
+
+    from pursuit_evasion_b200.local_game.geometry import CircleArena
+
+    z = np.load(Path(__file__).resolve().parent / "golden" / "vehicle_grid_posts3m.npz")
+    arena = CircleArena(z["circles"], float(z["half_width"]))
+    np.testing.assert_allclose(arena.clearance(z["query_states"], "evader"),
+                               z["query_clearance"], rtol=0, atol=1e-12)

@@ -234,7 +234,7 @@ def test_fast_path_does_not_depend_on_the_tile():
         with RelativeSolver(A3, grid, local_precision="float32") as s:
             if tile is not None:
                 s.set_tile(*tile)
-                assert s.tile()[:2] == tile
+                assert s.tile[:2] == tile
             s.initialize()
             s.advance(0.15)
             results.append((s.field().copy(), s.arrival().copy()))
