@@ -424,9 +424,9 @@ __global__ void __launch_bounds__(TARGET_THREADS, 2)
         }
       }
 
-      // two steps per iteration let the carried heading state alternate
-      // registers; stage 2's larger body keeps one (no spills)
-#pragma unroll(BLEND ? 1 : 2)
+      // one step per iteration: unrolling by two spills on stage 1 and the
+      // local-memory traffic costs more than the saved register moves
+#pragma unroll 1
       for (int k = 0; k < it.steps; k++) {
         const unsigned slot = gs & 1u;
         if (k > 0 && alive) alive = wait_phase(&full[slot], (gs >> 1) & 1u, timeout);
