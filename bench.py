@@ -475,6 +475,7 @@ def semilag_section(with_cpu=True):
     with SemiLagrangianSolver(a3_config(), grid, mode="tube") as s:
         stream = _timing_stream()
         s.set_stream(stream.cuda_stream)
+        s.set_skip(False)  # every cell is backed up in every timed backup
         backups = math.ceil(HORIZON / s.dt - 1e-9)
         s.initialize()
         s.iterate(3, tol=0.0, check_every=3)  # warm-up

@@ -493,6 +493,16 @@ int pe_semilag_residual(pe_semilag *h, double *residual);
  * cells and backups it is the work per cell behind the backup's on-chip
  * rate; the generic kernel does not count (0). */
 int pe_semilag_evaluations(pe_semilag *h, int64_t *evaluations);
+/* Work skipping of the tiled value backups (on by default): a work item
+ * (one speed pair and y tile over all headings) whose neighbouring items
+ * (speed pairs and tiles +-1, the reach of every successor) left all their
+ * cells unchanged, bit for bit, in the previous backup reads the same
+ * inputs as then, so its cells are copied instead of recomputed.  Results
+ * are identical with and without it.  No counterpart in the reference. */
+int pe_semilag_set_skip(pe_semilag *h, int enable);
+/* Waits; work items of the tiled kernel computed (not skipped) since the
+ * last pe_semilag_init*. */
+int pe_semilag_items_computed(pe_semilag *h, int64_t *items);
 int pe_semilag_copy_value(pe_semilag *h, float *host_value);
 /* Copy the value field into a dense device array on the handle's device. */
 int pe_semilag_copy_value_device(pe_semilag *h, float *device_value);

@@ -27,6 +27,11 @@ struct pe_semilag {
   pe::SLSpeedStep *pstep = nullptr, *estep = nullptr;
   uint8_t *hint = nullptr;
   pe::SLTiledPlan plan{};
+  // per-item change flags of the last two tiled backups (work skipping)
+  unsigned *changed[2] = {nullptr, nullptr};
+  int changed_cur = 0;       // changed[changed_cur]: the last backup's flags
+  bool skip_valid = false;   // ... are those of the field now in `a`
+  bool skip_enabled = true;
   int smem_limit = 0;  // dynamic shared memory available to the tiled kernel
   bool tiled_ok = false;    // the tiled kernel applies to this grid and dt
   bool tiled_auto = false;  // ... and has enough work items to be the faster one
@@ -155,7 +160,8 @@ void release(pe_semilag *h) {
   for (void *ptr : {(void *)h->a, (void *)h->b, (void *)h->plane, (void *)h->pol_p,
                     (void *)h->pol_e, (void *)h->parc, (void *)h->earc,
                     (void *)h->emove, (void *)h->stats, (void *)h->pstep,
-                    (void *)h->estep, (void *)h->hint, (void *)h->arrival})
+                    (void *)h->estep, (void *)h->hint, (void *)h->arrival,
+                    (void *)h->changed[0], (void *)h->changed[1]})
     cudaFree(ptr);
   if (h->host_stats) cudaFreeHost(h->host_stats);
   if (h->own) cudaStreamDestroy(h->own);
@@ -200,10 +206,16 @@ int backup(pe_semilag *h, bool policy) {
   bk.stats = h->stats;
   cudaEvent_t e0 = h->timer.begin(h->stream);
   if (!policy && use_tiled(h)) {
-    const pe::SLTiled tl{h->pstep, h->estep, h->hint};
+    const bool skip = h->skip_enabled && h->skip_valid;
+    const pe::SLTiled tl{h->pstep, h->estep, h->hint,
+                         skip ? h->changed[h->changed_cur] : nullptr,
+                         h->changed[h->changed_cur ^ 1]};
     PE_CUDA_TRY(pe::sl_backup_tiled(h->g, bk, tl, h->plan, h->stream));
+    h->changed_cur ^= 1;
+    h->skip_valid = true;
   } else {
     PE_CUDA_TRY(pe::sl_backup(h->g, bk, h->stream));
+    h->skip_valid = false;  // the generic kernel keeps no change flags
   }
   pe::count_launches(1);
   {
@@ -347,6 +359,10 @@ int pe_semilag_create(const pe_semilag_params *params, pe_semilag **out) {
     take(cudaMalloc(&h->pstep, sizeof(pe::SLSpeedStep) * pstep.size()));
     take(cudaMalloc(&h->estep, sizeof(pe::SLSpeedStep) * estep.size()));
     take(cudaMalloc(&h->hint, (size_t)g.n));
+    // flags for the finest possible tiling (one row per tile)
+    const size_t flags = sizeof(unsigned) * (size_t)g.nvp * g.nve * g.nx;
+    take(cudaMalloc(&h->changed[0], flags));
+    take(cudaMalloc(&h->changed[1], flags));
     if (err == cudaSuccess) {
       take(cudaMemcpy(h->pstep, pstep.data(), sizeof(pe::SLSpeedStep) * pstep.size(),
                       cudaMemcpyHostToDevice));
@@ -393,6 +409,7 @@ int pe_semilag_init(pe_semilag *h, const float *initial) {
   h->iterations = 0;
   h->initialized = true;
   h->policy_valid = false;
+  h->skip_valid = false;
   return PE_OK;
 }
 
@@ -409,6 +426,7 @@ int pe_semilag_init_device(pe_semilag *h, const float *device_initial) {
   h->iterations = 0;
   h->initialized = true;
   h->policy_valid = false;
+  h->skip_valid = false;
   return PE_OK;
 }
 
@@ -466,6 +484,23 @@ int pe_semilag_evaluations(pe_semilag *h, int64_t *evaluations) {
   rc = read_stats(h);
   if (rc) return rc;
   *evaluations = (int64_t)h->host_stats->evaluations;
+  return PE_OK;
+}
+
+int pe_semilag_set_skip(pe_semilag *h, int enable) {
+  int rc = enter(h);
+  if (rc) return rc;
+  h->skip_enabled = enable != 0;
+  return PE_OK;
+}
+
+int pe_semilag_items_computed(pe_semilag *h, int64_t *items) {
+  int rc = enter(h);
+  if (rc) return rc;
+  if (!items) return fail(PE_EINVAL, "items is NULL");
+  rc = read_stats(h);
+  if (rc) return rc;
+  *items = (int64_t)h->host_stats->items_computed;
   return PE_OK;
 }
 
@@ -541,6 +576,7 @@ int pe_semilag_set_tile(pe_semilag *h, int32_t rows) {
     return fail(PE_EINVAL, "tile of %d rows does not fit the tiled kernel", rows);
   PE_CUDA_TRY(cudaStreamSynchronize(h->stream));
   h->plan = plan;
+  h->skip_valid = false;  // the flags index the old tiling
   return PE_OK;
 }
 

@@ -40,6 +40,8 @@ struct SLStats {
   // interpolated action-pair evaluations of the tiled kernel's live cells
   // (probes, full reply scans and pruned replies) since the last reset
   unsigned long long evaluations;
+  // work items of the tiled kernel computed (not skipped) since the last reset
+  unsigned long long items_computed;
 };
 
 struct SLBackup {
@@ -72,6 +74,14 @@ struct SLTiled {
   const SLSpeedStep *estep;  // [nve]
   uint8_t *hint;             // [cells]: (pursuer action << 4) | evader reply of
                              // the previous backup; 0x44 before the first
+  // Work skipping: changed_in[item] != 0 where some cell of the item changed
+  // (in its bits) in the previous backup; an item whose 3x3x3 neighbourhood
+  // of items (vP, vE, y tile +-1) did not change reads the same inputs as
+  // then, so its cells are copied instead of recomputed.  nullptr: every
+  // item is computed.  changed_out (may be nullptr) receives this backup's
+  // flags.
+  const unsigned *changed_in;
+  unsigned *changed_out;
 };
 
 struct SLTiledPlan {

@@ -315,6 +315,8 @@ SIGNATURES = {
                                           ctypes.POINTER(ctypes.c_int32)]),
     "pe_semilag_residual": (ctypes.c_int, [_P, _DP]),
     "pe_semilag_evaluations": (ctypes.c_int, [_P, _I64P]),
+    "pe_semilag_set_skip": (ctypes.c_int, [_P, ctypes.c_int]),
+    "pe_semilag_items_computed": (ctypes.c_int, [_P, _I64P]),
     "pe_semilag_copy_value": (ctypes.c_int, [_P, _P]),
     "pe_semilag_copy_value_device": (ctypes.c_int, [_P, _P]),
     "pe_semilag_copy_policy": (ctypes.c_int, [_P, _P, _P]),

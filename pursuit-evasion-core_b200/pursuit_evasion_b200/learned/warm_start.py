@@ -51,8 +51,13 @@ def converge(config, grid, *, dt, tol, initial=None, max_iterations=20000,
         s.value_to_device(u.data_ptr())
         torch.cuda.synchronize(dev)
         seconds = start.elapsed_time(end) / 1e3
-    return u, dict(iterations=iters, residual=residual, converged=converged,
-                   seconds=seconds)
+        computed = s.items_computed()
+        items = s.tile()["items"] if s.kernel == "tiled" else 0
+    info = dict(iterations=iters, residual=residual, converged=converged, seconds=seconds)
+    if items:
+        # work skipping: the share of tiled work items actually computed
+        info["items_computed_fraction"] = computed / (items * max(iters, 1))
+    return u, info
 
 
 def surrogate_start(net, config, grid, out):

@@ -139,6 +139,17 @@ class SemiLagrangianSolver:
         _native.check(self._lib.pe_semilag_evaluations(self._h, ctypes.byref(n)))
         return n.value
 
+    def set_skip(self, enable=True):
+        """Copy, instead of recomputing, the tiled work items whose
+        neighbourhood did not change in the previous backup (exact)."""
+        _native.check(self._lib.pe_semilag_set_skip(self._h, int(bool(enable))))
+
+    def items_computed(self):
+        """Tiled work items computed (not skipped) since initialisation."""
+        n = ctypes.c_int64()
+        _native.check(self._lib.pe_semilag_items_computed(self._h, ctypes.byref(n)))
+        return n.value
+
     def value(self, out=None):
         out = np.empty(self.cells, np.float32) if out is None else out
         _native.check(self._lib.pe_semilag_copy_value(self._h, out.ctypes.data))

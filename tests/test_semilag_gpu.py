@@ -260,3 +260,25 @@ def test_full_size_tiled_backup_spot_checks(oracle):
     ref2, _, _ = oracle.sl_backup_cells(cfg, v1.astype(np.float64), cells)
     np.testing.assert_allclose(v2[cells], ref2, atol=VALUE_ATOL, rtol=0)
     assert np.isfinite(v2).all() and np.all(v2 <= v1)
+
+
+@pytest.mark.parametrize("mode", ["tube", "min_time"])
+def test_work_skipping_is_exact_and_skips(mode):
+    """Tiled value iteration with and without work skipping: the same
+    residual sequence and iteration count, bit-identical fields, and fewer
+    items computed with skipping (items whose neighbourhood did not change
+    are copied)."""
+    grid = RelativeGrid(33, 24, 7, 7, 6.0)
+    out = {}
+    for skip in (False, True):
+        with SemiLagrangianSolver(A3, grid, mode=mode) as s:
+            s.set_kernel("tiled")
+            s.set_skip(skip)
+            s.initialize()
+            iters, residual, converged = s.iterate(600, tol=1e-5, check_every=5)
+            items = s.tile()["items"]
+            out[skip] = (s.value().copy(), iters, residual, s.items_computed())
+    assert out[True][1] == out[False][1] and out[True][2] == out[False][2]
+    np.testing.assert_array_equal(out[True][0].view(np.uint32), out[False][0].view(np.uint32))
+    assert out[False][3] == items * out[False][1]
+    assert out[True][3] < out[False][3]
