@@ -52,7 +52,7 @@ def converge(config, grid, *, dt, tol, initial=None, max_iterations=20000,
         torch.cuda.synchronize(dev)
         seconds = start.elapsed_time(end) / 1e3
         computed = s.items_computed()
-        items = s.tile()["items"] if s.kernel == "tiled" else 0
+        items = s.tile["items"] if s.kernel == "tiled" else 0
     info = dict(iterations=iters, residual=residual, converged=converged, seconds=seconds)
     if items:
         # work skipping: the share of tiled work items actually computed

@@ -303,3 +303,21 @@ def test_fp64_table_error_of_float32_tables_on_the_subsampled_tile(oracle):
     assert expected["nodes"] == 9 * 9 * 12 * 17 * 17
     assert errors["float32"]["max_abs"] <= 2 * expected["max_abs"]
     assert errors["float32"]["mean_abs"] <= 2 * expected["mean_abs"]
+
+
+def test_compile_time_tile_equals_the_general_kernel():
+    """On 65-position grids the default 13-row tile runs a variant with
+    compile-time offsets; any other tile runs the general kernel.  Both give
+    the same bits."""
+    grid = RelativeGrid(65, 8, 5, 5, 8.0)
+    results = []
+    for tile in ((13, 8), (5, 8), (13, 4)):
+        with RelativeSolver(A3, grid, local_precision="float32") as s:
+            s.set_tile(*tile)
+            s.initialize()
+            s.advance(0.05)
+            results.append((s.field().copy(), s.arrival().copy(), s.stats()[0]))
+    for field, arrival, residual in results[1:]:
+        np.testing.assert_array_equal(bits(field), bits(results[0][0]))
+        np.testing.assert_array_equal(bits(arrival), bits(results[0][1]))
+        assert residual == results[0][2]

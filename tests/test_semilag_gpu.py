@@ -276,7 +276,7 @@ def test_work_skipping_is_exact_and_skips(mode):
             s.set_skip(skip)
             s.initialize()
             iters, residual, converged = s.iterate(600, tol=1e-5, check_every=5)
-            items = s.tile()["items"]
+            items = s.tile["items"]
             out[skip] = (s.value().copy(), iters, residual, s.items_computed())
     assert out[True][1] == out[False][1] and out[True][2] == out[False][2]
     np.testing.assert_array_equal(out[True][0].view(np.uint32), out[False][0].view(np.uint32))
