@@ -573,6 +573,17 @@ int pe_mlp_gemm(const void *A, const void *B, int M, int N, int K, int lda, int 
 int pe_mlp_gemm_tc(const void *A, const void *B, int M, int N, int K, int lda, int ldb,
                    int epilogue, float *C32, void *C16, int ldc, const float *bias,
                    const float *zpre, void *cuda_stream);
+/* C32 += A B^T on the tensor cores with split-K: both operands K-major as
+ * pe_mlp_gemm_tc, the K range cut into `splits` equal parts, one CTA per
+ * 128 x 128 tile and part, each adding its partial tile to C32 with 16-byte
+ * FP32 atomics (C32 pre-zeroed by the caller; the summation order, and so
+ * the last bits, vary between runs).  The weight gradients of the
+ * surrogate: A = transposed activation gradients [out][rows], B =
+ * transposed layer inputs [in][rows], K = rows.  M, N multiples of 128, K a
+ * multiple of 64 * splits; A, B, C32 16-byte aligned; lda, ldb >= K
+ * multiples of 8; ldc >= N a multiple of 4. */
+int pe_mlp_gemm_tc_splitk(const void *A, const void *B, int M, int N, int K, int lda, int ldb,
+                          int splits, float *C32, int ldc, void *cuda_stream);
 /* Number of pe_mlp_gemm_tc launches whose bounded waits timed out since the
  * last call (then cleared).  Synchronises the device. */
 int pe_mlp_gemm_tc_timeouts(int32_t *count);

@@ -8,8 +8,10 @@
 // and B stored as [N][K], the layout of a Linear layer's weight), the case
 // of the forward layers and, with a transposed weight copy, of the
 // activation gradients.  Epilogues as pe_mlp_gemm: 0 FP32 store, 1 bias +
-// SiLU (FP32 pre-activation optional, BF16 activation), 3 product with
-// SiLU'(pre-activation) to BF16.
+// SiLU (FP32 pre-activation optional, BF16 activation), 2 FP32 accumulate
+// (split-K: grid z splits the K range, each CTA adds its partial tile with
+// 16-byte vector atomics; the weight gradients, from transposed activation
+// copies), 3 product with SiLU'(pre-activation) to BF16.
 //
 // CTA tile 128 x TN x 64 (TN = 256 where N allows, else 128), 2 pipeline
 // stages (the surrogate's K is 128 or 256; 97 KB of shared memory and 256
@@ -124,6 +126,7 @@ __device__ __forceinline__ void mma_commit(uint64_t *bar) {
 
 struct TcArgs {
   int M, N, K, ldc;
+  int ksteps;  // k-steps of TK per CTA (K / TK without split-K)
   float *C32;
   __nv_bfloat16 *C16;
   const float *bias, *zpre;
@@ -148,7 +151,7 @@ __global__ void __launch_bounds__(THREADS, 1)
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int m0 = blockIdx.y * TM, n0 = blockIdx.x * TN;
-  const int kt = g.K / TK;
+  const int kt = g.ksteps, kbase = blockIdx.z * g.ksteps;  // this CTA's K range
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; s++) {
@@ -179,8 +182,8 @@ __global__ void __launch_bounds__(THREADS, 1)
       if (k >= STAGES) ok = mbar_wait(&empty[s], ((k / STAGES) - 1) & 1, g.error);
       if (!ok) break;
       mbar_expect_tx(&full[s], A_BYTES + B_BYTES);
-      tma_load_2d(sA + s * A_BYTES, &tma_a, k * TK, m0, &full[s]);
-      tma_load_2d(sB + s * B_BYTES, &tma_b, k * TK, n0, &full[s]);
+      tma_load_2d(sA + s * A_BYTES, &tma_a, (kbase + k) * TK, m0, &full[s]);
+      tma_load_2d(sB + s * B_BYTES, &tma_b, (kbase + k) * TK, n0, &full[s]);
       issued = k + 1;
     }
     // no copy may still be landing when the CTA leaves: wait (bounded) for
@@ -232,7 +235,18 @@ __global__ void __launch_bounds__(THREADS, 1)
 #pragma unroll
     for (int j = 0; j < 32; j++) stage[lane * 33 + j] = __uint_as_float(r[j]);
     __syncwarp();
-    if (have) {
+    if (have && EPI == 2) {
+      // lane l adds columns 4(l%8) .. 4(l%8)+3 of row l/8 of each group of
+      // four rows: one 16-byte atomic per lane, 128 contiguous bytes per row
+      const int rs = lane >> 3, cq = (lane & 7) * 4;
+#pragma unroll 4
+      for (int rr = 0; rr < 32; rr += 4) {
+        const int rl = rr + rs;
+        const float *src = stage + rl * 33 + cq;
+        float *dst = g.C32 + (size_t)(m0 + warp * 32 + rl) * g.ldc + n0 + c0 + cq;
+        atomicAdd(reinterpret_cast<float4 *>(dst), make_float4(src[0], src[1], src[2], src[3]));
+      }
+    } else if (have) {
       const int n = n0 + c0 + lane;
       const float bn = EPI == 1 ? g.bias[n] : 0.f;
 #pragma unroll 4
@@ -317,7 +331,7 @@ cudaError_t launch(const CUtensorMap &a, const CUtensorMap &b, const TcArgs &g,
   cudaError_t e =
       cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  kernel<<<dim3(g.N / TN, g.M / TM), THREADS, smem, stream>>>(a, b, g);
+  kernel<<<dim3(g.N / TN, g.M / TM, g.K / (g.ksteps * TK)), THREADS, smem, stream>>>(a, b, g);
   return cudaGetLastError();
 }
 
@@ -357,12 +371,38 @@ int pe_mlp_gemm_tc(const void *A, const void *B, int M, int N, int K, int lda, i
   if (make_map(&ma, A, M, K, lda, TM) != CUDA_SUCCESS ||
       make_map(&mb, B, N, K, ldb, tn) != CUDA_SUCCESS)
     return fail(PE_EINVAL, "gemm_tc: tensor map encoding failed");
-  TcArgs g{M, N, K, ldc, C32, static_cast<__nv_bfloat16 *>(C16), bias, zpre, error_word()};
+  TcArgs g{M, N, K, ldc, K / TK, C32, static_cast<__nv_bfloat16 *>(C16), bias, zpre,
+           error_word()};
   if (!g.error) return fail(PE_ENOMEM, "gemm_tc: error word");
   cudaStream_t s = static_cast<cudaStream_t>(cuda_stream);
   cudaError_t e = tn == 256 ? launch_epi<256>(epilogue, ma, mb, g, s)
                             : launch_epi<128>(epilogue, ma, mb, g, s);
   if (e != cudaSuccess) return cuda_fail(e, "pe_mlp_gemm_tc");
+  count_launches(1);
+  return PE_OK;
+}
+
+int pe_mlp_gemm_tc_splitk(const void *A, const void *B, int M, int N, int K, int lda, int ldb,
+                          int splits, float *C32, int ldc, void *cuda_stream) {
+  using namespace pe;
+  if (!A || !B || !C32 || M <= 0 || N <= 0 || K <= 0 || splits < 1 || M % TM || N % 128 ||
+      K % (TK * splits))
+    return fail(PE_EINVAL,
+                "gemm_tc_splitk: M, N multiples of 128, K a multiple of 64 * splits");
+  if ((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(B) |
+       reinterpret_cast<uintptr_t>(C32)) % 16 ||
+      lda % 8 || ldb % 8 || lda < K || ldb < K || ldc % 4 || ldc < N)
+    return fail(PE_EINVAL,
+                "gemm_tc_splitk: 16-byte aligned operands and C, lda, ldb >= K multiples "
+                "of 8, ldc >= N a multiple of 4");
+  CUtensorMap ma, mb;
+  if (make_map(&ma, A, M, K, lda, TM) != CUDA_SUCCESS ||
+      make_map(&mb, B, N, K, ldb, 128) != CUDA_SUCCESS)
+    return fail(PE_EINVAL, "gemm_tc_splitk: tensor map encoding failed");
+  TcArgs g{M, N, K, ldc, K / (TK * splits), C32, nullptr, nullptr, nullptr, error_word()};
+  if (!g.error) return fail(PE_ENOMEM, "gemm_tc_splitk: error word");
+  cudaError_t e = launch<2, 128>(ma, mb, g, static_cast<cudaStream_t>(cuda_stream));
+  if (e != cudaSuccess) return cuda_fail(e, "pe_mlp_gemm_tc_splitk");
   count_launches(1);
   return PE_OK;
 }

@@ -354,12 +354,14 @@ __global__ void __launch_bounds__(SL_TILED_MAX_THREADS, 1)
 #pragma unroll
         for (int a = 0; a < 3; a++) {
           const int lo = ps.slot[a];
-          const float w = ps.w[a], w0 = 1.f - w;
+          const float w = ps.w[a];
 #pragma unroll
           for (int e = 0; e < 3; e++) {
             const float x0 = lo == 0 ? v[e] : v[3 + e];
             const float x1 = lo == 0 ? v[3 + e] : v[6 + e];
-            pv[a][e] = fmaf(w, x1, w0 * x0);
+            // x0 + w (x1 - x0): equal speeds blend to the value itself, bit
+            // for bit, so an unchanged neighbourhood backs up unchanged
+            pv[a][e] = fmaf(w, x1 - x0, x0);
           }
         }
 #pragma unroll
@@ -367,10 +369,10 @@ __global__ void __launch_bounds__(SL_TILED_MAX_THREADS, 1)
 #pragma unroll
           for (int e = 0; e < 3; e++) {
             const int lo = es.slot[e];
-            const float w = es.w[e], w0 = 1.f - w;
+            const float w = es.w[e];
             const float x0 = lo == 0 ? pv[a][0] : pv[a][1];
             const float x1 = lo == 0 ? pv[a][1] : pv[a][2];
-            const float nv = fmaf(w, x1, w0 * x0);
+            const float nv = fmaf(w, x1 - x0, x0);
             const int c = (a * 3 + e) * 2 * pl + off;
             if (advance) {
               upper[c] = make_float2(prev[c].y, nv);

@@ -348,6 +348,8 @@ SIGNATURES = {
                                                                    _P, _P, _P]),
     "pe_mlp_gemm_tc": (ctypes.c_int, [_P, _P] + [ctypes.c_int] * 6 + [_P, _P, ctypes.c_int,
                                                                      _P, _P, _P]),
+    "pe_mlp_gemm_tc_splitk": (ctypes.c_int, [_P, _P] + [ctypes.c_int] * 6 + [_P, ctypes.c_int,
+                                                                            _P]),
     "pe_mlp_gemm_tc_timeouts": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int32)]),
     "pe_mlp_adam": (ctypes.c_int, [_P, _P, _P, _P, _P, ctypes.c_int64, ctypes.c_float,
                                    ctypes.c_float, ctypes.c_float, ctypes.c_float, _P,

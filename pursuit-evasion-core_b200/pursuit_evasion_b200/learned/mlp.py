@@ -7,7 +7,10 @@ The features of a relative 5D state [x, y, psi, vP, vE] are
 state, the same per car.  Every forward, backward and Adam kernel is
 hand-written (csrc/mlp.cu, csrc/mlp_tc.cu, C ABI pe_mlp_*): the layer and
 activation-gradient GEMMs run on the tensor cores with tcgen05.mma and the
-accumulator in tensor memory, the split-K weight-gradient GEMM on mma.sync.
+accumulator in tensor memory, the split-K weight-gradient GEMM on mma.sync,
+which reads the row-major activations as they are (the tcgen05 split-K
+product, pe_mlp_gemm_tc_splitk, is faster alone but needs both operands
+transposed first, and the transposes cost more than it saves).
 PyTorch only provides device memory, the stream, random numbers for
 minibatches and, in the tests, the FP64 autograd that checks the gradients.  The reference's precedent is a
 SiLU MLP trained with Adam on MSE against DP labels

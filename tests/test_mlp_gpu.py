@@ -196,3 +196,34 @@ def test_tensor_core_gemm_epilogues(M):
     ref, _, zpre, _, C16 = gemm_tc_case(3, M=M)
     s = torch.sigmoid(zpre)
     torch.testing.assert_close(C16, ref * s * (1 + zpre * (1 - s)), rtol=1e-2, atol=5e-2)
+
+
+# (M, N, K, splits): one k-step per CTA, several, and the surrogate's
+# weight-gradient shape (256 x 256 over a batch of 8192 rows)
+@pytest.mark.parametrize("M, N, K, splits", [(128, 128, 256, 4), (256, 128, 1024, 4),
+                                             (256, 256, 8192, 32), (384, 256, 512, 1)])
+def test_tensor_core_split_k_accumulates(M, N, K, splits):
+    """pe_mlp_gemm_tc_splitk adds A B^T to what C32 holds, over `splits` K
+    ranges with vector atomics; against the FP32 product of the same bf16
+    operands."""
+    import ctypes
+
+    from pursuit_evasion_b200 import _native
+
+    g = torch.Generator().manual_seed(M + K + splits)
+    A = torch.randn(M, K, generator=g).to(torch.bfloat16)
+    B = torch.randn(N, K, generator=g).to(torch.bfloat16)
+    C0 = torch.randn(M, N, generator=g)
+    ref = C0 + A.float() @ B.float().t()
+    dev = torch.device("cuda", 0)
+    Ad, Bd, C = A.to(dev), B.to(dev), C0.to(dev)
+    lib = _native.library()
+    p = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+    _native.check(lib.pe_mlp_gemm_tc_splitk(
+        p(Ad), p(Bd), M, N, K, K, K, splits, p(C), N,
+        ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+    torch.cuda.synchronize()
+    timeouts = ctypes.c_int32()
+    _native.check(lib.pe_mlp_gemm_tc_timeouts(ctypes.byref(timeouts)))
+    assert timeouts.value == 0
+    torch.testing.assert_close(C.cpu(), ref, rtol=1e-4, atol=1e-3 * (K / 256) ** 0.5)
