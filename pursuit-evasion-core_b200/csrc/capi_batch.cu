@@ -365,7 +365,7 @@ int pe_batch_synchronize(pe_batch *h) {
   PE_CUDA_TRY(cudaMemcpyAsync(h->host_stats, h->stats, sizeof(pe::Rel5Stats) * h->count,
                               cudaMemcpyDeviceToHost, h->stream));
   PE_CUDA_TRY(cudaStreamSynchronize(h->stream));
-  if (h->host_sync[2]) return fail(PE_ETIMEOUT, "batch: a grid barrier wait gave up");
+  if (h->host_sync[2]) return fail(PE_ETIMEOUT, "batch: a bounded device wait (grid barrier or staged heading) gave up");
   for (int i = 0; i < h->count; i++)
     if (h->host_stats[i].nonfinite)
       return fail(PE_ENONFINITE, "batch: non-finite field update in solve %d", i);

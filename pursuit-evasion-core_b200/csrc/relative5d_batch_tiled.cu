@@ -6,12 +6,15 @@
 // A work item is `rows` y rows of one (vP, vE) plane stack of one solve, all
 // headings.  A thread owns a 4-cell x chunk of one row and walks the
 // headings with a 5-heading register window (the psi stencil).  For each
-// heading the CTA stages, with 16-byte cp.async copies double-buffered
-// against the previous heading's arithmetic, the item's own plane rows with
-// a 2-row y halo and the rows of the 8 speed-neighbour planes (vE +-1, +-2,
-// vP +-1, +-2); the x, y and speed stencils then read shared memory.  The
-// persistent loop over steps, the active-item prefix and the bounded grid
-// barrier are those of relative5d_batch_impl.cuh.
+// heading the CTA stages, double-buffered against the previous heading's
+// arithmetic, the item's own plane rows with a 2-row y halo and the rows of
+// the 8 speed-neighbour planes (vE +-1, +-2, vP +-1, +-2): thread 0 issues
+// one bulk copy (cp.async.bulk, the TMA engine) per contiguous row range,
+// nine at most, all completing on the buffer's mbarrier, on which every
+// thread waits (bounded); the x, y and speed stencils then read shared
+// memory.  The persistent loop over steps, the active-item prefix and the
+// bounded grid barrier are those of relative5d_batch_impl.cuh.
+#include "bulk_copy.cuh"
 #include "relative5d_batch_impl.cuh"
 #include "relative5d_eno_f32.cuh"
 
@@ -22,18 +25,29 @@ using namespace eno32;
 
 constexpr int kThreads = kRel5BatchThreads;
 constexpr int kNb = 8;  // vE-2, vE-1, vE+1, vE+2, vP-2, vP-1, vP+1, vP+2
+// tries of a bounded wait for a staged heading
+constexpr unsigned kStageWaitLimit = 1u << 22;
 
-__device__ __forceinline__ void cp_async16(float *dst, const float *src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
-                   (unsigned)__cvta_generic_to_shared(dst)),
-               "l"(src)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() {
-  asm volatile("cp.async.commit_group;" ::: "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() {
-  asm volatile("cp.async.wait_group 0;" ::: "memory");
+// The two heading buffers' mbarriers, and the flag a wait that gives up
+// raises (set once per launch).
+__shared__ uint64_t stage_bar[2];
+__shared__ unsigned *stage_timeout;
+
+// Fill state of the two heading buffers, the same in every thread of the
+// CTA: bit b = number of fills of buffer b mod 2, bit 2 + b = buffer b was
+// filled at least once.
+struct StageRing {
+  unsigned bits = 0;
+  // parity of the mbarrier phase of buffer b's latest fill
+  __device__ __forceinline__ unsigned parity(int b) const { return ((bits >> b) & 1u) ^ 1u; }
+  __device__ __forceinline__ void filled(int b) { bits = (bits ^ (1u << b)) | (4u << b); }
+  __device__ __forceinline__ bool used(int b) const { return (bits >> (2 + b)) & 1u; }
+};
+
+__device__ __forceinline__ void wait_staged(const StageRing &ring, int b) {
+  for (unsigned i = 0; i < kStageWaitLimit; i++)
+    if (bulk::mbar_try_wait(&stage_bar[b], ring.parity(b))) return;
+  atomicOr(stage_timeout, 1u);
 }
 
 // Shared memory of one heading: own rows [R + 4][xp] then [kNb][R][xp].
@@ -45,42 +59,51 @@ struct ItemGeom {
   int iv, ie, y0, r_eff, R, xc;
 };
 
-// Stage heading `psi` of an item into buffer `buf`.
+// Stage heading `psi` of an item into buffer `buf` (called by warp 0): the
+// own plane rows y0-2 .. y0+r_eff+1 inside the box (lane 8) and rows
+// y0 .. y0+r_eff-1 of each speed-neighbour plane inside the grid (lane q for
+// neighbour q), each a contiguous range (rows are xp floats, xp a multiple
+// of 4, so every range starts and ends on 16 bytes), completing on `bar`.
+// Lane 0 first posts the byte count of all of them.
 __device__ __forceinline__ void stage_heading(const Rel5Grid &g, const float *__restrict__ src,
-                                              const ItemGeom &it, int psi, float *buf) {
-  const int xp = g.xp, xc = it.xc;
+                                              const ItemGeom &it, int psi, float *buf,
+                                              uint64_t *bar) {
+  const int lane = threadIdx.x & 31;
+  const int xp = g.xp;
   const int64_t PP = (int64_t)g.nx * xp;
-  // own plane rows y0-2 .. y0+r_eff+1 (inside the box)
+  const uint32_t nb_bytes = (uint32_t)(it.r_eff * xp * 4);
   const int lo = max(0, it.y0 - 2), hi = min(g.nx, it.y0 + it.r_eff + 2);
-  const float *own_src = src + (((int64_t)it.iv * g.nve + it.ie) * g.nh + psi) * PP;
-  const int own_chunks = (hi - lo) * xc;
-  for (int k = threadIdx.x; k < own_chunks; k += kThreads) {
-    const int row = lo + k / xc, col = 4 * (k % xc);
-    cp_async16(buf + (row - it.y0 + 2) * xp + col, own_src + (int64_t)row * xp + col);
+  const uint32_t own_bytes = (uint32_t)((hi - lo) * xp * 4);
+  if (lane == 0) {
+    // speed neighbours inside the grid: vE-2..vE+2 and vP-2..vP+2 minus the
+    // centre, cut at the ends
+    const int count = min(it.ie + 2, g.nve - 1) - max(it.ie - 2, 0) +
+                      min(it.iv + 2, g.nvp - 1) - max(it.iv - 2, 0);
+    bulk::mbar_expect_tx(bar, own_bytes + (uint32_t)count * nb_bytes);
   }
-  // neighbour planes, rows y0 .. y0+r_eff-1
-  float *nbr = buf + (it.R + 4) * xp;
-  const int nb_chunks = it.r_eff * xc;
-#pragma unroll 1
-  for (int q = 0; q < kNb; q++) {
-    const int d = (q & 3) < 2 ? (q & 3) - 2 : (q & 3) - 1;  // -2, -1, +1, +2
-    const int nv = it.iv + (q < 4 ? 0 : d), ne = it.ie + (q < 4 ? d : 0);
-    if (nv < 0 || nv >= g.nvp || ne < 0 || ne >= g.nve) continue;
-    const float *nsrc = src + (((int64_t)nv * g.nve + ne) * g.nh + psi) * PP +
-                        (int64_t)it.y0 * xp;
-    float *ndst = nbr + q * it.R * xp;
-    for (int k = threadIdx.x; k < nb_chunks; k += kThreads) {
-      const int row = k / xc, col = 4 * (k % xc);
-      cp_async16(ndst + row * xp + col, nsrc + (int64_t)row * xp + col);
+  __syncwarp();
+  if (lane < kNb) {
+    const int d = (lane & 3) < 2 ? (lane & 3) - 2 : (lane & 3) - 1;  // -2, -1, +1, +2
+    const int nv = it.iv + (lane < 4 ? 0 : d), ne = it.ie + (lane < 4 ? d : 0);
+    if (nv >= 0 && nv < g.nvp && ne >= 0 && ne < g.nve) {
+      bulk::fence_async_shared();
+      bulk::bulk_load(buf + (it.R + 4 + lane * it.R) * xp,
+                      src + (((int64_t)nv * g.nve + ne) * g.nh + psi) * PP + (int64_t)it.y0 * xp,
+                      nb_bytes, bar);
     }
+  } else if (lane == kNb) {
+    bulk::fence_async_shared();
+    bulk::bulk_load(buf + (lo - it.y0 + 2) * xp,
+                    src + (((int64_t)it.iv * g.nve + it.ie) * g.nh + psi) * PP + (int64_t)lo * xp,
+                    own_bytes, bar);
   }
 }
 
 // One stage of one item (all headings).  Returns the largest |change| of
 // this thread's cells (stage 2) and flags non-finite values.
 template <int ORDER, int BLEND>
-__device__ void item_stage(const Rel5Grid &g, const Rel5Stage &s, const ItemGeom &it,
-                           float *smem, float &change_max, float &change_up,
+__device__ __forceinline__ void item_stage(const Rel5Grid &g, const Rel5Stage &s, const ItemGeom &it,
+                           float *smem, StageRing &ring, float &change_max, float &change_up,
                            float2 &finite_acc) {
   const int xp = g.xp, xc = it.xc;
   const int64_t PP = (int64_t)g.nx * xp;
@@ -130,13 +153,17 @@ __device__ void item_stage(const Rel5Grid &g, const Rel5Stage &s, const ItemGeom
 #pragma unroll
   for (int d = 0; d < 5; d++) win[d] = load_window(d - 2);
 
-  stage_heading(g, s.src, it, 0, smem);
-  cp_async_commit();
+  if (tid < 32) stage_heading(g, s.src, it, 0, smem, &stage_bar[0]);
+  ring.filled(0);
   for (int k = 0; k < nh; k++) {
-    cp_async_wait_all();
+    const int b = k & 1;
+    wait_staged(ring, b);
     __syncthreads();  // heading k staged; heading k-1's buffer no longer read
-    if (k + 1 < nh) stage_heading(g, s.src, it, k + 1, smem + ((k + 1) & 1) * bufsz);
-    cp_async_commit();
+    if (k + 1 < nh) {
+      if (tid < 32)
+        stage_heading(g, s.src, it, k + 1, smem + (b ^ 1) * bufsz, &stage_bar[b ^ 1]);
+      ring.filled(b ^ 1);
+    }
     const float4 next = k + 1 < nh ? load_window(k + 3) : make_float4(0.f, 0.f, 0.f, 0.f);
     const float *own = smem + (k & 1) * bufsz;
     if (active) {
@@ -279,13 +306,12 @@ __device__ void item_stage(const Rel5Grid &g, const Rel5Stage &s, const ItemGeom
     for (int d = 0; d < 4; d++) win[d] = win[d + 1];
     win[4] = next;
   }
-  cp_async_wait_all();
   __syncthreads();  // the buffers are restaged by the next item
 }
 
 template <int BLEND>
-__device__ void tiled_stage(const Rel5BatchArgs &A, int step, int64_t n_items, double *scratch,
-                            Rel5Grid *sg, float *smem) {
+__device__ __forceinline__ void tiled_stage(const Rel5BatchArgs &A, int step, int64_t n_items, double *scratch,
+                            Rel5Grid *sg, float *smem, StageRing &ring) {
   int64_t lo = 0, hi = 0;
   const Rel5BatchSolve *S = nullptr;
   Rel5Stage s{};
@@ -340,7 +366,7 @@ __device__ void tiled_stage(const Rel5BatchArgs &A, int step, int64_t n_items, d
     it.xc = xc;
     it.y0 = slab * rows;
     it.r_eff = min(rows, g.nx - it.y0);
-    item_stage<2, BLEND>(g, s, it, smem, change_max, change_up, finite_acc);
+    item_stage<2, BLEND>(g, s, it, smem, ring, change_max, change_up, finite_acc);
   }
   flush();
 }
@@ -350,16 +376,32 @@ __global__ void __launch_bounds__(kThreads, 2)
   extern __shared__ __align__(16) float smem[];
   __shared__ double scratch[kThreads / 32];
   __shared__ Rel5Grid sg;
+  if (threadIdx.x == 0) {
+    bulk::mbar_init(&stage_bar[0], 1);
+    bulk::mbar_init(&stage_bar[1], 1);
+    bulk::fence_barrier_init();
+    // a stage wait that gives up raises the grid barrier's flag: every CTA
+    // leaves at its next barrier and the host reports the timeout
+    stage_timeout = &A.sync[2];
+  }
+  __syncthreads();
+  StageRing ring;
   unsigned round = 0;
   for (int step = 0; step < A.max_steps; step++) {
     const int64_t n_items = A.active_items[step];
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < A.count;
          k += gridDim.x * blockDim.x)
       if (step < A.solves[k].nsteps) A.solves[k].stats->residual = 0ull;
-    tiled_stage<0>(A, step, n_items, scratch, &sg, smem);
+    tiled_stage<0>(A, step, n_items, scratch, &sg, smem, ring);
     if (!batch_impl::grid_barrier(A.sync, ++round)) break;
-    tiled_stage<1>(A, step, n_items, scratch, &sg, smem);
+    tiled_stage<1>(A, step, n_items, scratch, &sg, smem, ring);
     if (!batch_impl::grid_barrier(A.sync, ++round)) break;
+  }
+  // no bulk copy may still be landing when the CTA exits (complete already
+  // unless a wait gave up)
+  if (threadIdx.x == 0) {
+    if (ring.used(0)) wait_staged(ring, 0);
+    if (ring.used(1)) wait_staged(ring, 1);
   }
 }
 
