@@ -28,6 +28,7 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kMaxBlockBytes = 96 * 1024;  // per buffer; two buffers per CTA
+constexpr size_t kMaxColumnBytes = 112 * 1024;  // column kernel: two CTAs per SM
 
 // e / d as __umulhi(e, m), m = ceil(2^32 / d): exact for e * (m*d - 2^32) <
 // 2^32, which holds for e < 2^24 and d < 256 and, in general, for e < 2^32/d.
@@ -137,6 +138,9 @@ __device__ __forceinline__ void cp_async_commit() {
 }
 __device__ __forceinline__ void cp_async_wait_one() {
   asm volatile("cp.async.wait_group 1;" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
 template <int ORDER>
@@ -332,11 +336,348 @@ cudaError_t launch_block(const FastW8Args &a, size_t smem, cudaStream_t stream) 
   return cudaGetLastError();
 }
 
+
+// ------------------------------------------------------------ column kernel
+// The same stage with the work of a pursuer pose split in two passes, so
+// that no per-cell position or end-rule logic is left:
+//   B (a thread per vE column, i.e. per (xE, yE, thE)): the four evader-axis
+//     stencils from the staged block.  vE runs along the column in registers
+//     with its end rules at compile-time positions (NE nodes); thE wraps by
+//     per-column offsets; xE and yE read a copy of the block padded by two
+//     ghost rows on each side, filled once per pose with the reference's
+//     extrapolated values (native_world.cpp:44-58: the value beyond an end
+//     is the end node pushed by m times the end difference), so every
+//     position takes the interior formula.  The evader terms and their
+//     dissipation go to part[cell] in shared memory;
+//   A + C (a thread per cell, consecutive cells on consecutive lanes): the
+//     four pursuer-axis stencils from the 16 neighbouring blocks (coalesced
+//     L2 loads of the next cell issued while the current one computes; the
+//     pose, hence every pursuer end rule, is uniform over the CTA), then the
+//     update, RK2 average, tube, avoid floor, arrival and residual with
+//     coalesced loads and stores.
+// The block of the next pose is requested by cp.async (a warp per (xE, yE)
+// row) as soon as pass B is done, and lands during pass A + C.  Sums are
+// taken evader part first, so results differ from world8_block_kernel's by
+// float rounding.
+constexpr int kColThreads = 256;
+constexpr int kCBatch = 8;  // cells per thread whose update loads are issued together
+
+struct ColW8Args {
+  World8Grid g;
+  World8Stage s;
+  int inner, outer, ncols;
+  Divisor dnh, dn;
+};
+
+// shared memory floats: padded block [n+4][n+4][nh][NE] + partial sums [inner]
+inline size_t column_smem_bytes(const World8Grid &g) {
+  const size_t row = (size_t)g.nh * g.shape[7];
+  return sizeof(float) * row * ((size_t)(g.n + 4) * (g.n + 4) + (size_t)g.n * g.n);
+}
+
+template <int ORDER, int NE, int SKIND>
+__global__ void __launch_bounds__(kColThreads, 2)
+    world8_column_kernel(const ColW8Args a) {
+  extern __shared__ __align__(16) float sm[];
+  __shared__ float warp_max[kColThreads / 32];
+  const World8Grid &g = a.g;
+  const World8Stage &s = a.s;
+  const int inner = a.inner, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  constexpr int nwarps = kColThreads / 32;
+  const int n = g.n, nh = g.nh;
+  const int rowlen = nh * NE;                  // one (xE, yE) row: all (thE, vE)
+  const int sy = rowlen, sx = (n + 4) * rowlen;  // padded strides of yE and xE
+  float *pad = sm;                             // [n+4][n+4][nh][NE]
+  float *part = sm + (n + 4) * sx;             // [inner]
+  const float ih[8] = {g.inv_spacing[0], g.inv_spacing[1], g.inv_spacing[2],
+                       g.inv_spacing[3], g.inv_spacing[4], g.inv_spacing[5],
+                       g.inv_spacing[6], g.inv_spacing[7]};
+  float change_max = 0.f;
+  bool bad = false;
+
+  // the block of pose o into the padded interior, a warp per (xE, yE) row
+  auto stage_block = [&](int o) {
+    const float *src = s.src + (int64_t)o * inner;
+    for (int r = warp; r < n * n; r += nwarps) {
+      const int q4 = r / n, q5 = r - q4 * n;
+      float *dst = pad + (q4 + 2) * sx + (q5 + 2) * sy;
+      const float *row = src + r * rowlen;
+      for (int j = lane; j < rowlen; j += 32) cp_async4(dst + j, row + j);
+    }
+  };
+  // ghost rows beyond the xE and yE ends (needs the interior in place):
+  // side 0-3 xE = -2, -1, n, n+1 at yE = idx; side 4-7 the same along yE at
+  // xE = idx
+  auto fill_ghosts = [&]() {
+    for (int gr = warp; gr < 8 * n; gr += nwarps) {
+      const int side = gr / n, idx = gr - side * n;
+      const int q = side & 3;  // ghost position -2, -1, n, n+1
+      const int pos = q < 2 ? q - 2 : n - 2 + q;
+      const float m = q == 0 || q == 3 ? 2.f : 1.f;
+      const int end = q < 2 ? 0 : n - 1, next = q < 2 ? 1 : n - 2;
+      const int along = side < 4 ? sx : sy, across = side < 4 ? sy : sx;
+      const float *row_a = pad + (end + 2) * along + (idx + 2) * across;
+      const float *row_b = pad + (next + 2) * along + (idx + 2) * across;
+      float *row_g = pad + (pos + 2) * along + (idx + 2) * across;
+      for (int j = lane; j < rowlen; j += 32) row_g[j] = ghost_value(row_a[j], row_b[j], m);
+    }
+  };
+
+  if ((int)blockIdx.x < a.outer) stage_block(blockIdx.x);
+  cp_async_commit();
+  for (int o = blockIdx.x; o < a.outer; o += gridDim.x) {
+    // pursuer pose (uniform over the CTA)
+    int qp[4];
+    {
+      int rest = o;
+      qp[3] = rest % g.shape[3];
+      rest /= g.shape[3];
+      qp[2] = rest % g.shape[2];
+      rest /= g.shape[2];
+      qp[1] = rest % g.shape[1];
+      qp[0] = rest / g.shape[1];
+    }
+    const float vp = __ldg(s.pv + qp[3]);
+    const float fpx = vp * __ldg(s.cs + qp[2]), fpy = vp * __ldg(s.sn + qp[2]);
+    const float wp = fabsf(vp) * g.kp;
+    const float palo = qp[3] == 0 ? 0.f : -g.ap;
+    const float pahi = qp[3] == g.np - 1 ? 0.f : g.ap;
+    const float wx_lo = fminf(fpx, 0.f) * ih[0], wx_hi = fmaxf(fpx, 0.f) * ih[0];
+    const float wy_lo = fminf(fpy, 0.f) * ih[1], wy_hi = fmaxf(fpy, 0.f) * ih[1];
+    float avoid = -INFINITY;
+    if (g.avoid_mode == 1) {
+      const float ax = fabsf(__ldg(s.x + qp[0])), ay = fabsf(__ldg(s.x + qp[1]));
+      avoid = (ax < ay ? ay : ax) - g.arena + 1e-6f;
+    } else if (g.avoid_mode == 2) {
+      avoid = -__ldg(s.p_clear + (qp[0] * g.n + qp[1]) * g.nh + qp[2]) + 1e-6f;
+    }
+    int poff[4][4];  // neighbour offsets along the pursuer axes, in cells
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      int om2, om1, op1, op2;
+      window_offsets(qp[k], g.shape[k], 1, k == 2, om2, om1, op1, op2);
+      const int st = (int)g.stride[k];
+      poff[k][0] = om2 * st;
+      poff[k][1] = om1 * st;
+      poff[k][2] = op1 * st;
+      poff[k][3] = op2 * st;
+    }
+    const int64_t j0 = (int64_t)o * inner;
+    const float *__restrict__ src_o = s.src + j0;
+
+    // A: pursuer axes, a thread per cell (consecutive cells on consecutive
+    // lanes), two cells at a time; the 2 x 17 loads (value and 16
+    // pursuer-axis neighbours, from L2 or HBM) of the next two cells are
+    // issued before the current two are computed
+    auto load_cells = [&](int e, float (&buf)[2][17]) {
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int c = min(e + h * kColThreads, inner - 1);
+        buf[h][16] = __ldg(src_o + c);
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+#pragma unroll
+          for (int m = 0; m < 4; m++) buf[h][4 * k + m] = __ldg(src_o + poff[k][m] + c);
+      }
+    };
+    auto pursuer_cells = [&](int e, const float (&buf)[2][17]) {
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int c = e + h * kColThreads;
+        if (c >= inner) break;
+        const float *v = buf[h];
+        const float f = v[16];
+        float dlo[4], dhi[4];
+        axis_slopes<ORDER>(v[0], v[1], f, v[2], v[3], qp[0], g.shape[0], kExtrapolated,
+                           dlo[0], dhi[0]);
+        axis_slopes<ORDER>(v[4], v[5], f, v[6], v[7], qp[1], g.shape[1], kExtrapolated,
+                           dlo[1], dhi[1]);
+        axis_slopes<ORDER>(v[8], v[9], f, v[10], v[11], qp[2], g.shape[2], kPeriodic, dlo[2],
+                           dhi[2]);
+        axis_slopes<ORDER>(v[12], v[13], f, v[14], v[15], qp[3], g.shape[3], SKIND, dlo[3],
+                           dhi[3]);
+        float total = fmaf(wx_lo, dlo[0], wx_hi * dhi[0]);
+        total = fmaf(wy_lo, dlo[1], fmaf(wy_hi, dhi[1], total));
+        const float g2 = 0.5f * ih[2] * (dlo[2] + dhi[2]);
+        total = fmaf(-wp, fabsf(g2), total);
+        const float g3 = 0.5f * ih[3] * (dlo[3] + dhi[3]);
+        total += fminf(palo * g3, pahi * g3);
+        float diss = wp * ih[2] * (dhi[2] - dlo[2]);
+        diss = fmaf(g.ap * ih[3], dhi[3] - dlo[3], diss);
+        part[c] = fmaf(0.5f, diss, total);
+      }
+    };
+    {
+      constexpr int step = 2 * kColThreads;
+      float bufA[2][17], bufB[2][17];
+      if (tid < inner) load_cells(tid, bufA);
+      for (int e = tid; e < inner; e += 2 * step) {
+        if (e + step < inner) load_cells(e + step, bufB);
+        pursuer_cells(e, bufA);
+        if (e + step >= inner) break;
+        if (e + 2 * step < inner) load_cells(e + 2 * step, bufA);
+        pursuer_cells(e + step, bufB);
+      }
+    }
+    cp_async_wait_all();
+    __syncthreads();  // the block and every pursuer part are in place
+    fill_ghosts();
+    __syncthreads();
+
+    // B: evader axes, a thread per vE column
+    for (int c = tid; c < a.ncols; c += kColThreads) {
+      int q6, q5;
+      const int r = split(c, a.dnh, q6);
+      const int q4 = split(r, a.dn, q5);
+      const float *col = pad + (q4 + 2) * sx + (q5 + 2) * sy + q6 * NE;
+      int om2, om1, op1, op2;
+      window_offsets(q6, nh, NE, true, om2, om1, op1, op2);
+      const float cs6 = __ldg(s.cs + q6), sn6 = __ldg(s.sn + q6);
+      float vc[NE];
+#pragma unroll
+      for (int i = 0; i < NE; i++) vc[i] = col[i];
+      float *pc = part + c * NE;
+#pragma unroll
+      for (int i = 0; i < NE; i++) {
+        const float f = vc[i];
+        float dlo4, dhi4, dlo5, dhi5, dlo6, dhi6, dlo7, dhi7;
+        // xE and yE: ghosts are in the padded block, every position is interior
+        axis_slopes<ORDER>(col[i - 2 * sx], col[i - sx], f, col[i + sx], col[i + 2 * sx], 2, 5,
+                           kPeriodic, dlo4, dhi4);
+        axis_slopes<ORDER>(col[i - 2 * sy], col[i - sy], f, col[i + sy], col[i + 2 * sy], 2, 5,
+                           kPeriodic, dlo5, dhi5);
+        axis_slopes<ORDER>(col[i + om2], col[i + om1], f, col[i + op1], col[i + op2], 2, 5,
+                           kPeriodic, dlo6, dhi6);
+        // vE: the column's registers, clamped window, compile-time end rules
+        axis_slopes<ORDER>(vc[i > 1 ? i - 2 : (i > 0 ? i - 1 : i)], vc[i > 0 ? i - 1 : i], f,
+                           vc[i < NE - 1 ? i + 1 : i],
+                           vc[i < NE - 2 ? i + 2 : (i < NE - 1 ? i + 1 : i)], i, NE, SKIND,
+                           dlo7, dhi7);
+        const float ve = __ldg(s.ev + i);
+        const float fex = ve * cs6, fey = ve * sn6;
+        const float we = fabsf(ve) * g.ke;
+        const float ealo = i == 0 ? 0.f : -g.ae;
+        const float eahi = i == NE - 1 ? 0.f : g.ae;
+        float total = fmaf(fminf(fex, 0.f) * ih[4], dlo4, fmaxf(fex, 0.f) * ih[4] * dhi4);
+        total = fmaf(fminf(fey, 0.f) * ih[5], dlo5, fmaf(fmaxf(fey, 0.f) * ih[5], dhi5, total));
+        const float g6 = 0.5f * ih[6] * (dlo6 + dhi6);
+        total = fmaf(we, fabsf(g6), total);
+        const float g7 = 0.5f * ih[7] * (dlo7 + dhi7);
+        total += fmaxf(ealo * g7, eahi * g7);
+        float diss = we * ih[6] * (dhi6 - dlo6);
+        diss = fmaf(g.ae * ih[7], dhi7 - dlo7, diss);
+        pc[i] += fmaf(0.5f, diss, total);
+      }
+    }
+    __syncthreads();  // every sum is complete; the padded block is free
+    const int next = o + gridDim.x;
+    if (next < a.outer) stage_block(next);
+    cp_async_commit();
+
+    // C: the update, a thread per cell, kCBatch cells at a time (their
+    // loads first)
+    const float *base_o = s.base ? s.base + j0 : nullptr;
+    for (int e0 = tid; e0 < inner; e0 += kCBatch * kColThreads) {
+      float fv[kCBatch], bv[kCBatch], tv[kCBatch];
+#pragma unroll
+      for (int h = 0; h < kCBatch; h++) {
+        const int c = min(e0 + h * kColThreads, inner - 1);
+        fv[h] = __ldg(src_o + c);
+        bv[h] = base_o ? __ldg(base_o + c) : fv[h];
+        tv[h] = part[c];
+      }
+#pragma unroll
+      for (int h = 0; h < kCBatch; h++) {
+        const int c = e0 + h * kColThreads;
+        if (c >= inner) break;
+        const int64_t j = j0 + c;
+        float value = fmaf(s.dt, tv[h], fv[h]);
+        if (base_o) value = 0.5f * (bv[h] + value);
+        if (g.order == 1 || base_o) {
+          const float previous = bv[h];  // the partner, or the stage input
+          const float tube = previous < value ? previous : value;
+          value = tube < avoid ? avoid : tube;
+          if (previous > 0.f && value <= 0.f && isnan(s.arrival[j]))
+            s.arrival[j] = (float)s.tau + s.dt * previous / (previous - value);
+          change_max = fmaxf(change_max, fabsf(value - previous));
+        }
+        bad |= !isfinite(value);
+        s.dst[j] = value;
+      }
+    }
+  }
+  cp_async_wait_all();
+
+  if (__syncthreads_or(bad) && tid == 0) atomicOr(&s.stats->nonfinite, 1u);
+  for (int off = 16; off > 0; off >>= 1)
+    change_max = fmaxf(change_max, __shfl_xor_sync(0xffffffffu, change_max, off));
+  if (lane == 0) warp_max[warp] = change_max;
+  __syncthreads();
+  if (tid == 0) {
+    float m = 0.f;
+    for (int w = 0; w < nwarps; w++) m = fmaxf(m, warp_max[w]);
+    if (m > 0.f)
+      atomicMax(&s.stats->residual, (unsigned long long)__double_as_longlong((double)m));
+  }
+}
+
+template <int ORDER, int NE, int SKIND>
+cudaError_t launch_column_kind(const ColW8Args &a, size_t smem, cudaStream_t stream) {
+  auto kernel = world8_column_kernel<ORDER, NE, SKIND>;
+  static size_t configured = 0;
+  static int resident = 0;
+  if (configured != smem || resident == 0) {
+    cudaError_t e =
+        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, kernel, kColThreads, smem);
+    if (e != cudaSuccess) return e;
+    if (resident < 1) return cudaErrorInvalidConfiguration;
+    configured = smem;
+  }
+  int device = 0, sms = 0;
+  cudaGetDevice(&device);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  const int blocks = a.outer < sms * resident ? a.outer : sms * resident;
+  kernel<<<blocks, kColThreads, smem, stream>>>(a);
+  return cudaGetLastError();
+}
+
+template <int ORDER, int NE>
+cudaError_t launch_column_ne(const ColW8Args &a, size_t smem, cudaStream_t stream) {
+  return a.g.linear_speed ? launch_column_kind<ORDER, NE, kInward>(a, smem, stream)
+                          : launch_column_kind<ORDER, NE, kExtrapolated>(a, smem, stream);
+}
+
+template <int ORDER>
+cudaError_t launch_column(const ColW8Args &a, size_t smem, cudaStream_t stream) {
+  switch (a.g.shape[7]) {
+    case 3: return launch_column_ne<ORDER, 3>(a, smem, stream);
+    case 4: return launch_column_ne<ORDER, 4>(a, smem, stream);
+    case 5: return launch_column_ne<ORDER, 5>(a, smem, stream);
+    case 6: return launch_column_ne<ORDER, 6>(a, smem, stream);
+    case 7: return launch_column_ne<ORDER, 7>(a, smem, stream);
+    default: return launch_column_ne<ORDER, 8>(a, smem, stream);
+  }
+}
 }  // namespace
 
 cudaError_t world8_stage_fast(const World8Grid &g, const World8Stage &s,
                               cudaStream_t stream) {
   const int64_t inner = (int64_t)g.shape[4] * g.shape[5] * g.shape[6] * g.shape[7];
+  // the column kernel: vE columns of 3 to 8 nodes, two CTAs per SM
+  if (g.shape[7] >= 3 && g.shape[7] <= 8 && column_smem_bytes(g) <= kMaxColumnBytes) {
+    ColW8Args c;
+    c.g = g;
+    c.s = s;
+    c.inner = (int)inner;
+    c.outer = (int)(g.cells / inner);
+    c.ncols = (int)(inner / g.shape[7]);
+    c.dnh = make_divisor(g.nh);
+    c.dn = make_divisor(g.n);
+    const size_t smem = column_smem_bytes(g);
+    return g.order == 1 ? launch_column<1>(c, smem, stream) : launch_column<2>(c, smem, stream);
+  }
   if (inner * 4 > kMaxBlockBytes) return w8::launch_stage<true>(g, s, stream);
   FastW8Args a;
   a.g = g;
