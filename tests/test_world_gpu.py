@@ -200,6 +200,8 @@ def _contact_run(grid, steps, fast, order=2, boundary="linear", avoid=False):
     (WorldGrid(7, 6, 4, 3, 3.0), 20, 1, "linear", False),
     (WorldGrid(7, 4, 3, 3, 4.0), 20, 1, "legacy_signed", True),
     (WorldGrid(9, 6, 5, 4, 4.0), 10, 2, "legacy_signed", True),
+    # 9 evader speeds: beyond the column kernel's 3-8, the block kernel
+    (WorldGrid(7, 4, 3, 9, 3.0), 10, 2, "linear", False),
 ])
 def test_fast_world_step_tracks_the_exact_step(grid, steps, order, boundary, avoid):
     """The fast stage (evader blocks staged in shared memory, reciprocal
