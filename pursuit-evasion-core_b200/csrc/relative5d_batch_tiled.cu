@@ -5,13 +5,13 @@
 //
 // A work item is `rows` y rows of one (vP, vE) plane stack of one solve, all
 // headings.  A thread owns a 4-cell x chunk of one row and walks the
-// headings with a 5-heading register window (the psi stencil).  For each
-// heading the CTA stages, double-buffered against the previous heading's
+// headings, carrying the heading differences and ENO selections from one
+// heading to the next (the psi stencil).  For each heading the CTA stages, double-buffered against the previous heading's
 // arithmetic, the item's own plane rows with a 2-row y halo and the rows of
-// the 8 speed-neighbour planes (vE +-1, +-2, vP +-1, +-2): thread 0 issues
-// one bulk copy (cp.async.bulk, the TMA engine) per contiguous row range,
-// nine at most, all completing on the buffer's mbarrier, on which every
-// thread waits (bounded); the x, y and speed stencils then read shared
+// the 8 speed-neighbour planes (vE +-1, +-2, vP +-1, +-2): lanes 0-8 of
+// warp 0 issue one bulk copy (cp.async.bulk, the TMA engine) each, one per
+// contiguous row range, all completing on the buffer's mbarrier, on which
+// every thread waits (bounded); the x, y and speed stencils then read shared
 // memory.  The persistent loop over steps, the active-item prefix and the
 // bounded grid barrier are those of relative5d_batch_impl.cuh.
 #include "bulk_copy.cuh"
@@ -102,9 +102,10 @@ __device__ __forceinline__ void stage_heading(const Rel5Grid &g, const float *__
 // One stage of one item (all headings).  Returns the largest |change| of
 // this thread's cells (stage 2) and flags non-finite values.
 template <int ORDER, int BLEND>
-__device__ __forceinline__ void item_stage(const Rel5Grid &g, const Rel5Stage &s, const ItemGeom &it,
-                           float *smem, StageRing &ring, float &change_max, float &change_up,
-                           float2 &finite_acc) {
+__device__ __forceinline__ void item_stage(const Rel5Grid &g, const Rel5Stage &s,
+                                           const ItemGeom &it, float *smem, StageRing &ring,
+                                           float &change_max, float &change_up,
+                                           float2 &finite_acc) {
   const int xp = g.xp, xc = it.xc;
   const int64_t PP = (int64_t)g.nx * xp;
   const int tid = threadIdx.x;
@@ -130,28 +131,58 @@ __device__ __forceinline__ void item_stage(const Rel5Grid &g, const Rel5Stage &s
   float xs[4];
 #pragma unroll
   for (int i = 0; i < 4; i++) xs[i] = fmaf((float)(x0 + i), dxf, -ext);
-  const float2 negx_a = make_float2(-xs[0], -xs[1]), negx_b = make_float2(-xs[2], -xs[3]);
-  const float2 absx_a = make_float2(fabsf(xs[0]), fabsf(xs[1]));
-  const float2 absx_b = make_float2(fabsf(xs[2]), fabsf(xs[3]));
-  const float hx = 0.5f * ihx, hp = 0.5f * ihp, hv = 0.5f * ihv, he = 0.5f * ihe;
+  // half reciprocal spacings: a centred gradient is (lo + hi) * h?s, so each
+  // axis enters the update through the sum S = lo + hi and the jump
+  // J = hi - lo of its slopes (the single-grid float32 kernel's arithmetic)
+  const float hxs = 0.5f * ihx, hps = 0.5f * ihp, hvs = 0.5f * ihv, hes = 0.5f * ihe;
+  const float2 nxs[2] = {make_float2(-xs[0] * hxs, -xs[1] * hxs),
+                         make_float2(-xs[2] * hxs, -xs[3] * hxs)};
+  const float2 day0[2] = {make_float2(wp * hxs * fabsf(xs[0]), wp * hxs * fabsf(xs[1])),
+                          make_float2(wp * hxs * fabsf(xs[2]), wp * hxs * fabsf(xs[3]))};
   const float dt = (float)s.dt;
   const float y = fmaf((float)iy, dxf, -ext);
-  const float ap_coef = (wp + we) * ihp, av_coef = ap * ihv, ae_coef = ae * ihe;
-  const float2 ay_a = __fmul2_rn(__fmul2_rn(f2(wp), absx_a), f2(ihx));
-  const float2 ay_b = __fmul2_rn(__fmul2_rn(f2(wp), absx_b), f2(ihx));
-  const float wy = wp * fabsf(y) * ihx;
+  const float ys = y * hxs;
+  const float wes = we * hps;                       // * |S_psi|
+  const float kv_in = -ap * hvs, ke_in = ae * hes;  // * |S_v|, |S_e| (inner)
+  const float dap = (wp + we) * hps, dav = ap * hvs, dae = ae * hes;
+  const float dax0 = wp * fabsf(y) * hxs;  // + |bx| * hxs per heading
   const int64_t stack = ((int64_t)it.iv * g.nve + it.ie) * g.nh * PP;
   const int64_t cell0 = stack + (int64_t)iy * xp + x0;  // heading 0
   const int nh = g.nh;
   auto wrap = [nh](int q) { return q < 0 ? q + nh : (q >= nh ? q - nh : q); };
-  auto load_window = [&](int q) {
+  auto load_plane = [&](int q) {
     return active ? *reinterpret_cast<const float4 *>(s.src + cell0 + (int64_t)wrap(q) * PP)
                   : make_float4(0.f, 0.f, 0.f, 0.f);
   };
 
-  float4 win[5];
+  // The heading axis is walked: its differences and ENO selection are
+  // carried from one heading to the next, per pair of cells.  VN = V(k+1),
+  // ER = V(k+1) - V(k), D2 = second difference at k, LO = low slope at k;
+  // C = V(k), VNEW = V(k+2), `next` = V(k+3) (one heading ahead, from L2).
+  float2 VN[2], ER[2], D2[2], LO[2];
+  float4 C, VNEW;
+  {
+    const float4 vm2 = load_plane(-2), vm1 = load_plane(-1), v0 = load_plane(0);
+    const float4 vp1 = load_plane(1);
+    VNEW = load_plane(2);
+    C = v0;
 #pragma unroll
-  for (int d = 0; d < 5; d++) win[d] = load_window(d - 2);
+    for (int h = 0; h < 2; h++) {
+      const float2 a_m2 = h ? hi2(vm2) : lo2(vm2), a_m1 = h ? hi2(vm1) : lo2(vm1);
+      const float2 a_0 = h ? hi2(v0) : lo2(v0), a_p1 = h ? hi2(vp1) : lo2(vp1);
+      const float2 el = sub2(a_0, a_m1);
+      ER[h] = sub2(a_p1, a_0);
+      VN[h] = a_p1;
+      if (ORDER == 1) {
+        LO[h] = el;
+        D2[h] = f2(0.f);
+      } else {
+        const float2 dm = sub2(el, sub2(a_m1, a_m2));
+        D2[h] = sub2(ER[h], el);
+        LO[h] = __ffma2_rn(f2(0.5f), pick2(dm, D2[h]), el);
+      }
+    }
+  }
 
   if (tid < 32) stage_heading(g, s.src, it, 0, smem, &stage_bar[0]);
   ring.filled(0);
@@ -164,115 +195,153 @@ __device__ __forceinline__ void item_stage(const Rel5Grid &g, const Rel5Stage &s
         stage_heading(g, s.src, it, k + 1, smem + (b ^ 1) * bufsz, &stage_bar[b ^ 1]);
       ring.filled(b ^ 1);
     }
-    const float4 next = k + 1 < nh ? load_window(k + 3) : make_float4(0.f, 0.f, 0.f, 0.f);
-    const float *own = smem + (k & 1) * bufsz;
+    const float4 next = k + 1 < nh ? load_plane(k + 3) : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float *own = smem + b * bufsz;
     if (active) {
       const float *o0 = own + (r + 2) * xp + x0;
       const float *nb = own + (it.R + 4) * xp + r * xp + x0;
-      const float4 C = win[2];
-      const float2 v_a = lo2(C), v_b = hi2(C);
-      const float2 xl = *reinterpret_cast<const float2 *>(o0 - 2);
-      const float2 xr = *reinterpret_cast<const float2 *>(o0 + 4);
-      // rows are padded: x0 - 2 < 0 and x0 + 5 >= xp only read the row's
-      // neighbours in the buffer, which the end rules of slopes_x ignore
-      const float w[8] = {xl.x, xl.y, C.x, C.y, C.z, C.w, xr.x, xr.y};
-      float xlo[4], xhi[4];
-      slopes_x<ORDER, true>(w, x0, g.nx, xlo, xhi);
-      const float2 lx_a = make_float2(xlo[0], xlo[1]), lx_b = make_float2(xlo[2], xlo[3]);
-      const float2 hx_a = make_float2(xhi[0], xhi[1]), hx_b = make_float2(xhi[2], xhi[3]);
-      float2 ly_a, ly_b, hy_a, hy_b;
-      {
+      const float bx = fmaf(ve, (float)s.cs[k], -vp), by = ve * (float)s.sn[k];
+      const float cx = bx * hxs, cy = by * hxs;
+      const float dax = fmaf(fabsf(bx), hxs, dax0);
+      const float aby = fabsf(by) * hxs;
+      // A: linear terms and x/y dissipation, D: heading and speed
+      // dissipation, T = y gx - x gy - gp, Hs: absolute-value and speed terms
+      float2 A[2], D[2], T[2];
+      float Hs[2][2];
+      {  // x: window x0-2 .. x0+5 of the padded row
+        const float2 xl = *reinterpret_cast<const float2 *>(o0 - 2);
+        const float2 xr = *reinterpret_cast<const float2 *>(o0 + 4);
+        // rows are padded: x0 - 2 < 0 and x0 + 5 >= xp only read the row's
+        // neighbours in the buffer, which the end rules of slopes_x ignore
+        const float w[8] = {xl.x, xl.y, C.x, C.y, C.z, C.w, xr.x, xr.y};
+        float xlo[4], xhi[4];
+        slopes_x<ORDER, true>(w, x0, g.nx, xlo, xhi);
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          const float2 lo = make_float2(xlo[2 * h], xlo[2 * h + 1]);
+          const float2 hi = make_float2(xhi[2 * h], xhi[2 * h + 1]);
+          const float2 S = add2(lo, hi), J = sub2(hi, lo);
+          A[h] = __ffma2_rn(f2(dax), J, __fmul2_rn(f2(cx), S));
+          T[h] = __fmul2_rn(f2(ys), S);
+        }
+      }
+      {  // y: rows iy-2 .. iy+2 of heading k
         const float4 m2 = *reinterpret_cast<const float4 *>(o0 - 2 * xp);
         const float4 m1 = *reinterpret_cast<const float4 *>(o0 - xp);
         const float4 p1 = *reinterpret_cast<const float4 *>(o0 + xp);
         const float4 p2 = *reinterpret_cast<const float4 *>(o0 + 2 * xp);
-        if (y_edge) {
-          slope_pair<ORDER, true>(lo2(m2), lo2(m1), v_a, lo2(p1), lo2(p2), iy, g.nx, ly_a, hy_a);
-          slope_pair<ORDER, true>(hi2(m2), hi2(m1), v_b, hi2(p1), hi2(p2), iy, g.nx, ly_b, hy_b);
-        } else {
-          slope_pair<ORDER, false>(lo2(m2), lo2(m1), v_a, lo2(p1), lo2(p2), iy, g.nx, ly_a, hy_a);
-          slope_pair<ORDER, false>(hi2(m2), hi2(m1), v_b, hi2(p1), hi2(p2), iy, g.nx, ly_b, hy_b);
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          float2 lo, hi;
+          const float2 c2 = h ? hi2(C) : lo2(C);
+          if (y_edge)
+            slope_pair<ORDER, true>(h ? hi2(m2) : lo2(m2), h ? hi2(m1) : lo2(m1), c2,
+                                    h ? hi2(p1) : lo2(p1), h ? hi2(p2) : lo2(p2), iy, g.nx,
+                                    lo, hi);
+          else
+            slope_pair<ORDER, false>(h ? hi2(m2) : lo2(m2), h ? hi2(m1) : lo2(m1), c2,
+                                     h ? hi2(p1) : lo2(p1), h ? hi2(p2) : lo2(p2), iy, g.nx,
+                                     lo, hi);
+          const float2 S = add2(lo, hi), J = sub2(hi, lo);
+          const float2 day = __fadd2_rn(day0[h], f2(aby));
+          A[h] = __ffma2_rn(f2(cy), S, A[h]);
+          A[h] = __ffma2_rn(day, J, A[h]);
+          T[h] = __ffma2_rn(nxs[h], S, T[h]);
         }
       }
-      float2 lp_a, lp_b, hp_a, hp_b;
-      slope_pair<ORDER, false>(lo2(win[0]), lo2(win[1]), v_a, lo2(win[3]), lo2(win[4]), 2, 5,
-                               lp_a, hp_a);
-      slope_pair<ORDER, false>(hi2(win[0]), hi2(win[1]), v_b, hi2(win[3]), hi2(win[4]), 2, 5,
-                               lp_b, hp_b);
+      // psi: extend the carried differences with heading k+2
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const float2 vnew = h ? hi2(VNEW) : lo2(VNEW);
+        const float2 en = sub2(vnew, VN[h]);  // V(k+2) - V(k+1)
+        float2 hi, lo_next;
+        if (ORDER == 1) {
+          hi = ER[h];
+          lo_next = ER[h];
+        } else {
+          const float2 d2n = sub2(en, ER[h]);
+          const float2 pr = pick2(D2[h], d2n);
+          hi = __ffma2_rn(f2(-0.5f), pr, ER[h]);
+          lo_next = __ffma2_rn(f2(0.5f), pr, ER[h]);
+          D2[h] = d2n;
+        }
+        const float2 S = add2(LO[h], hi), J = sub2(hi, LO[h]);
+        LO[h] = lo_next;
+        ER[h] = en;
+        T[h] = __ffma2_rn(f2(-hps), S, T[h]);
+        D[h] = __fmul2_rn(f2(dap), J);
+        Hs[h][0] = wes * fabsf(S.x);
+        Hs[h][1] = wes * fabsf(S.y);
+      }
       const int nbf = it.R * xp;
-      float2 le_a, le_b, he_a, he_b, lv_a, lv_b, hv_a, hv_b;
-      {
+      {  // vE: neighbour planes 0-3
         const float4 m2 = *reinterpret_cast<const float4 *>(nb + 0 * nbf);
         const float4 m1 = *reinterpret_cast<const float4 *>(nb + 1 * nbf);
         const float4 p1 = *reinterpret_cast<const float4 *>(nb + 2 * nbf);
         const float4 p2 = *reinterpret_cast<const float4 *>(nb + 3 * nbf);
-        if (e_slope_inner) {
-          slope_pair<ORDER, false>(lo2(m2), lo2(m1), v_a, lo2(p1), lo2(p2), it.ie, g.nve, le_a, he_a);
-          slope_pair<ORDER, false>(hi2(m2), hi2(m1), v_b, hi2(p1), hi2(p2), it.ie, g.nve, le_b, he_b);
-        } else {
-          slope_pair<ORDER, true>(lo2(m2), lo2(m1), v_a, lo2(p1), lo2(p2), it.ie, g.nve, le_a, he_a);
-          slope_pair<ORDER, true>(hi2(m2), hi2(m1), v_b, hi2(p1), hi2(p2), it.ie, g.nve, le_b, he_b);
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          float2 lo, hi;
+          const float2 c2 = h ? hi2(C) : lo2(C);
+          if (e_slope_inner)
+            slope_pair<ORDER, false>(h ? hi2(m2) : lo2(m2), h ? hi2(m1) : lo2(m1), c2,
+                                     h ? hi2(p1) : lo2(p1), h ? hi2(p2) : lo2(p2), it.ie,
+                                     g.nve, lo, hi);
+          else
+            slope_pair<ORDER, true>(h ? hi2(m2) : lo2(m2), h ? hi2(m1) : lo2(m1), c2,
+                                    h ? hi2(p1) : lo2(p1), h ? hi2(p2) : lo2(p2), it.ie,
+                                    g.nve, lo, hi);
+          const float2 S = add2(lo, hi), J = sub2(hi, lo);
+          D[h] = __ffma2_rn(f2(dae), J, D[h]);
+          if (e_inner) {
+            Hs[h][0] = fmaf(ke_in, fabsf(S.x), Hs[h][0]);
+            Hs[h][1] = fmaf(ke_in, fabsf(S.y), Hs[h][1]);
+          } else {  // max(elo*ge, ehi*ge), ge = S * hes
+            const float2 ge = __fmul2_rn(f2(hes), S);
+            Hs[h][0] += fmaxf(elo * ge.x, ehi * ge.x);
+            Hs[h][1] += fmaxf(elo * ge.y, ehi * ge.y);
+          }
         }
       }
-      {
+      {  // vP: neighbour planes 4-7
         const float4 m2 = *reinterpret_cast<const float4 *>(nb + 4 * nbf);
         const float4 m1 = *reinterpret_cast<const float4 *>(nb + 5 * nbf);
         const float4 p1 = *reinterpret_cast<const float4 *>(nb + 6 * nbf);
         const float4 p2 = *reinterpret_cast<const float4 *>(nb + 7 * nbf);
-        if (v_slope_inner) {
-          slope_pair<ORDER, false>(lo2(m2), lo2(m1), v_a, lo2(p1), lo2(p2), it.iv, g.nvp, lv_a, hv_a);
-          slope_pair<ORDER, false>(hi2(m2), hi2(m1), v_b, hi2(p1), hi2(p2), it.iv, g.nvp, lv_b, hv_b);
-        } else {
-          slope_pair<ORDER, true>(lo2(m2), lo2(m1), v_a, lo2(p1), lo2(p2), it.iv, g.nvp, lv_a, hv_a);
-          slope_pair<ORDER, true>(hi2(m2), hi2(m1), v_b, hi2(p1), hi2(p2), it.iv, g.nvp, lv_b, hv_b);
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          float2 lo, hi;
+          const float2 c2 = h ? hi2(C) : lo2(C);
+          if (v_slope_inner)
+            slope_pair<ORDER, false>(h ? hi2(m2) : lo2(m2), h ? hi2(m1) : lo2(m1), c2,
+                                     h ? hi2(p1) : lo2(p1), h ? hi2(p2) : lo2(p2), it.iv,
+                                     g.nvp, lo, hi);
+          else
+            slope_pair<ORDER, true>(h ? hi2(m2) : lo2(m2), h ? hi2(m1) : lo2(m1), c2,
+                                    h ? hi2(p1) : lo2(p1), h ? hi2(p2) : lo2(p2), it.iv,
+                                    g.nvp, lo, hi);
+          const float2 S = add2(lo, hi), J = sub2(hi, lo);
+          D[h] = __ffma2_rn(f2(dav), J, D[h]);
+          if (p_inner) {
+            Hs[h][0] = fmaf(kv_in, fabsf(S.x), Hs[h][0]);
+            Hs[h][1] = fmaf(kv_in, fabsf(S.y), Hs[h][1]);
+          } else {  // min(plo*gv, phi*gv), gv = S * hvs
+            const float2 gv = __fmul2_rn(f2(hvs), S);
+            Hs[h][0] += fminf(plo * gv.x, phi * gv.x);
+            Hs[h][1] += fminf(plo * gv.y, phi * gv.y);
+          }
         }
       }
-      // Hamiltonian + dissipation (native_relative.cpp:144-157)
-      const float bx = fmaf(ve, (float)s.cs[k], -vp);
-      const float by = ve * (float)s.sn[k];
-      const float2 bx2 = f2(bx), by2 = f2(by);
-      const float ax_coef = fmaf(fabsf(bx), ihx, wy);
-      const float aby = fabsf(by) * ihx;
       const int64_t cell = cell0 + (int64_t)k * PP;
       const float4 prev4 = BLEND ? *reinterpret_cast<const float4 *>(s.dst + cell) : C;
       float2 out[2];
 #pragma unroll
       for (int h = 0; h < 2; h++) {
-        const float2 lx = h ? lx_b : lx_a, hxv = h ? hx_b : hx_a;
-        const float2 ly = h ? ly_b : ly_a, hy = h ? hy_b : hy_a;
-        const float2 lp = h ? lp_b : lp_a, hpv = h ? hp_b : hp_a;
-        const float2 lv = h ? lv_b : lv_a, hvv = h ? hv_b : hv_a;
-        const float2 le = h ? le_b : le_a, hev = h ? he_b : he_a;
-        const float2 v = h ? v_b : v_a;
-        const float2 negx = h ? negx_b : negx_a;
-        const float2 ay = __fadd2_rn(h ? ay_b : ay_a, f2(aby));
-        const float2 gx = __fmul2_rn(__fadd2_rn(lx, hxv), f2(hx));
-        const float2 gy = __fmul2_rn(__fadd2_rn(ly, hy), f2(hx));
-        const float2 gpn = __fmul2_rn(__fadd2_rn(lp, hpv), f2(-hp));  // -gp
-        const float2 gv = __fmul2_rn(__fadd2_rn(lv, hvv), f2(hv));
-        const float2 ge = __fmul2_rn(__fadd2_rn(le, hev), f2(he));
-        float2 H = __ffma2_rn(by2, gy, __fmul2_rn(bx2, gx));
-        float2 t = __ffma2_rn(f2(y), gx, gpn);
-        t = __ffma2_rn(negx, gy, t);
-        float hs[2] = {H.x, H.y};
-        const float ts[2] = {t.x, t.y}, gps[2] = {gpn.x, gpn.y};
-        const float gvs[2] = {gv.x, gv.y}, ges[2] = {ge.x, ge.y};
-#pragma unroll
-        for (int l = 0; l < 2; l++) {
-          hs[l] = fmaf(-wp, fabsf(ts[l]), hs[l]);
-          hs[l] = fmaf(we, fabsf(gps[l]), hs[l]);
-          hs[l] = p_inner ? fmaf(-ap, fabsf(gvs[l]), hs[l])
-                          : hs[l] + fminf(plo * gvs[l], phi * gvs[l]);
-          hs[l] = e_inner ? fmaf(ae, fabsf(ges[l]), hs[l])
-                          : hs[l] + fmaxf(elo * ges[l], ehi * ges[l]);
-        }
-        H = make_float2(hs[0], hs[1]);
-        float2 diss = __fmul2_rn(f2(ax_coef), sub2(hxv, lx));
-        diss = __ffma2_rn(ay, sub2(hy, ly), diss);
-        diss = __ffma2_rn(f2(ap_coef), sub2(hpv, lp), diss);
-        diss = __ffma2_rn(f2(av_coef), sub2(hvv, lv), diss);
-        diss = __ffma2_rn(f2(ae_coef), sub2(hev, le), diss);
-        H = __ffma2_rn(f2(0.5f), diss, H);
+        const float2 v = h ? hi2(C) : lo2(C);
+        // H = A + D + Hs - wp * |T|
+        const float2 Hs2 = make_float2(fmaf(-wp, fabsf(T[h].x), Hs[h][0]),
+                                       fmaf(-wp, fabsf(T[h].y), Hs[h][1]));
+        const float2 H = __fadd2_rn(__fadd2_rn(A[h], D[h]), Hs2);
         float2 value = __ffma2_rn(f2(dt), make_float2(fminf(H.x, 0.f), fminf(H.y, 0.f)), v);
         const float2 prev = BLEND ? (h ? hi2(prev4) : lo2(prev4)) : v;
         if (BLEND) value = __fmul2_rn(f2(0.5f), __fadd2_rn(prev, value));
@@ -302,9 +371,11 @@ __device__ __forceinline__ void item_stage(const Rel5Grid &g, const Rel5Stage &s
       *reinterpret_cast<float4 *>(s.dst + cell) =
           make_float4(out[0].x, out[0].y, out[1].x, out[1].y);
     }
+    // advance the heading window: the next centre is V(k+1), carried in VN
+    C = make_float4(VN[0].x, VN[0].y, VN[1].x, VN[1].y);
 #pragma unroll
-    for (int d = 0; d < 4; d++) win[d] = win[d + 1];
-    win[4] = next;
+    for (int h = 0; h < 2; h++) VN[h] = h ? hi2(VNEW) : lo2(VNEW);
+    VNEW = next;
   }
   __syncthreads();  // the buffers are restaged by the next item
 }
