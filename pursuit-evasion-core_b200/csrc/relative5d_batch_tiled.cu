@@ -6,12 +6,13 @@
 // A work item is `rows` y rows of one (vP, vE) plane stack of one solve, all
 // headings.  A thread owns a 4-cell x chunk of one row and walks the
 // headings, carrying the heading differences and ENO selections from one
-// heading to the next (the psi stencil).  For each heading the CTA stages, double-buffered against the previous heading's
-// arithmetic, the item's own plane rows with a 2-row y halo and the rows of
-// the 8 speed-neighbour planes (vE +-1, +-2, vP +-1, +-2): lanes 0-8 of
-// warp 0 issue one bulk copy (cp.async.bulk, the TMA engine) each, one per
-// contiguous row range, all completing on the buffer's mbarrier, on which
-// every thread waits (bounded); the x, y and speed stencils then read shared
+// heading to the next (the psi stencil).  For each heading the CTA stages,
+// double-buffered against the previous heading's arithmetic, the item's own
+// plane rows with a 2-row y halo and the rows of the 8 speed-neighbour
+// planes (vE +-1, +-2, vP +-1, +-2): lanes 0-8 of warp 0 issue one bulk
+// copy (cp.async.bulk, the TMA engine) each, one per contiguous row range,
+// all completing on the buffer's mbarrier, on which every thread waits
+// (bounded); the x, y and speed stencils then read shared
 // memory.  The persistent loop over steps, the active-item prefix and the
 // bounded grid barrier are those of relative5d_batch_impl.cuh.
 #include "bulk_copy.cuh"
