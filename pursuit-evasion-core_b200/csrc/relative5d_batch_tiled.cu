@@ -466,8 +466,12 @@ __global__ void __launch_bounds__(kThreads, 2)
       if (step < A.solves[k].nsteps) A.solves[k].stats->residual = 0ull;
     tiled_stage<0>(A, step, n_items, scratch, &sg, smem, ring);
     if (!batch_impl::grid_barrier(A.sync, ++round)) break;
+    // the next stage's bulk copies read what other CTAs stored before the
+    // barrier: order it for the async proxy (warp 0 issues the copies)
+    if (threadIdx.x < 32) bulk::fence_async_global();
     tiled_stage<1>(A, step, n_items, scratch, &sg, smem, ring);
     if (!batch_impl::grid_barrier(A.sync, ++round)) break;
+    if (threadIdx.x < 32) bulk::fence_async_global();
   }
   // no bulk copy may still be landing when the CTA exits (complete already
   // unless a wait gave up)
