@@ -21,10 +21,15 @@
 // of world8d_stage.cuh.
 #include <cstdio>
 
+#include "relative5d_eno_f32.cuh"
 #include "world8d_stage.cuh"
 
 namespace pe {
 namespace {
+
+using eno32::add2;
+using eno32::f2;
+using eno32::sub2;
 
 constexpr int kThreads = 256;
 constexpr int kMaxBlockBytes = 96 * 1024;  // per buffer; two buffers per CTA
@@ -107,6 +112,52 @@ __device__ __forceinline__ void axis_slopes(float m2, float m1, float f, float p
   if (kind == kInward) {
     if (p == 0) dlo = dhi = p1 - f;
     if (p == n - 1) dlo = dhi = f - m1;
+  }
+}
+
+// The same slopes for two independent cells at the same position p of the
+// axis, in packed FP32 (__ffma2_rn / __fadd2_rn round each element as the
+// scalar operation does); the ENO selections and the end-node ghosts are
+// taken element by element.
+template <int ORDER>
+__device__ __forceinline__ void axis_slopes2(float2 m2, float2 m1, float2 f, float2 p1,
+                                             float2 p2, int p, int n, int kind, float2 &dlo,
+                                             float2 &dhi) {
+  if (kind == kExtrapolated && (p < 2 || p + 2 >= n)) {
+    if (p == 0) {
+      m1 = make_float2(ghost_value(f.x, p1.x, 1.f), ghost_value(f.y, p1.y, 1.f));
+      m2 = make_float2(ghost_value(f.x, p1.x, 2.f), ghost_value(f.y, p1.y, 2.f));
+    } else if (p == 1) {
+      m2 = make_float2(ghost_value(m1.x, f.x, 1.f), ghost_value(m1.y, f.y, 1.f));
+    }
+    if (p == n - 1) {
+      p1 = make_float2(ghost_value(f.x, m1.x, 1.f), ghost_value(f.y, m1.y, 1.f));
+      p2 = make_float2(ghost_value(f.x, m1.x, 2.f), ghost_value(f.y, m1.y, 2.f));
+    } else if (p == n - 2) {
+      p2 = make_float2(ghost_value(p1.x, f.x, 1.f), ghost_value(p1.y, f.y, 1.f));
+    }
+  }
+  dlo = sub2(f, m1);
+  dhi = sub2(p1, f);
+  if (ORDER == 2) {
+    // (fp - 2f) + fm with 2f exact, as the scalar form
+    const float2 c = add2(__ffma2_rn(f, f2(-2.f), p1), m1);
+    float2 l = add2(__ffma2_rn(m1, f2(-2.f), f), m2);
+    float2 r = add2(__ffma2_rn(p1, f2(-2.f), p2), f);
+    if (kind == kInward) {
+      if (p < 2) l = c;
+      if (p + 2 >= n) r = c;
+    }
+    const float2 el = make_float2(fabsf(l.x) <= fabsf(c.x) ? l.x : c.x,
+                                  fabsf(l.y) <= fabsf(c.y) ? l.y : c.y);
+    const float2 er = make_float2(fabsf(c.x) <= fabsf(r.x) ? c.x : r.x,
+                                  fabsf(c.y) <= fabsf(r.y) ? c.y : r.y);
+    dlo = __ffma2_rn(f2(0.5f), el, dlo);
+    dhi = __ffma2_rn(f2(-0.5f), er, dhi);
+  }
+  if (kind == kInward) {
+    if (p == 0) dlo = dhi = sub2(p1, f);
+    if (p == n - 1) dlo = dhi = sub2(f, m1);
   }
 }
 
@@ -480,32 +531,33 @@ __global__ void __launch_bounds__(kColThreads, 2)
           for (int m = 0; m < 4; m++) buf[h][4 * k + m] = __ldg(src_o + poff[k][m] + c);
       }
     };
+    // the two cells of a group in one packed pair (.x: e, .y: e + 256; the
+    // second may lie past the block, computed from a clamped load and not
+    // stored)
     auto pursuer_cells = [&](int e, const float (&buf)[2][17]) {
-#pragma unroll
-      for (int h = 0; h < 2; h++) {
-        const int c = e + h * kColThreads;
-        if (c >= inner) break;
-        const float *v = buf[h];
-        const float f = v[16];
-        float dlo[4], dhi[4];
-        axis_slopes<ORDER>(v[0], v[1], f, v[2], v[3], qp[0], g.shape[0], kExtrapolated,
-                           dlo[0], dhi[0]);
-        axis_slopes<ORDER>(v[4], v[5], f, v[6], v[7], qp[1], g.shape[1], kExtrapolated,
-                           dlo[1], dhi[1]);
-        axis_slopes<ORDER>(v[8], v[9], f, v[10], v[11], qp[2], g.shape[2], kPeriodic, dlo[2],
-                           dhi[2]);
-        axis_slopes<ORDER>(v[12], v[13], f, v[14], v[15], qp[3], g.shape[3], SKIND, dlo[3],
-                           dhi[3]);
-        float total = fmaf(wx_lo, dlo[0], wx_hi * dhi[0]);
-        total = fmaf(wy_lo, dlo[1], fmaf(wy_hi, dhi[1], total));
-        const float g2 = 0.5f * ih[2] * (dlo[2] + dhi[2]);
-        total = fmaf(-wp, fabsf(g2), total);
-        const float g3 = 0.5f * ih[3] * (dlo[3] + dhi[3]);
-        total += fminf(palo * g3, pahi * g3);
-        float diss = wp * ih[2] * (dhi[2] - dlo[2]);
-        diss = fmaf(g.ap * ih[3], dhi[3] - dlo[3], diss);
-        part[c] = fmaf(0.5f, diss, total);
-      }
+      auto at = [&](int i) { return make_float2(buf[0][i], buf[1][i]); };
+      const float2 f = at(16);
+      float2 dlo[4], dhi[4];
+      axis_slopes2<ORDER>(at(0), at(1), f, at(2), at(3), qp[0], g.shape[0], kExtrapolated,
+                          dlo[0], dhi[0]);
+      axis_slopes2<ORDER>(at(4), at(5), f, at(6), at(7), qp[1], g.shape[1], kExtrapolated,
+                          dlo[1], dhi[1]);
+      axis_slopes2<ORDER>(at(8), at(9), f, at(10), at(11), qp[2], g.shape[2], kPeriodic,
+                          dlo[2], dhi[2]);
+      axis_slopes2<ORDER>(at(12), at(13), f, at(14), at(15), qp[3], g.shape[3], SKIND,
+                          dlo[3], dhi[3]);
+      float2 total = __ffma2_rn(f2(wx_lo), dlo[0], __fmul2_rn(f2(wx_hi), dhi[0]));
+      total = __ffma2_rn(f2(wy_lo), dlo[1], __ffma2_rn(f2(wy_hi), dhi[1], total));
+      const float2 g2 = __fmul2_rn(f2(0.5f * ih[2]), add2(dlo[2], dhi[2]));
+      total = __ffma2_rn(f2(-wp), make_float2(fabsf(g2.x), fabsf(g2.y)), total);
+      const float2 g3 = __fmul2_rn(f2(0.5f * ih[3]), add2(dlo[3], dhi[3]));
+      total = add2(total, make_float2(fminf(palo * g3.x, pahi * g3.x),
+                                      fminf(palo * g3.y, pahi * g3.y)));
+      float2 diss = __fmul2_rn(f2(wp * ih[2]), sub2(dhi[2], dlo[2]));
+      diss = __ffma2_rn(f2(g.ap * ih[3]), sub2(dhi[3], dlo[3]), diss);
+      const float2 out = __ffma2_rn(f2(0.5f), diss, total);
+      part[e] = out.x;
+      if (e + kColThreads < inner) part[e + kColThreads] = out.y;
     };
     {
       constexpr int step = 2 * kColThreads;
