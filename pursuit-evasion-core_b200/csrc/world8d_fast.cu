@@ -589,8 +589,16 @@ __global__ void __launch_bounds__(kColThreads, 2)
 #pragma unroll
       for (int i = 0; i < NE; i++) vc[i] = col[i];
       float *pc = part + c * NE;
-#pragma unroll
-      for (int i = 0; i < NE; i++) {
+      // the clamped vE window of cell i: nodes i-2, i-1, i+1, i+2 (compile
+      // time once unrolled)
+      auto vw = [&](int i, int d) {
+        return d == -2 ? vc[i > 1 ? i - 2 : (i > 0 ? i - 1 : i)]
+             : d == -1 ? vc[i > 0 ? i - 1 : i]
+             : d == 1  ? vc[i < NE - 1 ? i + 1 : i]
+                       : vc[i < NE - 2 ? i + 2 : (i < NE - 1 ? i + 1 : i)];
+      };
+      // cell i alone
+      auto evader_one = [&](int i) {
         const float f = vc[i];
         float dlo4, dhi4, dlo5, dhi5, dlo6, dhi6, dlo7, dhi7;
         // xE and yE: ghosts are in the padded block, every position is interior
@@ -600,11 +608,9 @@ __global__ void __launch_bounds__(kColThreads, 2)
                            kPeriodic, dlo5, dhi5);
         axis_slopes<ORDER>(col[i + om2], col[i + om1], f, col[i + op1], col[i + op2], 2, 5,
                            kPeriodic, dlo6, dhi6);
-        // vE: the column's registers, clamped window, compile-time end rules
-        axis_slopes<ORDER>(vc[i > 1 ? i - 2 : (i > 0 ? i - 1 : i)], vc[i > 0 ? i - 1 : i], f,
-                           vc[i < NE - 1 ? i + 1 : i],
-                           vc[i < NE - 2 ? i + 2 : (i < NE - 1 ? i + 1 : i)], i, NE, SKIND,
-                           dlo7, dhi7);
+        // vE: the column's registers, compile-time end rules
+        axis_slopes<ORDER>(vw(i, -2), vw(i, -1), f, vw(i, 1), vw(i, 2), i, NE, SKIND, dlo7,
+                           dhi7);
         const float ve = __ldg(s.ev + i);
         const float fex = ve * cs6, fey = ve * sn6;
         const float we = fabsf(ve) * g.ke;
@@ -619,7 +625,49 @@ __global__ void __launch_bounds__(kColThreads, 2)
         float diss = we * ih[6] * (dhi6 - dlo6);
         diss = fmaf(g.ae * ih[7], dhi7 - dlo7, diss);
         pc[i] += fmaf(0.5f, diss, total);
-      }
+      };
+      // cells i and i+1 as one packed FP32 pair (vE slopes element by
+      // element, for their compile-time end rules)
+      auto evader_pair = [&](int i) {
+        auto at = [&](int off) { return make_float2(col[i + off], col[i + 1 + off]); };
+        const float2 f = make_float2(vc[i], vc[i + 1]);
+        float2 dlo4, dhi4, dlo5, dhi5, dlo6, dhi6;
+        axis_slopes2<ORDER>(at(-2 * sx), at(-sx), f, at(sx), at(2 * sx), 2, 5, kPeriodic, dlo4,
+                            dhi4);
+        axis_slopes2<ORDER>(at(-2 * sy), at(-sy), f, at(sy), at(2 * sy), 2, 5, kPeriodic, dlo5,
+                            dhi5);
+        axis_slopes2<ORDER>(at(om2), at(om1), f, at(op1), at(op2), 2, 5, kPeriodic, dlo6, dhi6);
+        float alo, ahi, blo, bhi;
+        axis_slopes<ORDER>(vw(i, -2), vw(i, -1), f.x, vw(i, 1), vw(i, 2), i, NE, SKIND, alo,
+                           ahi);
+        axis_slopes<ORDER>(vw(i + 1, -2), vw(i + 1, -1), f.y, vw(i + 1, 1), vw(i + 1, 2), i + 1,
+                           NE, SKIND, blo, bhi);
+        const float2 dlo7 = make_float2(alo, blo), dhi7 = make_float2(ahi, bhi);
+        const float2 ve = make_float2(__ldg(s.ev + i), __ldg(s.ev + i + 1));
+        const float2 fex = __fmul2_rn(ve, f2(cs6)), fey = __fmul2_rn(ve, f2(sn6));
+        const float2 we = __fmul2_rn(make_float2(fabsf(ve.x), fabsf(ve.y)), f2(g.ke));
+        const float2 ealo = make_float2(i == 0 ? 0.f : -g.ae, -g.ae);
+        const float2 eahi = make_float2(g.ae, i + 1 == NE - 1 ? 0.f : g.ae);
+        const float2 xlo = __fmul2_rn(make_float2(fminf(fex.x, 0.f), fminf(fex.y, 0.f)), f2(ih[4]));
+        const float2 xhi = __fmul2_rn(make_float2(fmaxf(fex.x, 0.f), fmaxf(fex.y, 0.f)), f2(ih[4]));
+        const float2 ylo = __fmul2_rn(make_float2(fminf(fey.x, 0.f), fminf(fey.y, 0.f)), f2(ih[5]));
+        const float2 yhi = __fmul2_rn(make_float2(fmaxf(fey.x, 0.f), fmaxf(fey.y, 0.f)), f2(ih[5]));
+        float2 total = __ffma2_rn(xlo, dlo4, __fmul2_rn(xhi, dhi4));
+        total = __ffma2_rn(ylo, dlo5, __ffma2_rn(yhi, dhi5, total));
+        const float2 g6 = __fmul2_rn(f2(0.5f * ih[6]), add2(dlo6, dhi6));
+        total = __ffma2_rn(we, make_float2(fabsf(g6.x), fabsf(g6.y)), total);
+        const float2 g7 = __fmul2_rn(f2(0.5f * ih[7]), add2(dlo7, dhi7));
+        total = add2(total, make_float2(fmaxf(ealo.x * g7.x, eahi.x * g7.x),
+                                        fmaxf(ealo.y * g7.y, eahi.y * g7.y)));
+        float2 diss = __fmul2_rn(__fmul2_rn(we, f2(ih[6])), sub2(dhi6, dlo6));
+        diss = __ffma2_rn(f2(g.ae * ih[7]), sub2(dhi7, dlo7), diss);
+        const float2 out = __ffma2_rn(f2(0.5f), diss, total);
+        pc[i] += out.x;
+        pc[i + 1] += out.y;
+      };
+#pragma unroll
+      for (int i = 0; i + 1 < NE; i += 2) evader_pair(i);
+      if (NE & 1) evader_one(NE - 1);
     }
     __syncthreads();  // every sum is complete; the padded block is free
     const int next = o + gridDim.x;
