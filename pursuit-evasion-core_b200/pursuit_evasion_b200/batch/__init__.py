@@ -7,7 +7,10 @@ With the exact arithmetic each solve's result equals a float64
 `RelativeSolver` advanced to the same horizon (and the reference
 executable's), bit for bit; the float32 cell update is the fast variant.
 `draw_batch` draws the heterogeneous solve set of the batched workload from
-a seed; `autotune.tune` picks the work-item tile per size bucket.
+a seed; `autotune.tune` picks the work-item tile per size bucket.  The
+solves are independent, so several GPUs split a batch with `partition`
+(each rank builds a `BatchSolver` on its own share, `local_share`) and
+exchange nothing.
 """
 
 from __future__ import annotations
@@ -20,7 +23,7 @@ import numpy as np
 from .. import _native
 from ..reversible.free_dp import RelativeGrid
 from ..reversible.model import ReversibleConfig, VehicleLimits
-from ..reversible.relative_solver import _params
+from ..reversible.relative_solver import _params, cfl_limit
 
 
 @dataclass(frozen=True)
@@ -68,6 +71,50 @@ def describe(solves):
                  e_acceleration=s.config.evader.acceleration,
                  capture_radius=s.config.capture_radius, horizon=s.horizon)
             for s in solves]
+
+
+def solve_steps(solve, *, cfl=0.8):
+    """RK2 steps of one solve to its horizon: steps of the CFL limit, the
+    last one cut to the horizon (the schedule of pe_batch_create)."""
+    limit = cfl_limit(solve.config, solve.grid, cfl=cfl)
+    t, steps = 0.0, 0
+    while t < solve.horizon - 1e-12:
+        t += min(limit, solve.horizon - t)
+        steps += 1
+    return steps
+
+
+def solve_work(solve, *, cfl=0.8):
+    """Cell-stages of one solve: cells x 2 stages x RK2 steps."""
+    return solve.grid.states * 2 * solve_steps(solve, cfl=cfl)
+
+
+def partition(solves, parts, *, cfl=0.8):
+    """Split a batch over `parts` GPUs: a list of `parts` sorted index
+    lists that together hold every solve once.  Greedy longest first: the
+    solves in decreasing cell-stages (ties by index) each go to the share
+    with the least work so far (ties to the lowest share), so every share
+    ends within one solve's work of the mean.  The result depends only on
+    the solves, so every rank computes the same split without talking."""
+    if parts < 1:
+        raise ValueError("parts must be >= 1")
+    work = [solve_work(s, cfl=cfl) for s in solves]
+    order = sorted(range(len(solves)), key=lambda i: (-work[i], i))
+    load = [0] * parts
+    shares = [[] for _ in range(parts)]
+    for i in order:
+        k = min(range(parts), key=lambda j: (load[j], j))
+        shares[k].append(i)
+        load[k] += work[i]
+    return [sorted(sh) for sh in shares]
+
+
+def local_share(solves, rank, world, *, cfl=0.8):
+    """(indices, solves) of rank `rank` of `world` under `partition`."""
+    if not 0 <= rank < world:
+        raise ValueError("rank must lie in [0, world)")
+    idx = partition(solves, world, cfl=cfl)[rank]
+    return idx, [solves[i] for i in idx]
 
 
 class BatchSolver:
