@@ -1,6 +1,6 @@
 """Learned warm start of minimum-time value iteration, and its evaluation.
 
-The plain DP is the reference and the judge: `time_to_converged` solves the
+The plain DP decides the answer: `time_to_converged` solves the
 relative 5D minimum-time game (semi-Lagrangian value iteration, a
 contraction) to a sup-norm residual `tol` from the cold start (u = 1 outside
 the capture disk) and again from a surrogate prediction, and reports the

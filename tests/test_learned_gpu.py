@@ -1,6 +1,6 @@
 """Learned warm start: a surrogate trained by the package's own kernels on a
 minimum-time table warm-starts value iteration, which converges to the same
-table as the cold start (the plain DP stays the judge) in fewer
+table as the cold start (the plain DP decides the answer) in fewer
 iterations; online queries of arbitrary states agree with the table."""
 
 import numpy as np
