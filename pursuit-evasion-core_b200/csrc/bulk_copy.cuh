@@ -1,5 +1,5 @@
 // Bulk asynchronous copies (the TMA engine's cp.async.bulk, global ->
-// shared, no tensor map, no multicast) and the shared-memory mbarriers they
+// shared, no tensor map, into this CTA only) and the shared-memory mbarriers they
 // complete on, as inline PTX for sm_100a.  Used by the persistent stage
 // kernels that stream planes into shared-memory rings.
 #pragma once
