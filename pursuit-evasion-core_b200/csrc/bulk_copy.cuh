@@ -1,7 +1,7 @@
 // Bulk asynchronous copies (the TMA engine's cp.async.bulk, global ->
-// shared, no tensor map, into this CTA only) and the shared-memory mbarriers they
-// complete on, as inline PTX for sm_100a.  Used by the persistent stage
-// kernels that stream planes into shared-memory rings.
+// shared, no tensor map, into this CTA only) and the shared-memory
+// mbarriers they complete on, as inline PTX for sm_100a.  Used by the
+// persistent stage kernels that stream planes into shared-memory rings.
 #pragma once
 
 #include <cstdint>
