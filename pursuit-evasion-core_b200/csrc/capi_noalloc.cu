@@ -116,6 +116,7 @@ extern "C" int pe_relative_step_noalloc(const pe_relative_params *params,
   g.acc_e = params->e_acceleration;
   g.curv_p = params->p_curvature;
   g.curv_e = params->e_curvature;
+  pe::set_reciprocals(g);
 
   // Heading tables (native_relative.cpp:84-89) into the scratch array:
   // only the nh sines and nh cosines this grid uses are copied.

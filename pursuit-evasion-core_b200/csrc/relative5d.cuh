@@ -27,7 +27,23 @@ struct Rel5Grid {
   // [own_lo, own_lo + own_n) of a buffer whose first slab is global slab
   // slab_lo; own_n == 0 means the whole grid in one buffer
   int own_lo, own_n, slab_lo;
+  // 1/h and 1/(h*h) of each axis, rounded to nearest (set_reciprocals):
+  // the exact stage's divisions by the spacings go through them
+  double rdx, rdx2, rdphi, rdphi2, rdvp, rdvp2, rdve, rdve2;
 };
+
+// The reciprocals of a grid's spacings and of their squares (the squares
+// rounded as the exact stage forms them, h * h).
+inline void set_reciprocals(Rel5Grid &g) {
+  g.rdx = 1.0 / g.dx;
+  g.rdx2 = 1.0 / (g.dx * g.dx);
+  g.rdphi = 1.0 / g.dphi;
+  g.rdphi2 = 1.0 / (g.dphi * g.dphi);
+  g.rdvp = 1.0 / g.dvp;
+  g.rdvp2 = 1.0 / (g.dvp * g.dvp);
+  g.rdve = 1.0 / g.dve;
+  g.rdve2 = 1.0 / (g.dve * g.dve);
+}
 
 // Device-side reduction words of one handle.
 struct Rel5Stats {

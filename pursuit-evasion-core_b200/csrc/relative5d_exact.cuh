@@ -18,19 +18,40 @@ struct Slopes {
   double lo, hi;
 };
 
-// One-axis ENO slopes at node j (native_relative.cpp:38-67).
+// a / b rounded to nearest, for b > 0 with r = 1/b rounded to nearest, by
+// Markstein's correction of the product a * r (P. Markstein, "IA-64 and
+// Elementary Functions", 2000; Muller et al., "Handbook of Floating-Point
+// Arithmetic", the correction theorem for division): with q0 = RN(a r), the
+// residual a - b q0 is exact through an FMA, and RN(q0 + residual * r)
+// equals RN(a / b) whenever nothing underflows or overflows.  A zero
+// residual means q0 is already exact (and keeps the sign of a zero a);
+// dividends outside [2^-900, 2^900] in magnitude (zeros, NaN, or far
+// outside any slope of these grids) take the division itself.  One
+// multiply and two FMAs instead of a full IEEE double division, with the
+// same result bit for bit.
+__device__ __forceinline__ double div_const(double a, double b, double r) {
+  const double m = fabs(a);
+  if (!(m >= 0x1p-900 && m <= 0x1p+900)) return a == 0.0 ? a * r : a / b;
+  const double q0 = a * r;
+  const double rho = fma(-q0, b, a);
+  return rho == 0.0 ? q0 : fma(rho, r, q0);
+}
+
+// One-axis ENO slopes at node j (native_relative.cpp:38-67); rh, rhh are
+// 1/h and 1/(h*h) rounded to nearest.
 template <int ORDER, typename T>
 __device__ __forceinline__ Slopes eno_axis(const T *__restrict__ s,
                                            int64_t j, int64_t stride, int pos,
-                                           int n, double h, bool periodic) {
+                                           int n, double h, double rh, double rhh,
+                                           bool periodic) {
   Slopes r;
   const double v = s[j];
   if (!periodic && pos == 0) {
-    r.lo = r.hi = ((double)s[j + stride] - v) / h;
+    r.lo = r.hi = div_const((double)s[j + stride] - v, h, rh);
     return r;
   }
   if (!periodic && pos == n - 1) {
-    r.lo = r.hi = (v - (double)s[j - stride]) / h;
+    r.lo = r.hi = div_const(v - (double)s[j - stride], h, rh);
     return r;
   }
   // Offsets of the neighbours, wrapped on the periodic axis.
@@ -39,20 +60,20 @@ __device__ __forceinline__ Slopes eno_axis(const T *__restrict__ s,
   const int64_t op1 = (periodic && pos + 1 >= n) ? stride - wrap : stride;
   const double vm = s[j + om1];
   const double vp = s[j + op1];
-  r.lo = (v - vm) / h;
-  r.hi = (vp - v) / h;
+  r.lo = div_const(v - vm, h, rh);
+  r.hi = div_const(vp - v, h, rh);
   if (ORDER == 1) return r;
   const double hh = h * h;
-  const double c2 = (vp - 2 * v + vm) / hh;
+  const double c2 = div_const(vp - 2 * v + vm, hh, rhh);
   double l2 = c2, r2 = c2;
   if (periodic || pos >= 2) {
     const int64_t om2 = (periodic && pos < 2) ? wrap - 2 * stride : -2 * stride;
-    l2 = (v - 2 * vm + (double)s[j + om2]) / hh;
+    l2 = div_const(v - 2 * vm + (double)s[j + om2], hh, rhh);
   }
   if (periodic || pos + 2 < n) {
     const int64_t op2 =
         (periodic && pos + 2 >= n) ? 2 * stride - wrap : 2 * stride;
-    r2 = ((double)s[j + op2] - 2 * vp + v) / hh;
+    r2 = div_const((double)s[j + op2] - 2 * vp + v, hh, rhh);
   }
   r.lo += .5 * h * (fabs(l2) < fabs(c2) ? l2 : c2);
   r.hi -= .5 * h * (fabs(c2) < fabs(r2) ? c2 : r2);
@@ -123,11 +144,14 @@ __device__ __forceinline__ void cell_update(const Rel5Grid &g, const Rel5Stage &
   const double wp = fabs(vp) * g.curv_p, we = fabs(ve) * g.curv_e;
   const double bx = ve * s.cs[ip] - vp, by = ve * s.sn[ip];
 
-  const Slopes sx = eno_axis<ORDER, T>(src, j, 1, ix, g.nx, g.dx, false);
-  const Slopes sy = eno_axis<ORDER, T>(src, j, g.sy, iy, g.nx, g.dx, false);
-  const Slopes sp = eno_axis<ORDER, T>(src, j, g.sp, ip, g.nh, g.dphi, true);
-  const Slopes sv = eno_axis<ORDER, T>(src, j, g.sv, iv, g.nvp, g.dvp, false);
-  const Slopes se = eno_axis<ORDER, T>(src, j, g.se, ie, g.nve, g.dve, false);
+  const Slopes sx = eno_axis<ORDER, T>(src, j, 1, ix, g.nx, g.dx, g.rdx, g.rdx2, false);
+  const Slopes sy = eno_axis<ORDER, T>(src, j, g.sy, iy, g.nx, g.dx, g.rdx, g.rdx2, false);
+  const Slopes sp =
+      eno_axis<ORDER, T>(src, j, g.sp, ip, g.nh, g.dphi, g.rdphi, g.rdphi2, true);
+  const Slopes sv =
+      eno_axis<ORDER, T>(src, j, g.sv, iv, g.nvp, g.dvp, g.rdvp, g.rdvp2, false);
+  const Slopes se =
+      eno_axis<ORDER, T>(src, j, g.se, ie, g.nve, g.dve, g.rdve, g.rdve2, false);
 
   const double gx = .5 * (sx.lo + sx.hi), gy = .5 * (sy.lo + sy.hi),
                gp = .5 * (sp.lo + sp.hi), gv = .5 * (sv.lo + sv.hi),

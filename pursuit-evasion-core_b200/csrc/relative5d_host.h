@@ -79,6 +79,7 @@ inline pe::Rel5Grid make_grid(const pe_relative_params *p) {
   g.acc_e = p->e_acceleration;
   g.curv_p = p->p_curvature;
   g.curv_e = p->e_curvature;
+  pe::set_reciprocals(g);
   return g;
 }
 
