@@ -1,6 +1,6 @@
 /* Test infrastructure (the oracle library): a check, in the host's IEEE
  * double arithmetic, of the division used by the GPU exact stage
- * (csrc/relative5d_exact.cuh, div_const): a / b for b > 0 as the product
+ * (csrc/div_rn.cuh, rn::div_const): a / b for b > 0 as the product
  * a * r with r = RN(1/b), corrected once through an FMA (Markstein's
  * correction theorem: with q0 = RN(a r) and the exact residual
  * a - b q0, RN(q0 + residual * r) = RN(a / b) when nothing underflows or
@@ -21,6 +21,14 @@ static double div_const(double a, double b, double r) {
   const double q0 = a * r;
   const double rho = fma(-q0, b, a);
   return rho == 0.0 ? q0 : fma(rho, r, q0);
+}
+
+static float div_constf(float a, float b, float r) {
+  const float m = fabsf(a);
+  if (!(m >= 0x1p-80f && m <= 0x1p+100f)) return a == 0.f ? a * r : a / b;
+  const float q0 = a * r;
+  const float rho = fmaf(-q0, b, a);
+  return rho == 0.f ? q0 : fmaf(rho, r, q0);
 }
 
 static uint64_t next(uint64_t *s) {
@@ -64,6 +72,40 @@ long long po_div_const_check(double b, long long n, unsigned long long seed) {
       }
     }
     const double q1 = a / b, q2 = div_const(a, b, r);
+    if (memcmp(&q1, &q2, sizeof q1) != 0) bad++;
+  }
+  return bad;
+}
+
+/* The same for the float32 stages (8D and 6D): b and 1/b in float. */
+long long po_div_const_checkf(float b, long long n, unsigned long long seed) {
+  uint64_t s = seed ? seed : 88172645463325252ull;
+  const float r = 1.0f / b;
+  long long bad = 0;
+  for (long long i = 0; i < n; i++) {
+    float a;
+    switch (i % 5) {
+      case 0: a = (float)((unit(&s) * 2 - 1) * ldexp(1.0, (int)(next(&s) % 60) - 50)); break;
+      case 1: a = (float)(unit(&s) * 2 - 1) - (float)(unit(&s) * 2 - 1); break;
+      case 2: {
+        const float f = (float)(unit(&s) * 4 - 2), g = (float)(unit(&s) * 4 - 2);
+        const float h = (float)(unit(&s) * 4 - 2);
+        a = g - 2 * f + h;
+        break;
+      }
+      case 3: {
+        uint32_t bits = (uint32_t)next(&s);
+        bits = (bits & 0x807FFFFFu) | ((uint32_t)(127 + (int)(next(&s) % 60) - 30) << 23);
+        memcpy(&a, &bits, sizeof a);
+        break;
+      }
+      default: {
+        const float z[8] = {-0.0f, 0.0f, 1e-40f, -1e-40f, 1e-30f, -3e-25f, ldexpf(1.0f, -149),
+                            -ldexpf(1.0f, -140)};
+        a = z[next(&s) % 8];
+      }
+    }
+    const float q1 = a / b, q2 = div_constf(a, b, r);
     if (memcmp(&q1, &q2, sizeof q1) != 0) bad++;
   }
   return bad;

@@ -102,5 +102,6 @@ void po_sl_init(const po_sl_cfg *c, double *V);
 /* Bits in which the exact stage's division by a spacing b (through RN(1/b)
  * and one FMA correction) differs from a / b, over n drawn dividends. */
 long long po_div_const_check(double b, long long n, unsigned long long seed);
+long long po_div_const_checkf(float b, long long n, unsigned long long seed);
 
 #endif

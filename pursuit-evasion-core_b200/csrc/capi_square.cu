@@ -54,6 +54,13 @@ pe::Square6Grid make_grid(const pe_square_params *p) {
   const float extent = (float)p->extent;
   g.dx = 2 * extent / (g.n - 1);  // native_square.cpp:87
   g.dh = (float)(2 * pi / g.nh);
+  {
+    const float dx2 = g.dx * g.dx, dh2 = g.dh * g.dh;  // rounded as the stage forms them
+    g.rdx = 1.f / g.dx;
+    g.rdx2 = 1.f / dx2;
+    g.rdh = 1.f / g.dh;
+    g.rdh2 = 1.f / dh2;
+  }
   g.vp = (float)p->p_speed;
   g.ve = (float)p->e_speed;
   g.wp = (float)p->p_turn_rate;

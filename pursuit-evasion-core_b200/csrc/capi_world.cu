@@ -82,6 +82,8 @@ pe::World8Grid make_grid(const pe_world_params *p) {
     g.shape[k] = shape[k];
     g.spacing[k] = spacing[k];
     g.inv_spacing[k] = 1.f / spacing[k];
+    const float sq = spacing[k] * spacing[k];
+    g.inv_spacing_sq[k] = 1.f / sq;
   }
   g.stride[7] = 1;
   for (int k = 6; k >= 0; k--) g.stride[k] = g.stride[k + 1] * shape[k + 1];

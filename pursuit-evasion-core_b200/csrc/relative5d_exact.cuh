@@ -9,6 +9,7 @@
 // with -fmad=false (no multiply-add contraction, IEEE double division), so
 // each stored float equals the reference CPU's bit for bit.
 #pragma once
+#include "div_rn.cuh"
 #include "relative5d.cuh"
 
 namespace pe {
@@ -18,24 +19,7 @@ struct Slopes {
   double lo, hi;
 };
 
-// a / b rounded to nearest, for b > 0 with r = 1/b rounded to nearest, by
-// Markstein's correction of the product a * r (P. Markstein, "IA-64 and
-// Elementary Functions", 2000; Muller et al., "Handbook of Floating-Point
-// Arithmetic", the correction theorem for division): with q0 = RN(a r), the
-// residual a - b q0 is exact through an FMA, and RN(q0 + residual * r)
-// equals RN(a / b) whenever nothing underflows or overflows.  A zero
-// residual means q0 is already exact (and keeps the sign of a zero a);
-// dividends outside [2^-900, 2^900] in magnitude (zeros, NaN, or far
-// outside any slope of these grids) take the division itself.  One
-// multiply and two FMAs instead of a full IEEE double division, with the
-// same result bit for bit.
-__device__ __forceinline__ double div_const(double a, double b, double r) {
-  const double m = fabs(a);
-  if (!(m >= 0x1p-900 && m <= 0x1p+900)) return a == 0.0 ? a * r : a / b;
-  const double q0 = a * r;
-  const double rho = fma(-q0, b, a);
-  return rho == 0.0 ? q0 : fma(rho, r, q0);
-}
+using rn::div_const;  // division by a spacing, bit for bit (div_rn.cuh)
 
 // One-axis ENO slopes at node j (native_relative.cpp:38-67); rh, rhh are
 // 1/h and 1/(h*h) rounded to nearest.

@@ -12,6 +12,9 @@ struct Square6Grid {
   int64_t cells;
   int64_t stride[6];  // [xP, yP, thP, xE, yE, thE], thE fastest
   float dx, dh;       // native_square.cpp:87
+  // 1/dx, 1/(dx*dx), 1/dh, 1/(dh*dh) rounded to nearest (squares rounded in
+  // float): the exact stage's divisions go through them (div_rn.cuh)
+  float rdx, rdx2, rdh, rdh2;
   float vp, ve, wp, we, arena;
 };
 

@@ -7,6 +7,7 @@
 // Storage [xP, yP, thP, xE, yE, thE], thE fastest.  One thread per cell:
 // blockIdx.y walks the pursuer block (xP, yP, thP), the x dimension the
 // evader block (xE, yE, thE).
+#include "div_rn.cuh"
 #include "square6d.cuh"
 
 namespace pe {
@@ -36,17 +37,20 @@ __device__ __forceinline__ float at(const float *__restrict__ v, int64_t j, int6
 }
 
 // Backward / forward ENO slopes (native_square.cpp:50-61).
+// rh, rhh: 1/h and 1/(h*h) rounded to nearest; the divisions keep the
+// reference's bits (rn::div_const).
 __device__ __forceinline__ void slopes(const float *__restrict__ v, int64_t j, int64_t stride,
-                                       int pos, int n, float h, bool periodic, int order,
-                                       float &left, float &right) {
+                                       int pos, int n, float h, float rh, float rhh,
+                                       bool periodic, int order, float &left, float &right) {
   const float f = v[j], fm = at(v, j, stride, pos, n, -1, periodic),
               fp = at(v, j, stride, pos, n, 1, periodic);
-  left = (f - fm) / h;
-  right = (fp - f) / h;
+  left = rn::div_const(f - fm, h, rh);
+  right = rn::div_const(fp - f, h, rh);
   if (order == 2) {
-    const float dl = (f - 2 * fm + at(v, j, stride, pos, n, -2, periodic)) / (h * h);
-    const float dc = (fp - 2 * f + fm) / (h * h);
-    const float dr = (at(v, j, stride, pos, n, 2, periodic) - 2 * fp + f) / (h * h);
+    const float hh = h * h;
+    const float dl = rn::div_const(f - 2 * fm + at(v, j, stride, pos, n, -2, periodic), hh, rhh);
+    const float dc = rn::div_const(fp - 2 * f + fm, hh, rhh);
+    const float dr = rn::div_const(at(v, j, stride, pos, n, 2, periodic) - 2 * fp + f, hh, rhh);
     const float a = fabsf(dl) <= fabsf(dc) ? dl : dc;
     const float b = fabsf(dc) <= fabsf(dr) ? dc : dr;
     left += .5f * h * a;
@@ -80,7 +84,8 @@ __global__ void __launch_bounds__(256)
         float lm, rp;
         const bool periodic = k == 2 || k == 5;
         slopes(s.src, j, g.stride[k], q[k], periodic ? g.nh : g.n, periodic ? g.dh : g.dx,
-               periodic, g.order, lm, rp);
+               periodic ? g.rdh : g.rdx, periodic ? g.rdh2 : g.rdx2, periodic, g.order, lm,
+               rp);
         gr[k] = (lm + rp) * .5f;
         const float alpha = k == 2 ? g.wp : k == 5 ? g.we : fabsf(f[k]);
         diss += alpha * (rp - lm) * .5f;

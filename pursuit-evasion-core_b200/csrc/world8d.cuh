@@ -19,7 +19,9 @@ struct World8Grid {
   int64_t stride[8];
   int shape[8];
   float spacing[8];
-  float inv_spacing[8];  // 1 / spacing (fast variant)
+  float inv_spacing[8];     // 1 / spacing rounded to nearest
+  float inv_spacing_sq[8];  // 1 / (spacing * spacing) rounded to nearest (the
+                            // square rounded in float, as the stage forms it)
   float extent, arena, ap, ae, kp, ke;
 };
 

@@ -70,6 +70,8 @@ class Oracle:
             "po_rel_cells": (ctypes.c_size_t, [_P]),
             "po_div_const_check": (ctypes.c_longlong, [ctypes.c_double, ctypes.c_longlong,
                                                        ctypes.c_ulonglong]),
+            "po_div_const_checkf": (ctypes.c_longlong, [ctypes.c_float, ctypes.c_longlong,
+                                                        ctypes.c_ulonglong]),
             "po_rel_cfl_limit": (ctypes.c_double, [_P]),
             "po_rel_init": (None, [_P, _P, _P]),
             "po_rel_init_f64": (None, [_P, _P]),
