@@ -345,15 +345,46 @@ __global__ void __launch_bounds__(kThreads)
         for (int u = 0; u < kMaxActions; u++) worst[u] = -1e30f;
         unsigned alive = in_group >> u0;  // bit g: action u0 + g
         const uint8_t *allowed_e = d.e_allowed + (long long)ie * d.nea;
+        // the stencil of reply a + 1 (and its allowed flag) is loaded while
+        // reply a is reduced, so that its L2 latency overlaps the gathers;
+        // a disallowed reply's stencil is loaded and dropped
+        const long long s0 = (long long)ie * d.nea * kStencil;
+        int4 next_i[kStencil / 4];
+        float4 next_w[kStencil / 4];
+        bool next_ok = false;
+        if (d.nea > 0) {
+          next_ok = __ldg(allowed_e) != 0;
+#pragma unroll
+          for (int q = 0; q < kStencil / 4; q++) {
+            next_i[q] = __ldg(reinterpret_cast<const int4 *>(d.e_ids + s0) + q);
+            next_w[q] = __ldg(reinterpret_cast<const float4 *>(d.e_w + s0) + q);
+          }
+        }
         for (int a = 0; a < d.nea && alive; a++) {
-          if (!__ldg(allowed_e + a)) continue;
-          const long long s = ((long long)ie * d.nea + a) * kStencil;
+          int4 cur_i[kStencil / 4];
+          float4 cur_w[kStencil / 4];
+          const bool ok = next_ok;
+#pragma unroll
+          for (int q = 0; q < kStencil / 4; q++) {
+            cur_i[q] = next_i[q];
+            cur_w[q] = next_w[q];
+          }
+          if (a + 1 < d.nea) {
+            const long long s = s0 + (long long)(a + 1) * kStencil;
+            next_ok = __ldg(allowed_e + a + 1) != 0;
+#pragma unroll
+            for (int q = 0; q < kStencil / 4; q++) {
+              next_i[q] = __ldg(reinterpret_cast<const int4 *>(d.e_ids + s) + q);
+              next_w[q] = __ldg(reinterpret_cast<const float4 *>(d.e_w + s) + q);
+            }
+          }
+          if (!ok) continue;
           int t[kStencil];
           float w[kStencil];
 #pragma unroll
           for (int q = 0; q < kStencil / 4; q++) {
-            const int4 i4 = __ldg(reinterpret_cast<const int4 *>(d.e_ids + s) + q);
-            const float4 w4 = __ldg(reinterpret_cast<const float4 *>(d.e_w + s) + q);
+            const int4 i4 = cur_i[q];
+            const float4 w4 = cur_w[q];
             w[4 * q] = w4.x;
             w[4 * q + 1] = w4.y;
             w[4 * q + 2] = w4.z;
