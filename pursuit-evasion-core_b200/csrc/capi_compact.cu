@@ -306,25 +306,36 @@ __global__ void __launch_bounds__(kThreads)
     for (int u0 = 0; u0 < d.npa; u0 += group) {
       const unsigned in_group = allowed_u & (((1u << group) - 1u) << u0);
       if (!in_group) continue;  // the same for the whole CTA
-      // rows of the group's allowed actions over the reach list
-      for (int t = tid; t < r_n; t += kThreads) {
+      // rows of the group's allowed actions over the reach list, two reach
+      // entries (t, t + kThreads) per thread at a time so that the
+      // dependent (lookup, field) loads of both are in flight together; the
+      // second entry of an odd tail repeats the first and is not stored
+      for (int t = tid; t < r_n; t += 2 * kThreads) {
+        const int t2 = t + kThreads;
+        const bool two = t2 < r_n;
         const int ie = __ldg(d.reach_index + r_begin + t);
+        const int ie2 = two ? __ldg(d.reach_index + r_begin + t2) : ie;
         for (int u = u0; u < u0 + group && u < d.npa; u++) {
           if (!((in_group >> u) & 1u)) continue;
-          float v = 0.f;
+          float v = 0.f, v2 = 0.f;
 #pragma unroll
           for (int k = 0; k < kStencil; k++)
             if (s_w[u][k] > 0.f) {
-              float x;
+              float x, x2;
               if (PACKED) {
                 const int rank = __ldg(d.lookup + s_row[u][k] + ie);
+                const int rank2 = __ldg(d.lookup + s_row[u][k] + ie2);
                 x = rank < 0 ? d.exit_value : __ldg(cur + s_off[u][k] + rank);
+                x2 = rank2 < 0 ? d.exit_value : __ldg(cur + s_off[u][k] + rank2);
               } else {
                 x = __ldg(cur + s_off[u][k] + ie);
+                x2 = __ldg(cur + s_off[u][k] + ie2);
               }
               v = fmaf(s_w[u][k], x, v);
+              v2 = fmaf(s_w[u][k], x2, v2);
             }
           G[(u - u0) * rcap + t] = v;
+          if (two) G[(u - u0) * rcap + t2] = v2;
         }
       }
       __syncthreads();
