@@ -319,21 +319,23 @@ __global__ void __launch_bounds__(kThreads)
           if (!((in_group >> u) & 1u)) continue;
           float v = 0.f, v2 = 0.f;
 #pragma unroll
-          for (int k = 0; k < kStencil; k++)
-            if (s_w[u][k] > 0.f) {
-              float x, x2;
-              if (PACKED) {
-                const int rank = __ldg(d.lookup + s_row[u][k] + ie);
-                const int rank2 = __ldg(d.lookup + s_row[u][k] + ie2);
-                x = rank < 0 ? d.exit_value : __ldg(cur + s_off[u][k] + rank);
-                x2 = rank2 < 0 ? d.exit_value : __ldg(cur + s_off[u][k] + rank2);
-              } else {
-                x = __ldg(cur + s_off[u][k] + ie);
-                x2 = __ldg(cur + s_off[u][k] + ie2);
-              }
-              v = fmaf(s_w[u][k], x, v);
-              v2 = fmaf(s_w[u][k], x2, v2);
+          for (int k = 0; k < kStencil; k++) {
+            // a zero-weight tap has row and offset 0, so its loads stay in
+            // bounds and need no branch; only its FMA is skipped
+            const float wk = s_w[u][k];
+            float x, x2;
+            if (PACKED) {
+              const int rank = __ldg(d.lookup + s_row[u][k] + ie);
+              const int rank2 = __ldg(d.lookup + s_row[u][k] + ie2);
+              x = rank < 0 ? d.exit_value : __ldg(cur + s_off[u][k] + rank);
+              x2 = rank2 < 0 ? d.exit_value : __ldg(cur + s_off[u][k] + rank2);
+            } else {
+              x = __ldg(cur + s_off[u][k] + ie);
+              x2 = __ldg(cur + s_off[u][k] + ie2);
             }
+            v = wk > 0.f ? fmaf(wk, x, v) : v;
+            v2 = wk > 0.f ? fmaf(wk, x2, v2) : v2;
+          }
           G[(u - u0) * rcap + t] = v;
           if (two) G[(u - u0) * rcap + t2] = v2;
         }
@@ -412,7 +414,7 @@ __global__ void __launch_bounds__(kThreads)
             float value = 0.f;
 #pragma unroll
             for (int q = 0; q < kStencil; q++)
-              if (w[q] > 0.f) value = fmaf(w[q], row[t[q]], value);
+              value = w[q] > 0.f ? fmaf(w[q], row[t[q]], value) : value;  // t[q] = 0 at w = 0
             worst[g] = fmaxf(worst[g], value);
             if (worst[g] >= best) alive &= ~(1u << g);
           }
